@@ -1,0 +1,456 @@
+// The actor chain run between steps: path-limit aborter, parameter
+// transporter (bound -> free -> bound Jacobian and covariance transport),
+// pointwise material interactor and parameter setter.
+//
+// Reference:
+//   pathlimit_aborter            propagator/actors/aborters.hpp:23-76
+//   parameter_transporter        propagator/actors/parameter_updater.hpp:314-419
+//   get_full_jacobian            parameter_updater.hpp:422-572; the product
+//                                F2B (P2F F2P + I) J_t B2F of
+//                                codegen/detray-sympy/gen_full_jacobian.py:47-59
+//   covariance transport         codegen gen_transport_covariance_to_bound_impl.py
+//                                (J C J^T with the identity q/p row and time
+//                                column the generator assumes)
+//   frame Jacobians              propagator/detail/jacobian_{cartesian,polar,
+//                                concentric_cylindrical}.hpp, jacobian_engine.hpp
+//   parameter_setter             parameter_updater.hpp:577-627
+//   external mask tolerance      propagator/detail/noise_estimation.hpp:22-107
+//   material interactor          propagator/actors/pointwise_material_interactor.hpp:59-326
+//   interaction formulas         material/interaction.hpp:28-310,
+//                                material/detail/relativistic_quantities.hpp
+#pragma once
+
+#include "navigator.cuh"
+#include "stepper.cuh"
+
+namespace dprop {
+
+// index of (i, j) in the row-wise upper triangle of a symmetric 6x6 matrix
+DPROP_HD constexpr int tri6(int i, int j) {
+    return (i <= j) ? (i * (11 - i)) / 2 + j : (j * (11 - j)) / 2 + i;
+}
+
+// Bound track parameters of the updater state: [loc0, loc1, phi, theta,
+// q/p, t], covariance, and the surface they are expressed on.
+template <typename S>
+struct bound_state {
+    S v[6];
+    S cov[21];
+    uint32_t sf;  // k_invalid: no surface yet
+};
+
+template <typename S>
+struct actor_cfg {
+    S path_limit;
+    bool use_path_limit;
+    bool use_interactor;
+    bool estimate_noise;
+    S n_stddev;
+    S accumulated_error;
+    S mass;
+    bool electron;  // Rossi-Greisen instead of Highland
+};
+
+// --------------------------------------------------------- local frames
+template <typename S>
+DPROP_HD vec3<S> bound_dir(S phi, S theta) {
+    const S st = sin(theta);
+    return {cos(phi) * st, sin(phi) * st, cos(theta)};
+}
+
+// bound -> free position for the surface frame (bound_to_free_vector,
+// tracks/detail/transform_track_parameters.hpp:43-74)
+template <typename S>
+DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S>& det,
+                                   const dev_surface& sf, S l0, S l1) {
+    const dev_transform<S>& trf = det.transforms[sf.transform];
+    switch (sf.shape) {
+        case e_ring:
+            return trf.point_to_global({l0 * cos(l1), l0 * sin(l1), S(0)});
+        case e_concentric_cylinder: {
+            const S r = det.masks[sf.mask_begin].v[0];
+            return {r * cos(l0), r * sin(l0), l1};
+        }
+        default:
+            return trf.point_to_global({l0, l1, S(0)});
+    }
+}
+
+// free -> bound vector on a surface (free_to_bound_vector)
+template <typename S>
+DPROP_HD void free_to_bound(const detector_view<S>& det, const dev_surface& sf,
+                            const step_state<S>& st, S out[6]) {
+    const dev_transform<S>& trf = det.transforms[sf.transform];
+    global_to_bound_local(sf.shape, trf, st.pos, out[0], out[1]);
+    out[2] = phi_of(st.dir);
+    out[3] = theta_of(st.dir);
+    out[4] = st.qop;
+    out[5] = st.time;
+}
+
+// columns d(pos)/d(loc0), d(pos)/d(loc1) (get_derivative_dpos_dloc)
+template <typename S>
+DPROP_HD void dpos_dloc(const detector_view<S>& det, const dev_surface& sf,
+                        vec3<S> pos, vec3<S>& c0, vec3<S>& c1) {
+    const dev_transform<S>& trf = det.transforms[sf.transform];
+    switch (sf.shape) {
+        case e_ring: {
+            const vec3<S> l = trf.point_to_local(pos);
+            const S lrad = perp(l);
+            const S lphi = phi_of(l);
+            const S cp = cos(lphi);
+            const S sp = sin(lphi);
+            const vec3<S> dx = trf.x();
+            const vec3<S> dy = trf.y();
+            c0 = dx * cp + dy * sp;
+            c1 = (dy * cp - dx * sp) * lrad;
+            return;
+        }
+        case e_concentric_cylinder: {
+            const S r = perp(pos);
+            const S ph = phi_of(pos);
+            c0 = {-r * sin(ph), r * cos(ph), S(0)};
+            c1 = {S(0), S(0), S(1)};
+            return;
+        }
+        default:
+            c0 = trf.x();
+            c1 = trf.y();
+            return;
+    }
+}
+
+// rows d(loc0)/d(pos), d(loc1)/d(pos) (get_derivative_dloc_dpos)
+template <typename S>
+DPROP_HD void dloc_dpos(const detector_view<S>& det, const dev_surface& sf,
+                        vec3<S> pos, vec3<S>& r0, vec3<S>& r1) {
+    const dev_transform<S>& trf = det.transforms[sf.transform];
+    switch (sf.shape) {
+        case e_ring: {
+            const vec3<S> l = trf.point_to_local(pos);
+            const S lrad = perp(l);
+            const S lphi = phi_of(l);
+            const S cp = cos(lphi);
+            const S sp = sin(lphi);
+            const vec3<S> du = trf.x();  // first row of R^T
+            const vec3<S> dv = trf.y();
+            r0 = du * cp + dv * sp;
+            r1 = (S(1) / lrad) * (cp * dv - sp * du);
+            return;
+        }
+        case e_concentric_cylinder: {
+            const S r_inv = S(1) / perp(pos);
+            const S ph = phi_of(pos);
+            r0 = {-r_inv * sin(ph), r_inv * cos(ph), S(0)};
+            r1 = {S(0), S(0), S(1)};
+            return;
+        }
+        default:
+            r0 = trf.x();
+            r1 = trf.y();
+            return;
+    }
+}
+
+// surface normal used by the path derivative and the incidence angle
+template <typename S>
+DPROP_HD vec3<S> surface_normal_at_pos(const detector_view<S>& det,
+                                       const dev_surface& sf, vec3<S> pos) {
+    if (sf.shape == e_concentric_cylinder) {
+        const S ph = phi_of(pos);
+        return {cos(ph), sin(ph), S(0)};
+    }
+    return det.transforms[sf.transform].z();
+}
+
+template <typename S>
+DPROP_HD vec3<S> surface_normal_at_bound(const detector_view<S>& det,
+                                         const dev_surface& sf, S l0) {
+    if (sf.shape == e_concentric_cylinder) {
+        return {cos(l0), sin(l0), S(0)};
+    }
+    return det.transforms[sf.transform].z();
+}
+
+// ---------------------------------------------------- full Jacobian
+// J_full (6x6) from the departure bound state, the transport Jacobian and
+// the current (destination) free state.  Only rows 0..3 x cols 0..4 are
+// non-trivial (the q/p row and the time column are identity, as the
+// covariance-transport generator assumes); they are returned in G[4][5].
+template <typename S>
+DPROP_HD void full_jacobian(const detector_view<S>& det,
+                            const bound_state<S>& dep, const dev_surface& dep_sf,
+                            const dev_surface& dst_sf, const step_state<S>& st,
+                            vec3<S> dtds, S G[4][5]) {
+    // bound -> free at the departure surface
+    const vec3<S> dep_pos = bound_to_free_pos(det, dep_sf, dep.v[0], dep.v[1]);
+    vec3<S> p0, p1;
+    dpos_dloc(det, dep_sf, dep_pos, p0, p1);
+    const S ph = dep.v[2];
+    const S th = dep.v[3];
+    const S ct = cos(th), st_ = sin(th), cp = cos(ph), sp = sin(ph);
+    // ddir/dphi, ddir/dtheta
+    const vec3<S> dd_phi{-st_ * sp, st_ * cp, S(0)};
+    const vec3<S> dd_th{ct * cp, ct * sp, -st_};
+
+    // M1 = J_t * B2F (8x6), rows pos(0..2), time(3), dir(4..6), qop(7)
+    // pos rows: [p0 | p1 | A dd_phi | A dd_th | c | 0]
+    // dir rows: [0 | 0 | B dd_phi | B dd_th | d | 0]
+    // qop row:  [0 0 0 0 e 0]; time row: e5
+    const transport_jac<S>& J = st.jac;
+    S m1p[3][5], m1d[3][5];
+    const S p0a[3] = {p0.x, p0.y, p0.z};
+    const S p1a[3] = {p1.x, p1.y, p1.z};
+    const S dpa[3] = {dd_phi.x, dd_phi.y, dd_phi.z};
+    const S dta[3] = {dd_th.x, dd_th.y, dd_th.z};
+    const S ca[3] = {J.c.x, J.c.y, J.c.z};
+    const S da[3] = {J.d.x, J.d.y, J.d.z};
+    for (int r = 0; r < 3; ++r) {
+        S a2 = S(0), a3 = S(0), b2 = S(0), b3 = S(0);
+        for (int k = 0; k < 3; ++k) {
+            a2 += J.A(r, k) * dpa[k];
+            a3 += J.A(r, k) * dta[k];
+            b2 += J.B(r, k) * dpa[k];
+            b3 += J.B(r, k) * dta[k];
+        }
+        m1p[r][0] = p0a[r];
+        m1p[r][1] = p1a[r];
+        m1p[r][2] = a2;
+        m1p[r][3] = a3;
+        m1p[r][4] = ca[r];
+        m1d[r][0] = S(0);
+        m1d[r][1] = S(0);
+        m1d[r][2] = b2;
+        m1d[r][3] = b3;
+        m1d[r][4] = da[r];
+    }
+
+    // path correction: M2 = M1 + P2F (F2P M1), F2P has position terms only
+    const vec3<S> n = surface_normal_at_pos(det, dst_sf, st.pos);
+    const S inv_nd = S(-1) / dot(n, st.dir);
+    const S f[3] = {inv_nd * n.x, inv_nd * n.y, inv_nd * n.z};
+    S s[5];
+    for (int c = 0; c < 5; ++c) {
+        s[c] = f[0] * m1p[0][c] + f[1] * m1p[1][c] + f[2] * m1p[2][c];
+    }
+    const S dir_a[3] = {st.dir.x, st.dir.y, st.dir.z};
+    const S dtds_a[3] = {dtds.x, dtds.y, dtds.z};
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 5; ++c) {
+            m1p[r][c] += dir_a[r] * s[c];
+            m1d[r][c] += dtds_a[r] * s[c];
+        }
+    }
+
+    // free -> bound at the destination
+    vec3<S> r0, r1;
+    dloc_dpos(det, dst_sf, st.pos, r0, r1);
+    const S dth = theta_of(st.dir);
+    const S dph = phi_of(st.dir);
+    const S cth = cos(dth), sth = sin(dth), cph = cos(dph), sph = sin(dph);
+    const S a_phi[3] = {-sph / sth, cph / sth, S(0)};
+    const S a_th[3] = {cph * cth, sph * cth, -sth};
+    const S r0a[3] = {r0.x, r0.y, r0.z};
+    const S r1a[3] = {r1.x, r1.y, r1.z};
+    for (int c = 0; c < 5; ++c) {
+        G[0][c] = r0a[0] * m1p[0][c] + r0a[1] * m1p[1][c] + r0a[2] * m1p[2][c];
+        G[1][c] = r1a[0] * m1p[0][c] + r1a[1] * m1p[1][c] + r1a[2] * m1p[2][c];
+        G[2][c] = a_phi[0] * m1d[0][c] + a_phi[1] * m1d[1][c];
+        G[3][c] = a_th[0] * m1d[0][c] + a_th[1] * m1d[1][c] +
+                  a_th[2] * m1d[2][c];
+    }
+}
+
+// C <- J C J^T with J = [[G (4x5), 0], [e4], [e5]]
+template <typename S>
+DPROP_HD void transport_covariance(const S G[4][5], S cov[21]) {
+    S C[6][6];
+    for (int i = 0; i < 6; ++i) {
+        for (int j = 0; j < 6; ++j) {
+            C[i][j] = cov[tri6(i, j)];
+        }
+    }
+    // T = G * C[0:5, 0:6]  (4x6)
+    S T[4][6];
+    for (int i = 0; i < 4; ++i) {
+        for (int j = 0; j < 6; ++j) {
+            S a = S(0);
+            for (int k = 0; k < 5; ++k) {
+                a += G[i][k] * C[k][j];
+            }
+            T[i][j] = a;
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        for (int j = i; j < 4; ++j) {
+            S a = S(0);
+            for (int k = 0; k < 5; ++k) {
+                a += T[i][k] * G[j][k];
+            }
+            cov[tri6(i, j)] = a;
+        }
+        cov[tri6(i, 4)] = T[i][4];
+        cov[tri6(i, 5)] = T[i][5];
+    }
+    // rows 4 and 5 (q/p, time) unchanged
+}
+
+// --------------------------------------------------- material physics
+template <typename S>
+struct rel_quantities {
+    S qop, q2_over_beta2, beta2, beta_gamma, gamma, gamma2, E, Wmax;
+};
+
+template <typename S>
+DPROP_HD rel_quantities<S> make_rq(S mass, S qop, S q) {
+    rel_quantities<S> rq;
+    rq.qop = qop;
+    rq.q2_over_beta2 = q * q + (mass * qop) * (mass * qop);
+    const S m_over_p = mass * ((q != S(0)) ? fabs(qop / q) : fabs(qop));
+    const S p_over_m = S(1) / m_over_p;
+    rq.beta2 = S(1) / (S(1) + m_over_p * m_over_p);
+    rq.beta_gamma = p_over_m;
+    rq.gamma = sqrt(S(1) + p_over_m * p_over_m);
+    rq.gamma2 = rq.gamma * rq.gamma;
+    rq.E = rq.gamma * mass;
+    const S me = static_cast<S>(constant::m_e);
+    const S mfrac = me / mass;
+    rq.Wmax = (S(2) * me * rq.beta_gamma * rq.beta_gamma) /
+              (S(1) + S(2) * rq.gamma * mfrac + mfrac * mfrac);
+    return rq;
+}
+
+template <typename S>
+DPROP_HD S eps_per_length(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
+    const S K = static_cast<S>(0.307075 * unit::MeV * unit::cm2);
+    return S(0.5) * K * mat.molar_electron_density * rq.q2_over_beta2;
+}
+
+template <typename S>
+DPROP_HD S delta_half(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
+    if (mat.has_density_effect == S(0)) {
+        if (rq.beta_gamma < S(10)) {
+            return S(0);
+        }
+        const S plasma = static_cast<S>(28.816 * unit::eV) *
+                         sqrt(S(1000) * mat.molar_electron_density);
+        return log(rq.beta_gamma * plasma / mat.mean_excitation_energy) -
+               S(0.5);
+    }
+    const S x = log10(rq.beta_gamma);
+    S delta = S(0);
+    if (x >= mat.density_x0) {
+        delta = S(2) * static_cast<S>(constant::ln10) * x - mat.density_c;
+        if (x < mat.density_x1) {
+            delta += mat.density_a * pow(mat.density_x1 - x, mat.density_m);
+        }
+    }
+    return S(0.5) * delta;
+}
+
+template <typename S>
+DPROP_HD S bethe_bloch(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
+    const S epl = eps_per_length(mat, rq);
+    if (epl <= S(0)) {
+        return S(0);
+    }
+    const S dhalf = delta_half(mat, rq);
+    const S I = mat.mean_excitation_energy;
+    const S u = S(2) * static_cast<S>(constant::m_e) * rq.beta_gamma *
+                rq.beta_gamma;
+    const S A = S(0.5) * log(u * rq.Wmax / (I * I));
+    return S(2) * epl * (A - rq.beta2 - dhalf);
+}
+
+template <typename S>
+DPROP_HD S landau_sigma_qop(S path_segment, const dev_slab<S>& mat,
+                            const rel_quantities<S>& rq, S q) {
+    const S fwhm = S(4) * eps_per_length(mat, rq) * path_segment;
+    const S sigmaE = S(0.5) * static_cast<S>(constant::inv_sqrt2) * fwhm /
+                     sqrt(static_cast<S>(constant::ln2));
+    const S p_inv = rq.qop / q;
+    return sqrt(rq.q2_over_beta2) * p_inv * p_inv * sigmaE;
+}
+
+template <typename S>
+DPROP_HD S scattering_theta0(S x_over_x0, const rel_quantities<S>& rq, S q,
+                             bool electron) {
+    if (x_over_x0 <= S(0)) {
+        return S(0);
+    }
+    const S mom_inv = fabs(rq.qop / q);
+    const S t = sqrt(x_over_x0 * rq.q2_over_beta2);
+    if (electron) {
+        return static_cast<S>(17.5 * unit::MeV) * mom_inv * t *
+               (S(1) + S(0.125) * log10(S(10) * x_over_x0));
+    }
+    return static_cast<S>(13.6 * unit::MeV) * mom_inv * t *
+           (S(1) + S(0.038) * S(2) * log(t));
+}
+
+// pointwise_material_interactor::update on the bound state
+template <typename S>
+DPROP_HD bool interact(const detector_view<S>& det, const dev_surface& sf,
+                       bound_state<S>& b, const actor_cfg<S>& cfg, S q,
+                       S nav_dir) {
+    if (sf.material == k_invalid) {
+        return false;
+    }
+    const dev_slab<S> mat = det.slabs[sf.material];
+    const vec3<S> dir = bound_dir(b.v[2], b.v[3]);
+    const vec3<S> n = surface_normal_at_bound(det, sf, b.v[0]);
+    const S cos_inc = fabs(dot(dir, n));
+    if (mat.thickness <= limits<S>::epsilon()) {
+        return false;
+    }
+    const S qop = b.v[4];
+    if (qop == S(0)) {
+        return false;
+    }
+    const S path_segment = mat.thickness / cos_inc;
+    const rel_quantities<S> rq = make_rq(cfg.mass, qop, q);
+    const S e_loss = path_segment * bethe_bloch(mat, rq);
+    const S sigma_qop = landau_sigma_qop(path_segment, mat, rq, q);
+    const S theta0 = scattering_theta0(mat.thickness_in_X0 / cos_inc, rq, q,
+                                       cfg.electron);
+    // energy loss
+    const S m = cfg.mass;
+    const S p = q / qop;
+    const S next_e = sqrt(m * m + p * p) - copysign(e_loss, nav_dir);
+    const S next_p = (m < next_e) ? sqrt(next_e * next_e - m * m) : S(0);
+    const S next_qop = (q != S(0)) ? q / next_p : S(1) / next_p;
+    b.v[4] = (next_p == S(0)) ? limits<S>::max() : next_qop;
+    b.cov[tri6(4, 4)] += sigma_qop * sigma_qop;
+    // multiple scattering (uses the unmodified direction)
+    const S var = theta0 * theta0;
+    b.cov[tri6(2, 2)] += (dir.z == S(1)) ? limits<S>::max()
+                                         : var / (S(1) - dir.z * dir.z);
+    b.cov[tri6(3, 3)] += var;
+    return true;
+}
+
+// estimate_external_mask_tolerance (noise_estimation.hpp:22-107)
+template <typename S>
+DPROP_HD void estimate_external_tol(nav_state<S>& nav, const bound_state<S>& b,
+                                    const step_state<S>& st,
+                                    const actor_cfg<S>& cfg, S q) {
+    const S n = cfg.n_stddev;
+    const S var0 = b.cov[tri6(0, 0)];
+    const S var1 = b.cov[tri6(1, 1)];
+    const S dphi = n * sqrt(b.cov[tri6(2, 2)]);
+    const S dth = n * sqrt(b.cov[tri6(3, 3)]);
+    const S phi_err = b.v[2] + dphi;
+    const S th_err = b.v[3] + dth;
+    const S ste = sin(th_err);
+    vec3<S> displ{cos(phi_err) * ste, sin(phi_err) * ste, cos(th_err)};
+    const S max_tol = S(5);
+    const S path = nav.cache_exhausted() ? max_tol : fabs(nav.target().path);
+    displ = path * (displ - st.dir);
+    const S p = q / st.qop;
+    const S noise = S(1) / p * cfg.accumulated_error *
+                    static_cast<S>(st.path_length);
+    const S ext = sqrt(n * n * (var0 + var1) + dot(displ, displ) + noise * noise);
+    nav.external_tol = ext > max_tol ? max_tol : ext;
+}
+
+}  // namespace dprop

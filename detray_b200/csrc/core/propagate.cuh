@@ -1,0 +1,284 @@
+// The propagation loop for one track: actors, navigation update and RK
+// stepping in the reference's alternating order A N S N A N S N ...
+//
+// Reference: propagator::propagate, core/include/detray/propagator/
+// propagator.hpp:260-400, with the actor chain of the device tests
+// (tests/include/detray/test/device/propagator_test.hpp:84-93):
+//   pathlimit_aborter -> parameter_updater<pointwise_material_interactor>
+// followed by a surface recorder, and the stepper policy
+// stepper_rk_policy (navigation/policies.hpp:98-139).
+#pragma once
+
+#include "actors.cuh"
+
+namespace dprop {
+
+template <typename S>
+struct prop_cfg {
+    step_cfg<S> step;
+    nav_cfg<S> nav;
+    actor_cfg<S> act;
+    S step_constraint;      // stepping::config::step_constraint (accuracy)
+    bool record_all;
+    uint32_t max_records;
+    uint32_t max_iterations;
+};
+
+// Where a track writes its records: slot-major arrays, index k * n + t.
+template <typename S>
+struct record_sink {
+    uint64_t* barcode;
+    S* bound[6];
+    S* cov[21];
+    S* path;
+    uint8_t* flags;
+    uint64_t n_tracks;
+    uint64_t track;
+    uint32_t capacity;
+    uint32_t count;
+
+    DPROP_HD void write(uint64_t bc, const S* b, const S* c, S p, uint8_t fl) {
+        if (count < capacity) {
+            const uint64_t o = static_cast<uint64_t>(count) * n_tracks + track;
+            barcode[o] = bc;
+            if (fl & 1u) {
+                for (int i = 0; i < 6; ++i) {
+                    if (bound[i]) {
+                        bound[i][o] = b[i];
+                    }
+                }
+                for (int i = 0; i < 21; ++i) {
+                    if (cov[i]) {
+                        cov[i][o] = c[i];
+                    }
+                }
+            }
+            if (path) {
+                path[o] = p;
+            }
+            if (flags) {
+                flags[o] = fl;
+            }
+        }
+        ++count;
+    }
+};
+
+// All per-track state of one propagation flow
+template <typename S>
+struct track_state {
+    step_state<S> step;
+    nav_state<S> nav;
+    bound_state<S> bound;
+    S q;        // particle charge (sign of q/p)
+    bool heartbeat;
+};
+
+template <typename S>
+DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
+                               vec3<S> dir, S qop, const prop_cfg<S>& cfg) {
+    step_state<S>& st = ts.step;
+    st.pos = pos;
+    st.dir = dir;
+    st.qop = qop;
+    st.time = time;
+    st.path_length = 0.;
+    st.abs_path_length = 0.;
+    st.step_size = S(0);
+    st.next_step_size = S(0);
+    st.dtds = {S(0), S(0), S(0)};
+    st.dqopds = S(0);
+    st.constraint = min_(limits<S>::max(), fabs(cfg.step_constraint));
+    st.jac.reset();
+    st.n_trials = 0u;
+    st.n_steps = 0u;
+    ts.nav.reset(0u);
+    for (int i = 0; i < 6; ++i) {
+        ts.bound.v[i] = S(0);
+    }
+    for (int i = 0; i < 21; ++i) {
+        ts.bound.cov[i] = S(0);
+    }
+    ts.bound.sf = k_invalid;
+    // particle hypothesis with the charge sign of the track
+    ts.q = (qop < S(0)) ? S(-1) : S(1);
+    ts.heartbeat = false;
+}
+
+// Run the actor chain once (propagator.hpp:308).
+template <typename S>
+DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
+                         const field_view<S>& field, const prop_cfg<S>& cfg,
+                         record_sink<S>& rec) {
+    step_state<S>& st = ts.step;
+    nav_state<S>& nav = ts.nav;
+
+    // pathlimit_aborter
+    if (!nav.finished()) {
+        const S step_limit =
+            cfg.act.path_limit - static_cast<S>(fabs(st.abs_path_length));
+        if (step_limit <= S(0)) {
+            nav.abort(e_reason_path_limit);
+            ts.heartbeat = false;
+        }
+        st.constraint = min_(st.constraint, fabs(step_limit));
+    }
+
+    // parameter_transporter and its observers
+    if (!nav.is_on_surface()) {
+        return;
+    }
+    const uint32_t cur_sf = nav.current().sf;
+    const dev_surface dst = det.surfaces[cur_sf];
+    const bool on_sensitive =
+        nav.status == e_on_object && dst.kind == e_sensitive;
+    const bool has_material = dst.material != k_invalid;
+    const bool transported = on_sensitive || has_material;
+    if (transported) {
+        bound_state<S>& b = ts.bound;
+        bool update_vector = true;
+        if (b.sf != k_invalid) {
+            if (b.sf == cur_sf) {
+                update_vector = false;  // already on the departure surface
+            } else {
+                const dev_surface dep = det.surfaces[b.sf];
+                S G[4][5];
+                full_jacobian(det, b, dep, dst, st, current_dtds(st, field), G);
+                if (fabs(st.path_length) > 0.) {
+                    st.jac.reset();
+                }
+                transport_covariance(G, b.cov);
+            }
+        } else {
+            for (int i = 0; i < 21; ++i) {
+                b.cov[i] = S(0);
+            }
+            for (int i = 0; i < 6; ++i) {
+                b.cov[tri6(i, i)] = S(1);
+            }
+        }
+        if (update_vector) {
+            free_to_bound(det, dst, st, b.v);
+            b.sf = cur_sf;
+        }
+        // pointwise_material_interactor
+        bool success = false;
+        if (cfg.act.use_interactor && has_material) {
+            success = interact(det, dst, b, cfg.act, ts.q, nav.direction);
+        }
+        // parameter_setter
+        if (success) {
+            const vec3<S> d = bound_dir(b.v[2], b.v[3]);
+            st.pos = bound_to_free_pos(det, dst, b.v[0], b.v[1]);
+            st.time = b.v[5];
+            st.dir = d;
+            st.qop = b.v[4];
+            if (cfg.act.estimate_noise) {
+                estimate_external_tol(nav, b, st, cfg.act, ts.q);
+            }
+        }
+    }
+    // surface recorder
+    if (transported || cfg.record_all) {
+        uint8_t fl = 0u;
+        if (transported && ts.bound.sf == cur_sf) {
+            fl |= 1u;
+        }
+        if (dst.kind == e_portal) {
+            fl |= 2u;
+        }
+        if (has_material) {
+            fl |= 4u;
+        }
+        rec.write(dst.barcode, ts.bound.v, ts.bound.cov,
+                  static_cast<S>(st.path_length), fl);
+    }
+}
+
+// stepper_rk_policy: downgrade the navigation trust after a step
+template <typename S>
+DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
+    const S d = nav.dist();
+    if (fabs(d) <= S(unit::um)) {
+        nav.set_high_trust();
+        return;
+    }
+    const S rel = (st.step_size - d) / d;
+    if (rel > S(0.1)) {
+        nav.set_no_trust();
+    } else if (rel > S(0.05)) {
+        nav.set_fair_trust();
+    } else {
+        nav.set_high_trust();
+    }
+}
+
+// Propagate one track to the end; returns a dprop_track_status code.
+template <typename S>
+DPROP_HD uint8_t propagate_track(track_state<S>& ts,
+                                 const detector_view<S>& det,
+                                 const field_view<S>& field,
+                                 const prop_cfg<S>& cfg, record_sink<S>& rec) {
+    step_state<S>& st = ts.step;
+    nav_state<S>& nav = ts.nav;
+
+    navigator_init(nav, det, track_view<S>{st.pos, st.dir}, cfg.nav);
+    ts.heartbeat = nav.is_alive();
+    bool is_init = true;
+    double path_prev = 0.;
+    uint32_t stall = 0u;
+    uint32_t i = 0u;
+    bool out_of_budget = false;
+    for (; (i % 2u == 0u) || ts.heartbeat; ++i) {
+        if (i >= cfg.max_iterations) {
+            out_of_budget = true;
+            break;
+        }
+        if (i % 2u == 0u) {
+            run_actors(ts, det, field, cfg, rec);
+            if (!ts.heartbeat) {
+                continue;
+            }
+            path_prev = st.path_length;
+        } else {
+            const bool reset = nav.is_on_surface() || is_init;
+            ts.heartbeat =
+                ts.heartbeat && rk_step(st, nav.dist(), cfg.step, reset, field);
+            rk_policy(nav, st);
+            if (i > 0u) {
+                is_init = false;
+            }
+            if (fabs(st.path_length) <=
+                fabs(path_prev) + static_cast<double>(cfg.nav.isect.path_tol)) {
+                if (stall >= 10u) {
+                    ts.heartbeat = false;
+                    nav.abort(e_reason_stalled);
+                }
+                ++stall;
+            } else {
+                stall = 0u;
+            }
+        }
+        is_init = navigator_update(nav, det, track_view<S>{st.pos, st.dir},
+                                   cfg.nav) ||
+                  is_init;
+        ts.heartbeat = ts.heartbeat && nav.is_alive();
+    }
+    if (out_of_budget) {
+        return 4u;  // DPROP_TRK_MAX_ITER
+    }
+    const bool paused = !ts.heartbeat && nav.is_alive();
+    if (nav.finished() || paused) {
+        return 0u;  // DPROP_TRK_EXITED
+    }
+    switch (nav.reason) {
+        case e_reason_path_limit:
+            return 1u;
+        case e_reason_stalled:
+            return 2u;
+        default:
+            return 3u;
+    }
+}
+
+}  // namespace dprop

@@ -1,0 +1,604 @@
+// C ABI of the B200 track propagator (include/detray_b200/dprop.h) and the
+// propagation kernels.
+//
+// Kernels:
+//   propagate_plain_kernel       one thread per track, the whole propagation;
+//                                the same launch form as the reference's
+//                                propagator_benchmark_kernel
+//                                (tests/benchmarks/include/detray/benchmarks/
+//                                device/cuda/propagation_benchmark.cu:13-68)
+//   propagate_persistent_kernel  a grid sized to the SMs whose threads pull
+//                                track indices from a device work queue until
+//                                it is empty, so lanes freed by short tracks
+//                                are refilled while loopers run on.
+// Both write the slot-major records of dprop_results.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "core/config.hpp"
+#include "core/convert.hpp"
+#include "core/propagate.cuh"
+#include "detray_b200/dprop.h"
+
+using namespace dprop;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+dprop_status fail(dprop_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+dprop_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? DPROP_E_OOM : DPROP_E_CUDA;
+}
+
+#define DPROP_CUDA(call)                              \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) {                      \
+            return cuda_fail(e_, #call);              \
+        }                                             \
+    } while (0)
+
+template <typename T>
+dprop_status upload(const std::vector<T>& h, T** d) {
+    *d = nullptr;
+    if (h.empty()) {
+        return DPROP_OK;
+    }
+    DPROP_CUDA(cudaMalloc(reinterpret_cast<void**>(d), h.size() * sizeof(T)));
+    DPROP_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T),
+                          cudaMemcpyHostToDevice));
+    return DPROP_OK;
+}
+
+}  // namespace
+
+struct dprop_detector {
+    int device{0};
+    dev_volume* volumes{nullptr};
+    dev_surface* surfaces{nullptr};
+    dev_mask<float>* masks{nullptr};
+    dev_transform<float>* transforms{nullptr};
+    dev_slab<float>* slabs{nullptr};
+    uint32_t* bf_surfaces{nullptr};
+    dev_grid<float>* grids{nullptr};
+    uint32_t* grid_bins{nullptr};
+    uint32_t n_volumes{0}, n_surfaces{0};
+    detector_view<float> view() const {
+        detector_view<float> v;
+        v.volumes = volumes;
+        v.surfaces = surfaces;
+        v.masks = masks;
+        v.transforms = transforms;
+        v.slabs = slabs;
+        v.bf_surfaces = bf_surfaces;
+        v.grids = grids;
+        v.grid_bins = grid_bins;
+        v.n_volumes = n_volumes;
+        v.n_surfaces = n_surfaces;
+        return v;
+    }
+};
+
+struct dprop_field {
+    int device{0};
+    float4* nodes{nullptr};
+    field_view<float> view{};
+};
+
+namespace {
+
+// Device scratch owned by the library for the host-buffer entry point:
+// grow-only, reused across calls (not thread-safe across host threads).
+struct host_path_scratch {
+    void* buf{nullptr};
+    size_t bytes{0};
+    unsigned int* counter{nullptr};
+};
+host_path_scratch g_scratch;
+
+dprop_status ensure_scratch(size_t bytes) {
+    if (g_scratch.bytes >= bytes) {
+        return DPROP_OK;
+    }
+    if (g_scratch.buf) {
+        cudaFree(g_scratch.buf);
+        g_scratch.buf = nullptr;
+        g_scratch.bytes = 0;
+    }
+    DPROP_CUDA(cudaMalloc(&g_scratch.buf, bytes));
+    g_scratch.bytes = bytes;
+    return DPROP_OK;
+}
+
+unsigned int* g_queue_counter = nullptr;
+
+// Device pointers of the inputs/outputs, by value into the kernels
+template <typename In>
+struct io_ptrs {
+    const In* trk[8];
+    uint8_t* status;
+    uint32_t* n_records;
+    uint32_t* n_steps;
+    uint32_t* n_trials;
+    float* path_length;
+    float* final_free[8];
+    uint64_t* rec_barcode;
+    float* rec_bound[6];
+    float* rec_cov[21];
+    float* rec_path;
+    uint8_t* rec_flags;
+};
+
+template <typename In>
+io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
+    io_ptrs<In> io{};
+    for (int i = 0; i < 3; ++i) {
+        io.trk[i] = static_cast<const In*>(t.pos[i]);
+        io.trk[4 + i] = static_cast<const In*>(t.dir[i]);
+    }
+    io.trk[3] = static_cast<const In*>(t.time);
+    io.trk[7] = static_cast<const In*>(t.qop);
+    io.status = r.status;
+    io.n_records = r.n_records;
+    io.n_steps = r.n_steps;
+    io.n_trials = r.n_trials;
+    io.path_length = static_cast<float*>(r.path_length);
+    for (int i = 0; i < 8; ++i) {
+        io.final_free[i] = static_cast<float*>(r.final_free[i]);
+    }
+    io.rec_barcode = r.rec_barcode;
+    for (int i = 0; i < 6; ++i) {
+        io.rec_bound[i] = static_cast<float*>(r.rec_bound[i]);
+    }
+    for (int i = 0; i < 21; ++i) {
+        io.rec_cov[i] = static_cast<float*>(r.rec_cov[i]);
+    }
+    io.rec_path = static_cast<float*>(r.rec_path);
+    io.rec_flags = r.rec_flags;
+    return io;
+}
+
+template <typename In>
+__device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
+                                        const detector_view<float>& det,
+                                        const field_view<float>& field,
+                                        const prop_cfg<float>& cfg,
+                                        const io_ptrs<In>& io) {
+    const vec3<float> pos{static_cast<float>(io.trk[0][t]),
+                          static_cast<float>(io.trk[1][t]),
+                          static_cast<float>(io.trk[2][t])};
+    const vec3<float> dir{static_cast<float>(io.trk[4][t]),
+                          static_cast<float>(io.trk[5][t]),
+                          static_cast<float>(io.trk[6][t])};
+    const float time = static_cast<float>(io.trk[3][t]);
+    const float qop = static_cast<float>(io.trk[7][t]);
+
+    track_state<float> ts;
+    init_track_state(ts, pos, time, dir, qop, cfg);
+
+    record_sink<float> rec;
+    rec.barcode = io.rec_barcode;
+    for (int i = 0; i < 6; ++i) {
+        rec.bound[i] = io.rec_bound[i];
+    }
+    for (int i = 0; i < 21; ++i) {
+        rec.cov[i] = io.rec_cov[i];
+    }
+    rec.path = io.rec_path;
+    rec.flags = io.rec_flags;
+    rec.n_tracks = n;
+    rec.track = t;
+    rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
+    rec.count = 0u;
+
+    const uint8_t status = propagate_track(ts, det, field, cfg, rec);
+
+    if (io.status) io.status[t] = status;
+    if (io.n_records) io.n_records[t] = rec.count;
+    if (io.n_steps) io.n_steps[t] = ts.step.n_steps;
+    if (io.n_trials) io.n_trials[t] = ts.step.n_trials;
+    if (io.path_length) io.path_length[t] = static_cast<float>(ts.step.path_length);
+    const float fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
+                          ts.step.time,  ts.step.dir.x, ts.step.dir.y,
+                          ts.step.dir.z, ts.step.qop};
+    for (int i = 0; i < 8; ++i) {
+        if (io.final_free[i]) io.final_free[i][t] = fin[i];
+    }
+}
+
+constexpr int k_plain_block = 128;
+
+template <typename In>
+__global__ void __launch_bounds__(k_plain_block)
+    propagate_plain_kernel(const detector_view<float> det,
+                           const field_view<float> field,
+                           const prop_cfg<float> cfg, const io_ptrs<In> io,
+                           uint64_t n) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) {
+        return;
+    }
+    run_one(t, n, det, field, cfg, io);
+}
+
+template <typename In>
+__global__ void __launch_bounds__(k_plain_block)
+    propagate_persistent_kernel(const detector_view<float> det,
+                                const field_view<float> field,
+                                const prop_cfg<float> cfg, const io_ptrs<In> io,
+                                uint64_t n, unsigned int* queue) {
+    // each thread pulls the next unprocessed track until the queue is empty
+    while (true) {
+        const unsigned int t = atomicAdd(queue, 1u);
+        if (t >= n) {
+            break;
+        }
+        run_one(static_cast<uint64_t>(t), n, det, field, cfg, io);
+    }
+}
+
+template <typename In>
+dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
+                    const dprop_detector* det, const dprop_field* field,
+                    const io_ptrs<In>& io, uint64_t n, cudaStream_t stream) {
+    if (n == 0) {
+        return DPROP_OK;
+    }
+    const prop_cfg<float> cfg = make_prop_cfg<float>(c);
+    const uint32_t method = launch_cfg ? launch_cfg->method : DPROP_METHOD_PLAIN;
+    if (method == DPROP_METHOD_PERSISTENT) {
+        if (n > 0xffffff00ull) {
+            return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
+        }
+        if (!g_queue_counter) {
+            DPROP_CUDA(cudaMalloc(&g_queue_counter, sizeof(unsigned int)));
+        }
+        DPROP_CUDA(cudaMemsetAsync(g_queue_counter, 0, sizeof(unsigned int),
+                                   stream));
+        int dev = 0, sms = 0;
+        DPROP_CUDA(cudaGetDevice(&dev));
+        DPROP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        uint32_t per_sm = (launch_cfg && launch_cfg->ctas_per_sm)
+                              ? launch_cfg->ctas_per_sm
+                              : 8u;
+        uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+        const uint64_t need = (n + k_plain_block - 1) / k_plain_block;
+        if (grid > need) {
+            grid = need;
+        }
+        propagate_persistent_kernel<In><<<static_cast<unsigned int>(grid),
+                                          k_plain_block, 0, stream>>>(
+            det->view(), field->view, cfg, io, n, g_queue_counter);
+    } else {
+        const uint64_t grid = (n + k_plain_block - 1) / k_plain_block;
+        propagate_plain_kernel<In><<<static_cast<unsigned int>(grid),
+                                     k_plain_block, 0, stream>>>(
+            det->view(), field->view, cfg, io, n);
+    }
+    DPROP_CUDA(cudaGetLastError());
+    return DPROP_OK;
+}
+
+dprop_status check_config(const dprop_config* cfg) {
+    if (!cfg) {
+        return fail(DPROP_E_INVALID, "config is NULL");
+    }
+    if (cfg->use_field_gradient) {
+        return fail(DPROP_E_UNSUPPORTED,
+                    "use_field_gradient is not supported on the device path");
+    }
+    if (cfg->use_eloss_gradient) {
+        return fail(DPROP_E_UNSUPPORTED,
+                    "use_eloss_gradient needs volume material, which the "
+                    "device path does not support");
+    }
+    if (cfg->max_iterations == 0u) {
+        return fail(DPROP_E_INVALID, "max_iterations must be > 0");
+    }
+    return DPROP_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+uint32_t dprop_abi_version(void) { return DPROP_ABI_VERSION; }
+
+const char* dprop_last_error(void) { return g_last_error.c_str(); }
+
+void dprop_config_default(dprop_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->min_stepsize = 1e-4f;
+    c->rk_error_tol = 1e-4f;
+    c->step_constraint = FLT_MAX;
+    c->path_limit = 5000.f;
+    c->max_rk_updates = 10000u;
+    c->use_mean_loss = 1;
+    c->use_eloss_gradient = 0;
+    c->use_field_gradient = 0;
+    c->do_covariance_transport = 1;
+    c->min_mask_tolerance = 1e-5f;
+    c->max_mask_tolerance = 3.f;
+    c->mask_tolerance_scalor = 5e-2f;
+    c->path_tolerance = 1e-3f;
+    c->overstep_tolerance = -1.f;
+    c->search_window[0] = 0u;
+    c->search_window[1] = 0u;
+    c->accumulated_error = 0.001f;
+    c->n_scattering_stddev = 3;
+    c->estimate_scattering_noise = 1;
+    c->use_path_limit_aborter = 1;
+    c->use_material_interactor = 1;
+    c->record_all_surfaces = 0;
+    c->mass = 0.1056583755f;
+    c->pdg = 13;
+    c->max_records = 32u;
+    c->max_iterations = 200000u;
+}
+
+dprop_status dprop_detector_create(const dprop_detector_desc* d, int device,
+                                   dprop_detector** out) {
+    if (!d || !out) {
+        return fail(DPROP_E_INVALID, "detector_create: NULL argument");
+    }
+    *out = nullptr;
+    const std::string problem = validate_desc(d);
+    if (!problem.empty()) {
+        const bool unsupported = problem.find("not supported") != std::string::npos;
+        return fail(unsupported ? DPROP_E_UNSUPPORTED : DPROP_E_INVALID,
+                    "detector_create: " + problem);
+    }
+    const host_tables<float> t = convert_desc<float>(d);
+    DPROP_CUDA(cudaSetDevice(device));
+    auto* det = new dprop_detector();
+    det->device = device;
+    det->n_volumes = d->n_volumes;
+    det->n_surfaces = d->n_surfaces;
+    dprop_status st = DPROP_OK;
+    if ((st = upload(t.volumes, &det->volumes)) != DPROP_OK ||
+        (st = upload(t.surfaces, &det->surfaces)) != DPROP_OK ||
+        (st = upload(t.masks, &det->masks)) != DPROP_OK ||
+        (st = upload(t.transforms, &det->transforms)) != DPROP_OK ||
+        (st = upload(t.slabs, &det->slabs)) != DPROP_OK ||
+        (st = upload(t.bf_surfaces, &det->bf_surfaces)) != DPROP_OK ||
+        (st = upload(t.grids, &det->grids)) != DPROP_OK ||
+        (st = upload(t.grid_bins, &det->grid_bins)) != DPROP_OK) {
+        dprop_detector_destroy(det);
+        return st;
+    }
+    *out = det;
+    return DPROP_OK;
+}
+
+dprop_status dprop_detector_destroy(dprop_detector* det) {
+    if (!det) {
+        return DPROP_OK;
+    }
+    cudaFree(det->volumes);
+    cudaFree(det->surfaces);
+    cudaFree(det->masks);
+    cudaFree(det->transforms);
+    cudaFree(det->slabs);
+    cudaFree(det->bf_surfaces);
+    cudaFree(det->grids);
+    cudaFree(det->grid_bins);
+    delete det;
+    return DPROP_OK;
+}
+
+dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
+                                 uint32_t* n_surfaces) {
+    if (!det) {
+        return fail(DPROP_E_INVALID, "detector_info: NULL detector");
+    }
+    if (n_volumes) *n_volumes = det->n_volumes;
+    if (n_surfaces) *n_surfaces = det->n_surfaces;
+    return DPROP_OK;
+}
+
+dprop_status dprop_field_create_const(double bx, double by, double bz,
+                                      int device, dprop_field** out) {
+    if (!out) {
+        return fail(DPROP_E_INVALID, "field_create_const: NULL out");
+    }
+    auto* f = new dprop_field();
+    f->device = device;
+    f->view.kind = 0u;
+    f->view.n_r = f->view.n_phi = f->view.n_z = 1u;
+    f->view.b[0] = static_cast<float>(bx);
+    f->view.b[1] = static_cast<float>(by);
+    f->view.b[2] = static_cast<float>(bz);
+    f->view.nodes = nullptr;
+    *out = f;
+    return DPROP_OK;
+}
+
+dprop_status dprop_field_create_grid(const double* lo, const double* hi,
+                                     const uint32_t* n, const float* values,
+                                     int device, dprop_field** out) {
+    if (!lo || !hi || !n || !values || !out) {
+        return fail(DPROP_E_INVALID, "field_create_grid: NULL argument");
+    }
+    if (n[0] == 0 || n[1] == 0 || n[2] == 0 || (n[0] > 1 && !(hi[0] > lo[0])) ||
+        (n[2] > 1 && !(hi[2] > lo[2]))) {
+        return fail(DPROP_E_INVALID, "field_create_grid: bad axes");
+    }
+    const uint64_t nodes = static_cast<uint64_t>(n[0]) * n[1] * n[2];
+    std::vector<float4> h(nodes);
+    for (uint64_t i = 0; i < nodes; ++i) {
+        h[i] = make_float4(values[3 * i], values[3 * i + 1], values[3 * i + 2], 0.f);
+    }
+    DPROP_CUDA(cudaSetDevice(device));
+    auto* f = new dprop_field();
+    f->device = device;
+    dprop_status st = upload(h, &f->nodes);
+    if (st != DPROP_OK) {
+        delete f;
+        return st;
+    }
+    field_view<float>& v = f->view;
+    v.kind = 1u;
+    v.n_r = n[0];
+    v.n_phi = n[1];
+    v.n_z = n[2];
+    v.b[0] = v.b[1] = v.b[2] = 0.f;
+    v.r_lo = static_cast<float>(lo[0]);
+    v.r_step_inv = n[0] > 1 ? static_cast<float>((n[0] - 1) / (hi[0] - lo[0])) : 0.f;
+    v.phi_lo = static_cast<float>(lo[1]);
+    v.phi_step_inv = static_cast<float>(n[1] / (2.0 * constant::pi));
+    v.z_lo = static_cast<float>(lo[2]);
+    v.z_step_inv = n[2] > 1 ? static_cast<float>((n[2] - 1) / (hi[2] - lo[2])) : 0.f;
+    v.nodes = f->nodes;
+    *out = f;
+    return DPROP_OK;
+}
+
+dprop_status dprop_field_destroy(dprop_field* f) {
+    if (!f) {
+        return DPROP_OK;
+    }
+    cudaFree(f->nodes);
+    delete f;
+    return DPROP_OK;
+}
+
+dprop_status dprop_propagate(const dprop_config* cfg, const dprop_launch* lc,
+                             const dprop_detector* det, const dprop_field* field,
+                             const dprop_tracks* tracks,
+                             const dprop_results* results, uint64_t n,
+                             void* stream) {
+    dprop_status s = check_config(cfg);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    if (!det || !field || !tracks || !results) {
+        return fail(DPROP_E_INVALID, "propagate: NULL argument");
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (!tracks->pos[i] || !tracks->dir[i]) {
+            return fail(DPROP_E_INVALID, "propagate: missing track array");
+        }
+    }
+    if (!tracks->time || !tracks->qop || !results->status) {
+        return fail(DPROP_E_INVALID, "propagate: missing track/status array");
+    }
+    const io_ptrs<float> io = make_io<float>(*tracks, *results);
+    return launch<float>(*cfg, lc, det, field, io, n,
+                         static_cast<cudaStream_t>(stream));
+}
+
+dprop_status dprop_propagate_host(const dprop_config* cfg,
+                                  const dprop_launch* lc,
+                                  const dprop_detector* det,
+                                  const dprop_field* field,
+                                  const dprop_tracks* tracks,
+                                  const dprop_results* results, uint64_t n) {
+    dprop_status s = check_config(cfg);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    if (!det || !field || !tracks || !results || !results->status) {
+        return fail(DPROP_E_INVALID, "propagate_host: NULL argument");
+    }
+    if (n == 0) {
+        return DPROP_OK;
+    }
+    const uint64_t cap = cfg->max_records;
+    // device scratch: inputs (8 doubles), per-track outputs, records
+    const size_t in_bytes = 8 * n * sizeof(double);
+    const size_t trk_bytes = n * (1 + 3 * 4 + 4 + 8 * 4);
+    const size_t rec_bytes = cap * n * (8 + 6 * 4 + 21 * 4 + 4 + 1);
+    s = ensure_scratch(in_bytes + trk_bytes + rec_bytes + 4096);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    char* p = static_cast<char*>(g_scratch.buf);
+    auto take = [&](size_t bytes) {
+        char* r = p;
+        p += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    const double* d_trk[8];
+    for (int i = 0; i < 8; ++i) {
+        d_trk[i] = reinterpret_cast<const double*>(take(n * sizeof(double)));
+    }
+    const void* h_trk[8] = {tracks->pos[0], tracks->pos[1], tracks->pos[2],
+                            tracks->time,   tracks->dir[0], tracks->dir[1],
+                            tracks->dir[2], tracks->qop};
+    for (int i = 0; i < 8; ++i) {
+        if (!h_trk[i]) {
+            return fail(DPROP_E_INVALID, "propagate_host: missing track array");
+        }
+        DPROP_CUDA(cudaMemcpyAsync(const_cast<double*>(d_trk[i]), h_trk[i],
+                                   n * sizeof(double), cudaMemcpyHostToDevice, 0));
+    }
+    dprop_results dr{};
+    dr.status = reinterpret_cast<uint8_t*>(take(n));
+    dr.n_records = results->n_records ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
+    dr.n_steps = results->n_steps ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
+    dr.n_trials = results->n_trials ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
+    dr.path_length = results->path_length ? take(4 * n) : nullptr;
+    for (int i = 0; i < 8; ++i) {
+        dr.final_free[i] = results->final_free[i] ? take(4 * n) : nullptr;
+    }
+    dr.rec_barcode = results->rec_barcode ? reinterpret_cast<uint64_t*>(take(8 * cap * n)) : nullptr;
+    for (int i = 0; i < 6; ++i) {
+        dr.rec_bound[i] = results->rec_bound[i] ? take(4 * cap * n) : nullptr;
+    }
+    for (int i = 0; i < 21; ++i) {
+        dr.rec_cov[i] = results->rec_cov[i] ? take(4 * cap * n) : nullptr;
+    }
+    dr.rec_path = results->rec_path ? take(4 * cap * n) : nullptr;
+    dr.rec_flags = results->rec_flags ? reinterpret_cast<uint8_t*>(take(cap * n)) : nullptr;
+
+    dprop_tracks dt{};
+    for (int i = 0; i < 3; ++i) {
+        dt.pos[i] = d_trk[i];
+        dt.dir[i] = d_trk[4 + i];
+    }
+    dt.time = d_trk[3];
+    dt.qop = d_trk[7];
+    const io_ptrs<double> io = make_io<double>(dt, dr);
+    s = launch<double>(*cfg, lc, det, field, io, n, 0);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    auto d2h = [&](void* h, const void* d, size_t bytes) -> dprop_status {
+        if (h && d) {
+            DPROP_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, 0));
+        }
+        return DPROP_OK;
+    };
+    if ((s = d2h(results->status, dr.status, n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_records, dr.n_records, 4 * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_steps, dr.n_steps, 4 * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_trials, dr.n_trials, 4 * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->path_length, dr.path_length, 4 * n)) != DPROP_OK) return s;
+    for (int i = 0; i < 8; ++i) {
+        if ((s = d2h(results->final_free[i], dr.final_free[i], 4 * n)) != DPROP_OK) return s;
+    }
+    if ((s = d2h(results->rec_barcode, dr.rec_barcode, 8 * cap * n)) != DPROP_OK) return s;
+    for (int i = 0; i < 6; ++i) {
+        if ((s = d2h(results->rec_bound[i], dr.rec_bound[i], 4 * cap * n)) != DPROP_OK) return s;
+    }
+    for (int i = 0; i < 21; ++i) {
+        if ((s = d2h(results->rec_cov[i], dr.rec_cov[i], 4 * cap * n)) != DPROP_OK) return s;
+    }
+    if ((s = d2h(results->rec_path, dr.rec_path, 4 * cap * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->rec_flags, dr.rec_flags, cap * n)) != DPROP_OK) return s;
+    DPROP_CUDA(cudaStreamSynchronize(0));
+    return DPROP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,328 @@
+/*
+ * detray-b200 C ABI: batched charged-track propagation on one B200.
+ *
+ * This header is the whole drop-in boundary.  It replaces the device side of
+ * detray's track propagation, which in the reference is reached through
+ *
+ *   (i)   detray::get_buffer(det, dev_mr, copy) / detray::get_data(buffer)
+ *         core/include/detray/core/detail/container_buffers.hpp:82-195
+ *         -> here: dprop_detector_create() from flattened tables;
+ *   (ii)  a covfie field view handed to the stepper
+ *         tests/include/detray/test/common/bfield.hpp:35-47 (host),
+ *         tests/include/detray/test/device/cuda/bfield.hpp:28-32 (device)
+ *         -> here: dprop_field_create_const() / dprop_field_create_grid();
+ *   (iii) the batch launcher run_propagation_kernel<propagator_t>(cfg,
+ *         det_view, field_view, actor_states, tracks, n)
+ *         tests/benchmarks/include/detray/benchmarks/device/cuda/
+ *         propagation_benchmark.hpp:83-93 and propagation_benchmark.cu:96-118
+ *         -> here: dprop_propagate() (device buffers, stream ordered) and
+ *            dprop_propagate_host() (host buffers, copies included).
+ *
+ * The actor chain is the one the reference's device tests compose
+ * (tests/include/detray/test/device/propagator_test.hpp:84-93):
+ *   pathlimit_aborter -> parameter_updater< pointwise_material_interactor >
+ * with the run-time switches of propagation::config
+ * (core/include/detray/propagator/propagation_config.hpp:22-40) mirrored in
+ * dprop_config.
+ *
+ * Conventions: plain C types only, no exceptions cross this boundary, every
+ * function returns a dprop_status; dprop_last_error() gives the message of
+ * the last failure on the calling thread.  Units are detray's: mm, GeV, T
+ * expressed in detray's internal unit system (1 T = 0.000299792458 GeV/mm/e).
+ */
+#ifndef DETRAY_B200_DPROP_H
+#define DETRAY_B200_DPROP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPROP_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------ status */
+typedef enum dprop_status {
+    DPROP_OK = 0,
+    DPROP_E_INVALID = 1,   /* bad argument or inconsistent tables          */
+    DPROP_E_CUDA = 2,      /* a CUDA runtime call failed                   */
+    DPROP_E_NO_DEVICE = 3, /* no usable sm_100 device                      */
+    DPROP_E_OOM = 4,       /* device allocation failed                     */
+    DPROP_E_TIMEOUT = 5,   /* a bounded device wait ran out                */
+    DPROP_E_UNSUPPORTED = 6
+} dprop_status;
+
+/* Per-track outcome, written to dprop_results.status.  Mirrors the
+ * navigation status reached at the end of propagator::propagate
+ * (core/include/detray/propagator/propagator.hpp:389-399) and the abort
+ * reasons of the reference (navigation_state.hpp:414-433, aborters.hpp:62-70,
+ * propagator.hpp:349-373, navigation_functions.hpp:327-330). */
+typedef enum dprop_track_status {
+    DPROP_TRK_EXITED = 0,        /* left the world: propagate() returned true */
+    DPROP_TRK_PATH_LIMIT = 1,    /* pathlimit_aborter fired                   */
+    DPROP_TRK_STALLED = 2,       /* > 10 non-advancing steps                  */
+    DPROP_TRK_NO_SURFACE = 3,    /* loose re-initialisation found nothing     */
+    DPROP_TRK_MAX_ITER = 4,      /* device iteration budget exhausted         */
+    DPROP_TRK_NOT_RUN = 5,       /* never started (e.g. invalid input)        */
+    DPROP_TRK_NONFINITE = 6      /* state became NaN/inf                      */
+} dprop_track_status;
+
+/* --------------------------------------------------------- detector tables
+ * The flattened form of detray::detector<metadata> (core/detector.hpp:57-355).
+ * All indices are 0-based positions in the arrays below.  Tables are given
+ * in double precision on the host; the library stores its own device copy. */
+
+/* Mask shapes on the path (geometry/shapes/*.hpp). */
+typedef enum dprop_shape {
+    DPROP_SHAPE_RECTANGLE = 0,     /* rectangle2D: v0 half_x, v1 half_y                 */
+    DPROP_SHAPE_TRAPEZOID = 1,     /* trapezoid2D: v0 hl_x(-y), v1 hl_x(+y), v2 hl_y, v3 1/(2 hl_y) */
+    DPROP_SHAPE_RING = 2,          /* ring2D: v0 inner_r, v1 outer_r                    */
+    DPROP_SHAPE_CYLINDER = 3,      /* cylinder2D: v0 r, v1 lower_z, v2 upper_z          */
+    DPROP_SHAPE_CONCENTRIC_CYL = 4,/* concentric_cylinder2D: v0 r, v1 lower_z, v2 upper_z */
+    DPROP_SHAPE_LINE = 5,          /* line (straw/wire cell): v0 cell r, v1 half_z, v2 square(1)/radial(0) */
+    DPROP_SHAPE_COUNT = 6
+} dprop_shape;
+
+/* Surface categories, same values as detray::surface_id
+ * (core/include/detray/definitions/geometry.hpp:40-46). */
+typedef enum dprop_surface_kind {
+    DPROP_SF_PORTAL = 0,
+    DPROP_SF_SENSITIVE = 1,
+    DPROP_SF_PASSIVE = 2
+} dprop_surface_kind;
+
+#define DPROP_INVALID_INDEX 0xffffffffu
+#define DPROP_INVALID_LINK 0xffffu
+
+typedef struct dprop_surface_desc {
+    uint64_t barcode;       /* geometry::identifier value (identifier.hpp:153-157) */
+    uint32_t mask_begin;    /* [mask_begin, mask_end) into masks                   */
+    uint32_t mask_end;
+    uint32_t transform;     /* into transforms                                     */
+    uint32_t material;      /* into slabs, or DPROP_INVALID_INDEX                  */
+    uint32_t volume;        /* owning volume                                       */
+    uint8_t shape;          /* dprop_shape of all masks of this surface            */
+    uint8_t kind;           /* dprop_surface_kind                                  */
+    uint8_t pad[2];
+} dprop_surface_desc;
+
+typedef struct dprop_mask_desc {
+    double values[6];       /* shape bounds, meaning per dprop_shape               */
+    uint32_t volume_link;   /* next volume through this mask, DPROP_INVALID_LINK = leaves world */
+    uint32_t pad;
+} dprop_mask_desc;
+
+/* Placement: rotation columns (local x, y, z axes in global frame),
+ * translation, and the inverse transform as stored by the reference's
+ * transform3 (algebra/generic/impl/generic_transform3.hpp). */
+typedef struct dprop_transform_desc {
+    double rot[9];          /* column-major: x axis, y axis, z axis            */
+    double translation[3];
+    double inv_rot[9];      /* column-major rotation part of the inverse       */
+    double inv_translation[3];
+} dprop_transform_desc;
+
+/* Homogeneous material slab (material/material_slab.hpp:78-97) with the
+ * derived quantities the interaction formulas read
+ * (material/material.hpp, material/detail/relativistic_quantities.hpp). */
+typedef struct dprop_slab_desc {
+    double thickness;
+    double thickness_in_X0;
+    double X0;
+    double molar_electron_density;  /* Z * molar density                 */
+    double mean_excitation_energy;  /* I                                 */
+    double density_a, density_m, density_x0, density_x1, density_c;
+    uint32_t has_density_effect;
+    uint32_t pad;
+} dprop_slab_desc;
+
+typedef enum dprop_grid_kind {
+    DPROP_GRID_NONE = 0,
+    DPROP_GRID_CYLINDER = 1, /* axes (phi circular [-pi,pi], z closed), ref. radius */
+    DPROP_GRID_DISC = 2      /* axes (r closed, phi circular [-pi,pi])              */
+} dprop_grid_kind;
+
+/* A 2D surface grid, spatial_grid<..., static_array<surface,1>> of
+ * navigation/accelerators/spatial_grid.hpp with regular binning. */
+typedef struct dprop_grid_desc {
+    uint32_t kind;          /* dprop_grid_kind                                  */
+    uint32_t n_bins[2];
+    uint32_t bin_offset;    /* into grid_bins: n_bins[0]*n_bins[1] entries,
+                               serialised as bin0 + bin1 * n_bins[0]            */
+    uint32_t transform;     /* grid placement (the volume's transform)          */
+    uint32_t pad;
+    double axis_min[2];
+    double axis_max[2];
+    double radius;          /* reference cylinder radius (DPROP_GRID_CYLINDER)  */
+} dprop_grid_desc;
+
+typedef struct dprop_volume_desc {
+    uint32_t transform;
+    uint32_t bf_begin;      /* [bf_begin, bf_end) into bf_surfaces: portals and
+                               passives searched by brute force                 */
+    uint32_t bf_end;
+    uint32_t grid;          /* into grids, or DPROP_INVALID_INDEX                */
+} dprop_volume_desc;
+
+typedef struct dprop_detector_desc {
+    uint32_t abi_version;           /* = DPROP_ABI_VERSION */
+    uint32_t n_volumes, n_surfaces, n_masks, n_transforms, n_slabs;
+    uint32_t n_bf_surfaces, n_grids, n_grid_bins;
+    const dprop_volume_desc* volumes;
+    const dprop_surface_desc* surfaces;
+    const dprop_mask_desc* masks;
+    const dprop_transform_desc* transforms;
+    const dprop_slab_desc* slabs;
+    const uint32_t* bf_surfaces;    /* surface indices                          */
+    const dprop_grid_desc* grids;
+    const uint32_t* grid_bins;      /* surface index or DPROP_INVALID_INDEX      */
+} dprop_detector_desc;
+
+typedef struct dprop_detector dprop_detector;
+typedef struct dprop_field dprop_field;
+
+/* ------------------------------------------------------------------ config
+ * Mirrors propagation::config = {navigation, stepping} and the actor chain
+ * switches.  Defaults (dprop_config_default) are the reference's defaults:
+ * stepping_config.hpp:27-77, navigation_config.hpp:23-56,
+ * intersection_config.hpp:20-33. */
+typedef struct dprop_config {
+    /* stepping::config */
+    float min_stepsize;
+    float rk_error_tol;
+    float step_constraint;
+    float path_limit;
+    uint32_t max_rk_updates;
+    uint8_t use_mean_loss;
+    uint8_t use_eloss_gradient;
+    uint8_t use_field_gradient;
+    uint8_t do_covariance_transport;
+    /* intersection::config */
+    float min_mask_tolerance;
+    float max_mask_tolerance;
+    float mask_tolerance_scalor;
+    float path_tolerance;
+    float overstep_tolerance;
+    /* navigation::config */
+    uint32_t search_window[2];
+    float accumulated_error;
+    int32_t n_scattering_stddev;
+    uint8_t estimate_scattering_noise;
+    /* actor chain */
+    uint8_t use_path_limit_aborter;   /* pathlimit_aborter in the chain        */
+    uint8_t use_material_interactor;  /* pointwise_material_interactor        */
+    uint8_t record_all_surfaces;      /* 0: record surfaces the transporter
+                                         visits (sensitive or with material);
+                                         1: also portals/passives w/o material */
+    /* particle hypothesis (muon by default, charge sign follows q/p) */
+    float mass;
+    int32_t pdg;
+    /* device limits */
+    uint32_t max_records;             /* per-track record capacity            */
+    uint32_t max_iterations;          /* A/N/S loop bound per track           */
+} dprop_config;
+
+/* ------------------------------------------------------------------ tracks
+ * Struct-of-arrays free track parameters, detray's free vector layout
+ * [x, y, z, t, tx, ty, tz, q/p] (definitions/track_parametrization.hpp:49-63).
+ * Device-side float arrays for dprop_propagate; host double arrays for
+ * dprop_propagate_host. */
+typedef struct dprop_tracks {
+    const void* pos[3];
+    const void* time;
+    const void* dir[3];
+    const void* qop;
+} dprop_tracks;
+
+/* Results.  Records are laid out slot-major: record k of track t sits at
+ * index k * n_tracks + t, so that lanes of a warp writing the same slot
+ * coalesce.  Bound parameters follow detray's bound vector
+ * [loc0, loc1, phi, theta, q/p, t]; the covariance is the upper triangle of
+ * the 6x6 matrix, row by row (21 values). */
+typedef struct dprop_results {
+    uint8_t* status;          /* [n] dprop_track_status                        */
+    uint32_t* n_records;      /* [n] records written (may exceed capacity: then
+                                  only the first max_records are stored)        */
+    uint32_t* n_steps;        /* [n] accepted RK steps                          */
+    uint32_t* n_trials;       /* [n] RK trials                                  */
+    void* path_length;        /* [n] final path length                          */
+    void* final_free[8];      /* [n] each; may be NULL                          */
+    uint64_t* rec_barcode;    /* [max_records * n]                              */
+    void* rec_bound[6];       /* [max_records * n] each; may be NULL            */
+    void* rec_cov[21];        /* [max_records * n] each; may be NULL            */
+    void* rec_path;           /* [max_records * n]; may be NULL                 */
+    uint8_t* rec_flags;       /* [max_records * n]; bit0: transported (bound +
+                                  cov valid), bit1: portal, bit2: material     */
+} dprop_results;
+
+/* Launch shape; zero fields pick the library defaults / autotuned values. */
+typedef enum dprop_method {
+    DPROP_METHOD_PLAIN = 0,      /* one thread per track, whole propagation   */
+    DPROP_METHOD_PERSISTENT = 1  /* persistent lanes pulling tracks from a
+                                    device work queue                         */
+} dprop_method;
+
+typedef struct dprop_launch {
+    uint32_t method;             /* dprop_method                               */
+    uint32_t block_size;         /* threads per CTA                            */
+    uint32_t ctas_per_sm;        /* persistent grid = SMs * ctas_per_sm         */
+    uint32_t reserved[5];
+} dprop_launch;
+
+/* ------------------------------------------------------------------ API */
+uint32_t dprop_abi_version(void);
+const char* dprop_last_error(void);
+
+void dprop_config_default(dprop_config* cfg);
+
+/* Replaces detray::get_buffer + get_data for the detector stores. */
+dprop_status dprop_detector_create(const dprop_detector_desc* desc,
+                                   int device, dprop_detector** out);
+dprop_status dprop_detector_destroy(dprop_detector* det);
+
+/* Constant field, like covfie::backend::constant (bfield.hpp:35-40). */
+dprop_status dprop_field_create_const(double bx, double by, double bz,
+                                      int device, dprop_field** out);
+/* Field map on a regular (r, phi, z) grid, values (Br, Bphi, Bz) per node,
+ * node index ((iz * n_phi) + iphi) * n_r + ir; trilinear interpolation with
+ * clamping at the grid edges.  Stands where the reference plugs a covfie
+ * affine<linear<clamp<strided<...>>>> view (bfield.hpp:43-47). */
+dprop_status dprop_field_create_grid(const double* r_phi_z_min,
+                                     const double* r_phi_z_max,
+                                     const uint32_t* n_r_phi_z,
+                                     const float* values, int device,
+                                     dprop_field** out);
+dprop_status dprop_field_destroy(dprop_field* field);
+
+/* Propagate n tracks whose parameters and results live in device memory.
+ * Stream ordered; returns once the work is enqueued on `stream`
+ * (a cudaStream_t, or NULL for the legacy default stream). */
+dprop_status dprop_propagate(const dprop_config* cfg,
+                             const dprop_launch* launch,
+                             const dprop_detector* det,
+                             const dprop_field* field,
+                             const dprop_tracks* tracks,
+                             const dprop_results* results, uint64_t n_tracks,
+                             void* stream);
+
+/* Same, with host double-precision inputs and host outputs (the result
+ * pointers then point to host memory, float fields as double).  Copies in,
+ * propagates, copies out and synchronises. */
+dprop_status dprop_propagate_host(const dprop_config* cfg,
+                                  const dprop_launch* launch,
+                                  const dprop_detector* det,
+                                  const dprop_field* field,
+                                  const dprop_tracks* tracks,
+                                  const dprop_results* results,
+                                  uint64_t n_tracks);
+
+/* Number of surfaces / volumes held by a detector (for callers sizing output). */
+dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
+                                 uint32_t* n_surfaces);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DETRAY_B200_DPROP_H */

@@ -1,0 +1,2 @@
+#pragma once
+#include "vecmem/containers/data/vector_view.hpp"

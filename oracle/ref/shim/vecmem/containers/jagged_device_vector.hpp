@@ -1,0 +1,22 @@
+#pragma once
+#include "vecmem/containers/device_vector.hpp"
+
+namespace vecmem {
+template <typename T>
+class jagged_device_vector {
+   public:
+    using size_type = unsigned int;
+    jagged_device_vector() = default;
+    explicit jagged_device_vector(const data::jagged_vector_view<T>& v)
+        : m_view(v) {}
+    device_vector<T> operator[](size_type i) const {
+        return device_vector<T>(m_view.ptr()[i]);
+    }
+    device_vector<T> at(size_type i) const { return (*this)[i]; }
+    size_type size() const { return m_view.size(); }
+    bool empty() const { return m_view.size() == 0; }
+
+   private:
+    data::jagged_vector_view<T> m_view;
+};
+}  // namespace vecmem

@@ -1,0 +1,271 @@
+"""ORACLE - test infrastructure only.
+
+Python access to the reference detray propagator compiled by
+``oracle/ref/Makefile`` into ``oracle/_ref/libdetray_ref_{f64,f32}.so``.
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module; the product never does.
+
+Functions:
+  * ``build_toy`` / ``build_telescope``: the reference's detector builders
+    (tests/include/detray/test/common/build_toy_detector.hpp:1237,
+    build_telescope_detector.hpp:187) and their flattened tables;
+  * ``propagate``: propagator::propagate over a batch with OpenMP
+    (core/include/detray/propagator/propagator.hpp:260-400), actor chain
+    pathlimit_aborter -> parameter_updater<pointwise_material_interactor>
+    -> surface recorder, results in the dprop_results layout (doubles).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from detray_b200 import abi
+
+_HERE = Path(__file__).resolve().parent
+REF_DIR = _HERE / "_ref"
+
+
+class _RefTelCfg(C.Structure):
+    _fields_ = [
+        ("half_x", C.c_double),
+        ("half_y", C.c_double),
+        ("positions", C.POINTER(C.c_double)),
+        ("n_positions", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("pilot_dir", C.c_double * 3),
+        ("mat_thickness", C.c_double),
+        ("envelope", C.c_double),
+    ]
+
+
+class _RefToyCfg(C.Structure):
+    _fields_ = [
+        ("n_brl_layers", C.c_uint32),
+        ("n_edc_layers", C.c_uint32),
+        ("module_mat_thickness", C.c_double),
+        ("beampipe_mat_thickness", C.c_double),
+        ("use_material_maps", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+class RefFieldDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("n", C.c_uint32 * 3),
+        ("b", C.c_double * 3),
+        ("lo", C.c_double * 3),
+        ("hi", C.c_double * 3),
+        ("values", C.POINTER(C.c_float)),
+    ]
+
+
+_LIBS: dict[str, C.CDLL] = {}
+
+
+def available(precision: str = "f64") -> bool:
+    return (REF_DIR / f"libdetray_ref_{precision}.so").exists()
+
+
+def load(precision: str = "f64") -> C.CDLL:
+    if precision in _LIBS:
+        return _LIBS[precision]
+    path = REF_DIR / f"libdetray_ref_{precision}.so"
+    if not path.exists():
+        raise FileNotFoundError(
+            f"{path} missing: build it with `make -C oracle/ref` "
+            "(needs the reference checkout)")
+    lib = C.CDLL(str(path))
+    lib.ref_last_error.restype = C.c_char_p
+    lib.ref_build_toy.argtypes = [C.POINTER(_RefToyCfg), C.POINTER(C.c_void_p)]
+    lib.ref_build_telescope.argtypes = [C.POINTER(_RefTelCfg),
+                                        C.POINTER(C.c_void_p)]
+    lib.ref_tables.argtypes = [C.c_void_p, C.POINTER(abi.DetectorDesc)]
+    lib.ref_destroy.argtypes = [C.c_void_p]
+    lib.ref_propagate.argtypes = [
+        C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
+        C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
+        C.c_int, C.c_int]
+    lib.ref_field_eval.argtypes = [C.POINTER(RefFieldDesc),
+                                   C.POINTER(C.c_double), C.c_uint64,
+                                   C.POINTER(C.c_double)]
+    _LIBS[precision] = lib
+    return lib
+
+
+class RefDetector:
+    """A reference-built detector plus its flattened tables."""
+
+    def __init__(self, lib: C.CDLL, handle: C.c_void_p):
+        self._lib = lib
+        self.handle = handle
+        self.desc = abi.DetectorDesc()
+        lib.ref_tables(handle, C.byref(self.desc))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self._lib.ref_destroy(self.handle)
+            self.handle = None
+
+    def tables(self) -> dict:
+        """Copies of the flat tables as numpy structured arrays."""
+        d = self.desc
+
+        def arr(ptr, n, ctype):
+            if n == 0:
+                return np.zeros(0, dtype=np.ctypeslib.as_ctypes_type(ctype)
+                                if False else None)
+            buf = (ctype * n).from_address(C.addressof(ptr.contents))
+            return np.ctypeslib.as_array(buf).copy()
+
+        out = {}
+        out["volumes"] = np.ctypeslib.as_array(
+            (abi.VolumeDesc * d.n_volumes).from_address(
+                C.addressof(d.volumes.contents))).copy()
+        out["surfaces"] = np.ctypeslib.as_array(
+            (abi.SurfaceDesc * d.n_surfaces).from_address(
+                C.addressof(d.surfaces.contents))).copy()
+        out["masks"] = np.ctypeslib.as_array(
+            (abi.MaskDesc * d.n_masks).from_address(
+                C.addressof(d.masks.contents))).copy()
+        out["transforms"] = np.ctypeslib.as_array(
+            (abi.TransformDesc * d.n_transforms).from_address(
+                C.addressof(d.transforms.contents))).copy()
+        if d.n_slabs:
+            out["slabs"] = np.ctypeslib.as_array(
+                (abi.SlabDesc * d.n_slabs).from_address(
+                    C.addressof(d.slabs.contents))).copy()
+        else:
+            out["slabs"] = np.zeros(0, dtype=np.dtype(abi.SlabDesc))
+        out["bf_surfaces"] = np.ctypeslib.as_array(
+            (C.c_uint32 * d.n_bf_surfaces).from_address(
+                C.addressof(d.bf_surfaces.contents))).copy()
+        if d.n_grids:
+            out["grids"] = np.ctypeslib.as_array(
+                (abi.GridDesc * d.n_grids).from_address(
+                    C.addressof(d.grids.contents))).copy()
+            out["grid_bins"] = np.ctypeslib.as_array(
+                (C.c_uint32 * d.n_grid_bins).from_address(
+                    C.addressof(d.grid_bins.contents))).copy()
+        else:
+            out["grids"] = np.zeros(0, dtype=np.dtype(abi.GridDesc))
+            out["grid_bins"] = np.zeros(0, dtype=np.uint32)
+        return out
+
+
+def _check(lib, rc):
+    if rc != 0:
+        raise RuntimeError(lib.ref_last_error().decode())
+
+
+def build_toy(n_brl_layers=4, n_edc_layers=7, module_mat_thickness=0.15,
+              beampipe_mat_thickness=0.0, use_material_maps=False,
+              precision="f64") -> RefDetector:
+    lib = load(precision)
+    cfg = _RefToyCfg(n_brl_layers, n_edc_layers, module_mat_thickness,
+                     beampipe_mat_thickness, int(use_material_maps), 0)
+    h = C.c_void_p()
+    _check(lib, lib.ref_build_toy(C.byref(cfg), C.byref(h)))
+    return RefDetector(lib, h)
+
+
+def build_telescope(positions=tuple(50.0 * i for i in range(10)),
+                    half_x=500.0, half_y=500.0, pilot_dir=(1.0, 0.0, 0.0),
+                    mat_thickness=0.3, envelope=0.0,
+                    precision="f64") -> RefDetector:
+    lib = load(precision)
+    pos = (C.c_double * len(positions))(*positions)
+    cfg = _RefTelCfg(half_x, half_y, pos, len(positions), 0,
+                     (C.c_double * 3)(*pilot_dir), mat_thickness, envelope)
+    h = C.c_void_p()
+    _check(lib, lib.ref_build_telescope(C.byref(cfg), C.byref(h)))
+    return RefDetector(lib, h)
+
+
+def field_desc(field) -> tuple[RefFieldDesc, object]:
+    """Translate a detray_b200 field specification (dict) into the oracle's
+    descriptor.  Returns (desc, keepalive)."""
+    fd = RefFieldDesc()
+    keep = None
+    if field["kind"] == "const":
+        fd.kind = 0
+        for i in range(3):
+            fd.b[i] = float(field["b"][i])
+    else:
+        fd.kind = 1
+        vals = np.ascontiguousarray(field["values"], dtype=np.float32)
+        keep = vals
+        for i in range(3):
+            fd.n[i] = int(field["n"][i])
+            fd.lo[i] = float(field["lo"][i])
+            fd.hi[i] = float(field["hi"][i])
+        fd.values = vals.ctypes.data_as(C.POINTER(C.c_float))
+    return fd, keep
+
+
+def field_eval(field, xyz: np.ndarray, precision="f64") -> np.ndarray:
+    lib = load(precision)
+    fd, keep = field_desc(field)
+    pts = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros_like(pts)
+    lib.ref_field_eval(C.byref(fd), pts.ctypes.data_as(C.POINTER(C.c_double)),
+                       pts.shape[0], out.ctypes.data_as(C.POINTER(C.c_double)))
+    del keep
+    return out
+
+
+def alloc_results(n: int, max_records: int) -> tuple[dict, abi.Results]:
+    """Host result buffers (doubles for floating fields) + the ABI struct."""
+    res = {
+        "status": np.full(n, 255, dtype=np.uint8),
+        "n_records": np.zeros(n, dtype=np.uint32),
+        "n_steps": np.zeros(n, dtype=np.uint32),
+        "n_trials": np.zeros(n, dtype=np.uint32),
+        "path_length": np.zeros(n, dtype=np.float64),
+        "final_free": np.zeros((8, n), dtype=np.float64),
+        "rec_barcode": np.full((max_records, n), np.iinfo(np.uint64).max,
+                               dtype=np.uint64),
+        "rec_bound": np.zeros((6, max_records, n), dtype=np.float64),
+        "rec_cov": np.zeros((21, max_records, n), dtype=np.float64),
+        "rec_path": np.zeros((max_records, n), dtype=np.float64),
+        "rec_flags": np.zeros((max_records, n), dtype=np.uint8),
+    }
+    r = abi.Results()
+    r.status = res["status"].ctypes.data
+    r.n_records = res["n_records"].ctypes.data
+    r.n_steps = res["n_steps"].ctypes.data
+    r.n_trials = res["n_trials"].ctypes.data
+    r.path_length = res["path_length"].ctypes.data
+    for i in range(8):
+        r.final_free[i] = res["final_free"][i].ctypes.data
+    r.rec_barcode = res["rec_barcode"].ctypes.data
+    for i in range(6):
+        r.rec_bound[i] = res["rec_bound"][i].ctypes.data
+    for i in range(21):
+        r.rec_cov[i] = res["rec_cov"][i].ctypes.data
+    r.rec_path = res["rec_path"].ctypes.data
+    r.rec_flags = res["rec_flags"].ctypes.data
+    return res, r
+
+
+def propagate(det: RefDetector, field: dict, cfg: abi.Config,
+              tracks: np.ndarray, n_threads: int = 0, chunk: int = 1,
+              abort_reasons: bool = True) -> dict:
+    """Run the reference propagator on ``tracks`` (shape (8, n) float64, the
+    free vector rows [x, y, z, t, tx, ty, tz, q/p])."""
+    lib = det._lib
+    trk = np.ascontiguousarray(tracks, dtype=np.float64)
+    n = trk.shape[1]
+    ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    res, r = alloc_results(n, cfg.max_records)
+    fd, keep = field_desc(field)
+    if n_threads <= 0:
+        n_threads = os.cpu_count() or 1
+    _check(lib, lib.ref_propagate(det.handle, C.byref(fd), C.byref(cfg), ptrs,
+                                  n, C.byref(r), n_threads, chunk,
+                                  int(abort_reasons)))
+    del keep
+    return res

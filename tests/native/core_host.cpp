@@ -1,0 +1,144 @@
+// TEST-ONLY host build of the device propagation core.
+//
+// The propagation core (detray_b200/csrc/core/*.cuh) is written as
+// __host__ __device__ templates.  This file compiles it with the host
+// compiler so the tests can compare its navigation and transport logic with
+// the reference oracle without a GPU, in double and in float precision.  It
+// is not part of the product library and the library never calls it.
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "core/config.hpp"
+#include "core/convert.hpp"
+#include "core/propagate.cuh"
+
+using namespace dprop;
+
+namespace {
+thread_local std::string g_err;
+
+template <typename S>
+struct sink_bufs {
+    std::vector<S> bound[6];
+    std::vector<S> cov[21];
+    std::vector<S> path;
+};
+
+template <typename S>
+int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
+        const double* lo, const double* hi, const uint32_t* nn,
+        const float* values, const dprop_config* c, const double* const* trk,
+        uint64_t n, const dprop_results* out) {
+    const std::string problem = validate_desc(desc);
+    if (!problem.empty()) {
+        g_err = problem;
+        return 1;
+    }
+    const host_tables<S> tables = convert_desc<S>(desc);
+    const detector_view<S> det = tables.view();
+    field_view<S> f{};
+    std::vector<float4> nodes;
+    if (field_kind == 0u) {
+        f.kind = 0u;
+        f.n_r = f.n_phi = f.n_z = 1u;
+        for (int i = 0; i < 3; ++i) {
+            f.b[i] = static_cast<S>(b[i]);
+        }
+    } else {
+        const uint64_t nn_all = static_cast<uint64_t>(nn[0]) * nn[1] * nn[2];
+        nodes.resize(nn_all);
+        for (uint64_t i = 0; i < nn_all; ++i) {
+            nodes[i] = float4{values[3 * i], values[3 * i + 1],
+                              values[3 * i + 2], 0.f};
+        }
+        f.kind = 1u;
+        f.n_r = nn[0];
+        f.n_phi = nn[1];
+        f.n_z = nn[2];
+        f.r_lo = static_cast<S>(lo[0]);
+        f.r_step_inv = nn[0] > 1 ? static_cast<S>((nn[0] - 1) / (hi[0] - lo[0])) : S(0);
+        f.phi_lo = static_cast<S>(lo[1]);
+        f.phi_step_inv = static_cast<S>(nn[1] / (2.0 * constant::pi));
+        f.z_lo = static_cast<S>(lo[2]);
+        f.z_step_inv = nn[2] > 1 ? static_cast<S>((nn[2] - 1) / (hi[2] - lo[2])) : S(0);
+        f.nodes = nodes.data();
+    }
+    const prop_cfg<S> cfg = make_prop_cfg<S>(*c);
+    const uint32_t cap = c->max_records;
+    for (uint64_t t = 0; t < n; ++t) {
+        track_state<S> ts;
+        init_track_state(ts,
+                         vec3<S>{static_cast<S>(trk[0][t]), static_cast<S>(trk[1][t]),
+                                 static_cast<S>(trk[2][t])},
+                         static_cast<S>(trk[3][t]),
+                         vec3<S>{static_cast<S>(trk[4][t]), static_cast<S>(trk[5][t]),
+                                 static_cast<S>(trk[6][t])},
+                         static_cast<S>(trk[7][t]), cfg);
+        // records into per-track scratch, then widened into the double outputs
+        std::vector<uint64_t> bc(cap);
+        std::vector<S> bnd[6], cv[21];
+        std::vector<S> pth(cap);
+        std::vector<uint8_t> fl(cap);
+        record_sink<S> rec{};
+        rec.barcode = bc.data();
+        for (int i = 0; i < 6; ++i) {
+            bnd[i].assign(cap, S(0));
+            rec.bound[i] = bnd[i].data();
+        }
+        for (int i = 0; i < 21; ++i) {
+            cv[i].assign(cap, S(0));
+            rec.cov[i] = cv[i].data();
+        }
+        rec.path = pth.data();
+        rec.flags = fl.data();
+        rec.n_tracks = 1u;
+        rec.track = 0u;
+        rec.capacity = cap;
+        rec.count = 0u;
+        const uint8_t status = propagate_track(ts, det, f, cfg, rec);
+        out->status[t] = status;
+        if (out->n_records) out->n_records[t] = rec.count;
+        if (out->n_steps) out->n_steps[t] = ts.step.n_steps;
+        if (out->n_trials) out->n_trials[t] = ts.step.n_trials;
+        if (out->path_length)
+            static_cast<double*>(out->path_length)[t] = ts.step.path_length;
+        const double fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
+                               ts.step.time,  ts.step.dir.x, ts.step.dir.y,
+                               ts.step.dir.z, ts.step.qop};
+        for (int i = 0; i < 8; ++i) {
+            if (out->final_free[i]) static_cast<double*>(out->final_free[i])[t] = fin[i];
+        }
+        const uint32_t m = rec.count < cap ? rec.count : cap;
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint64_t o = static_cast<uint64_t>(k) * n + t;
+            if (out->rec_barcode) out->rec_barcode[o] = bc[k];
+            if (out->rec_flags) out->rec_flags[o] = fl[k];
+            if (out->rec_path) static_cast<double*>(out->rec_path)[o] = pth[k];
+            for (int i = 0; i < 6; ++i) {
+                if (out->rec_bound[i]) static_cast<double*>(out->rec_bound[i])[o] = bnd[i][k];
+            }
+            for (int i = 0; i < 21; ++i) {
+                if (out->rec_cov[i]) static_cast<double*>(out->rec_cov[i])[o] = cv[i][k];
+            }
+        }
+    }
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+const char* core_host_last_error(void) { return g_err.c_str(); }
+
+int core_host_propagate(int precision_bytes, const dprop_detector_desc* desc,
+                        uint32_t field_kind, const double* b, const double* lo,
+                        const double* hi, const uint32_t* nn, const float* values,
+                        const dprop_config* cfg, const double* const* trk,
+                        uint64_t n, const dprop_results* out) {
+    if (precision_bytes == 8) {
+        return run<double>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
+    }
+    return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
+}
+}
