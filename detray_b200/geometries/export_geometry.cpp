@@ -1,0 +1,103 @@
+// Build-time geometry exporter.
+//
+// Builds the reference's benchmark detectors with detray's own builders
+// (tests/include/detray/test/common/build_toy_detector.hpp:1237,
+// build_telescope_detector.hpp:187) and writes their flattened device tables
+// (dprop::flatten, include/detray_b200/detray_adapter.hpp) to a raw table
+// file that make_geometries.py packs into the .npz files the product loads.
+// It is a detray *user* of the product adapter, compiled against the detray
+// headers of a reference checkout; the device library never runs it.
+//
+// usage: export_geometry toy <n_brl> <n_edc> <module_thickness_mm> <out>
+//        export_geometry telescope <half_x> <half_y> <thickness_mm> <out> <x0> [x1 ...]
+#include "detray/definitions/algebra.hpp"
+#include "detray/test/common/build_telescope_detector.hpp"
+#include "detray/test/common/build_toy_detector.hpp"
+#include "detray/tracks/ray.hpp"
+
+#include <vecmem/memory/host_memory_resource.hpp>
+
+#include "detray_b200/detray_adapter.hpp"
+
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+using namespace detray;
+using algebra_t = detray::array<double>;
+using scalar = double;
+
+namespace {
+
+template <typename T>
+void write_vec(std::FILE* f, const std::vector<T>& v) {
+    if (!v.empty()) {
+        std::fwrite(v.data(), sizeof(T), v.size(), f);
+    }
+}
+
+int write_tables(const dprop::flat_detector& t, const char* path) {
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        std::perror(path);
+        return 1;
+    }
+    const uint32_t header[12] = {0x4f454744u,  // "DGEO"
+                                 DPROP_ABI_VERSION,
+                                 static_cast<uint32_t>(t.volumes.size()),
+                                 static_cast<uint32_t>(t.surfaces.size()),
+                                 static_cast<uint32_t>(t.masks.size()),
+                                 static_cast<uint32_t>(t.transforms.size()),
+                                 static_cast<uint32_t>(t.slabs.size()),
+                                 static_cast<uint32_t>(t.bf_surfaces.size()),
+                                 static_cast<uint32_t>(t.grids.size()),
+                                 static_cast<uint32_t>(t.grid_bins.size()),
+                                 0u,
+                                 0u};
+    std::fwrite(header, sizeof(uint32_t), 12, f);
+    write_vec(f, t.volumes);
+    write_vec(f, t.surfaces);
+    write_vec(f, t.masks);
+    write_vec(f, t.transforms);
+    write_vec(f, t.slabs);
+    write_vec(f, t.bf_surfaces);
+    write_vec(f, t.grids);
+    write_vec(f, t.grid_bins);
+    std::fclose(f);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: see source header\n");
+        return 2;
+    }
+    vecmem::host_memory_resource mr;
+    const std::string kind = argv[1];
+    if (kind == "toy" && argc == 6) {
+        toy_det_config<scalar> cfg{};
+        cfg.n_brl_layers(static_cast<unsigned int>(std::atoi(argv[2])))
+            .n_edc_layers(static_cast<unsigned int>(std::atoi(argv[3])))
+            .use_material_maps(false)
+            .module_mat_thickness(std::atof(argv[4]));
+        auto [det, names] = build_toy_detector<algebra_t>(mr, cfg);
+        return write_tables(dprop::flatten(det), argv[5]);
+    }
+    if (kind == "telescope" && argc >= 7) {
+        std::vector<scalar> pos;
+        for (int i = 6; i < argc; ++i) {
+            pos.push_back(std::atof(argv[i]));
+        }
+        tel_det_config<algebra_t, rectangle2D> cfg{std::atof(argv[2]),
+                                                   std::atof(argv[3])};
+        detail::ray<algebra_t> pilot{{0., 0., 0.}, 0., {1., 0., 0.}, -1.};
+        cfg.positions(pos).pilot_track(pilot).mat_thickness(std::atof(argv[4]));
+        auto [det, names] = build_telescope_detector<algebra_t, rectangle2D>(mr, cfg);
+        return write_tables(dprop::flatten(det), argv[5]);
+    }
+    std::fprintf(stderr, "bad arguments\n");
+    return 2;
+}

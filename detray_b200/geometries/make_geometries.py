@@ -1,0 +1,60 @@
+"""Regenerate the committed benchmark geometries (build-time step).
+
+Compiles export_geometry.cpp against the detray headers of a reference
+checkout (path in $DETRAY_REF, default /root/reference) and packs the tables
+of the benchmark detectors into compressed .npz files next to this script:
+
+  toy_4brl_7edc.npz          toy barrel + endcap detector, 4 barrel layers,
+                             7 endcap discs per side, 0.15 mm Si modules
+  telescope_10x1m_300um.npz  10 1 m x 1 m Si planes normal to x at
+                             x = 0, 50, ..., 450 mm, 0.3 mm thick
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+sys.path.insert(0, str(REPO))
+
+from detray_b200 import geometry  # noqa: E402
+
+GEOMETRIES = {
+    "toy_4brl_7edc": ["toy", "4", "7", "0.15"],
+    "telescope_10x1m_300um": ["telescope", "500", "500", "0.3"],
+}
+TELESCOPE_POSITIONS = [str(50.0 * i) for i in range(10)]
+
+
+def build_exporter(ref: Path, out: Path) -> None:
+    cmd = ["g++", "-std=c++20", "-O3", "-march=x86-64-v3", "-w", "-DDETRAY_ALGEBRA_ARRAY=1",
+           "-DDETRAY_CUSTOM_SCALARTYPE=double", f"-I{HERE / 'shim'}",
+           f"-I{ref / 'core/include'}",
+           f"-I{ref / 'plugins/algebra/array/include'}",
+           f"-I{ref / 'detectors/include'}", f"-I{ref / 'tests/include'}",
+           f"-I{ref / 'io/include'}", f"-I{REPO / 'include'}",
+           str(HERE / "export_geometry.cpp"), "-o", str(out)]
+    subprocess.run(cmd, check=True)
+
+
+def main() -> None:
+    ref = Path(os.environ.get("DETRAY_REF", "/root/reference"))
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = Path(tmp) / "export_geometry"
+        build_exporter(ref, exe)
+        for name, args in GEOMETRIES.items():
+            raw = Path(tmp) / f"{name}.bin"
+            extra = TELESCOPE_POSITIONS if args[0] == "telescope" else []
+            subprocess.run([str(exe), *args[:4], str(raw), *extra], check=True)
+            tables = geometry.read_raw_tables(raw)
+            geometry.save_npz(tables, HERE / f"{name}.npz")
+            print(f"wrote {name}.npz: "
+                  + ", ".join(f"{k}={len(v)}" for k, v in tables.items()))
+
+
+if __name__ == "__main__":
+    main()

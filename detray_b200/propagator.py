@@ -1,0 +1,314 @@
+"""Python binding of the B200 propagator over its C ABI.
+
+Mirrors the reference's device propagation call shape
+(tests/benchmarks/include/detray/benchmarks/device/cuda/
+propagation_benchmark.hpp:83-93):
+
+    det   = Detector(tables)                       # detray::get_buffer/get_data
+    field = Field.constant((0, 0, 2 * unit.T))     # covfie constant field view
+    res   = propagate(cfg, det, field, tracks)     # run_propagation_kernel
+
+Device memory and streams come from PyTorch; the propagation itself is the
+sm_100a library ``detray_b200/_lib/libdetray_b200.so``.  There is no CPU
+fallback: if the library or a CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .geometry import Descriptor
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdetray_b200.so"
+
+_lib = None
+
+#: exported symbols of the C ABI (include/detray_b200/dprop.h)
+ABI_SYMBOLS = [
+    "dprop_abi_version", "dprop_last_error", "dprop_config_default",
+    "dprop_detector_create", "dprop_detector_destroy", "dprop_detector_info",
+    "dprop_field_create_const", "dprop_field_create_grid",
+    "dprop_field_destroy", "dprop_propagate", "dprop_propagate_host",
+]
+
+
+class PropagationError(RuntimeError):
+    pass
+
+
+def load_library() -> C.CDLL:
+    """Load the device library; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise PropagationError(
+            f"{LIB_PATH} not found: the CUDA library is not built "
+            "(run __graft_entry__.build() or detray_b200/build.py)")
+    lib = C.CDLL(str(LIB_PATH))
+    lib.dprop_abi_version.restype = C.c_uint32
+    lib.dprop_last_error.restype = C.c_char_p
+    lib.dprop_config_default.argtypes = [C.POINTER(abi.Config)]
+    lib.dprop_detector_create.argtypes = [C.POINTER(abi.DetectorDesc), C.c_int,
+                                          C.POINTER(C.c_void_p)]
+    lib.dprop_detector_destroy.argtypes = [C.c_void_p]
+    lib.dprop_detector_info.argtypes = [C.c_void_p, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint32)]
+    lib.dprop_field_create_const.argtypes = [C.c_double, C.c_double,
+                                             C.c_double, C.c_int,
+                                             C.POINTER(C.c_void_p)]
+    lib.dprop_field_create_grid.argtypes = [
+        C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+        C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_void_p)]
+    lib.dprop_field_destroy.argtypes = [C.c_void_p]
+    lib.dprop_propagate.argtypes = [
+        C.POINTER(abi.Config), C.POINTER(abi.Launch), C.c_void_p, C.c_void_p,
+        C.POINTER(abi.Tracks), C.POINTER(abi.Results), C.c_uint64, C.c_void_p]
+    lib.dprop_propagate_host.argtypes = [
+        C.POINTER(abi.Config), C.POINTER(abi.Launch), C.c_void_p, C.c_void_p,
+        C.POINTER(abi.Tracks), C.POINTER(abi.Results), C.c_uint64]
+    if lib.dprop_abi_version() != abi.DPROP_ABI_VERSION:
+        raise PropagationError("detray-b200 library ABI version mismatch")
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != abi.DPROP_OK:
+        msg = load_library().dprop_last_error().decode()
+        raise PropagationError(f"dprop status {rc}: {msg}")
+
+
+def default_config(**overrides) -> abi.Config:
+    """propagation::config defaults plus the actor-chain switches."""
+    return abi.make_config(**overrides)
+
+
+class Detector:
+    """Device copy of a detector's flat tables (immutable once created)."""
+
+    def __init__(self, tables: dict, device: int = 0):
+        lib = load_library()
+        self._desc = Descriptor(tables)
+        self.handle = C.c_void_p()
+        _check(lib.dprop_detector_create(C.byref(self._desc.desc), device,
+                                         C.byref(self.handle)))
+        self.device = device
+        self.n_surfaces = len(self._desc.tables["surfaces"])
+        self.n_volumes = len(self._desc.tables["volumes"])
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            load_library().dprop_detector_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field:
+    """Magnetic field view on the device."""
+
+    def __init__(self, handle: C.c_void_p, spec: dict):
+        self.handle = handle
+        self.spec = spec
+
+    @classmethod
+    def constant(cls, b, device: int = 0) -> "Field":
+        lib = load_library()
+        h = C.c_void_p()
+        _check(lib.dprop_field_create_const(float(b[0]), float(b[1]),
+                                            float(b[2]), device, C.byref(h)))
+        return cls(h, {"kind": "const", "b": tuple(float(x) for x in b)})
+
+    @classmethod
+    def grid(cls, spec: dict, device: int = 0) -> "Field":
+        """spec: {"lo": (r, phi, z), "hi": ..., "n": (nr, nphi, nz),
+        "values": float32 array (nz, nphi, nr, 3)}"""
+        lib = load_library()
+        lo = (C.c_double * 3)(*spec["lo"])
+        hi = (C.c_double * 3)(*spec["hi"])
+        n = (C.c_uint32 * 3)(*spec["n"])
+        vals = np.ascontiguousarray(spec["values"], dtype=np.float32)
+        h = C.c_void_p()
+        _check(lib.dprop_field_create_grid(
+            lo, hi, n, vals.ctypes.data_as(C.POINTER(C.c_float)), device,
+            C.byref(h)))
+        return cls(h, dict(spec, kind="grid"))
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            load_library().dprop_field_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
+                ctas_per_sm: int = 0) -> abi.Launch:
+    lc = abi.Launch()
+    lc.method = method
+    lc.block_size = block_size
+    lc.ctas_per_sm = ctas_per_sm
+    return lc
+
+
+@dataclass
+class DeviceResults:
+    """Device result buffers (torch tensors) + the ABI struct pointing at
+    them."""
+    tensors: dict
+    struct: abi.Results
+
+
+def alloc_device_results(n: int, max_records: int, device="cuda",
+                         with_records=True, with_cov=True) -> DeviceResults:
+    import torch
+    f32 = dict(dtype=torch.float32, device=device)
+    t = {
+        "status": torch.empty(n, dtype=torch.uint8, device=device),
+        "n_records": torch.empty(n, dtype=torch.int32, device=device),
+        "n_steps": torch.empty(n, dtype=torch.int32, device=device),
+        "n_trials": torch.empty(n, dtype=torch.int32, device=device),
+        "path_length": torch.empty(n, **f32),
+        "final_free": torch.empty((8, n), **f32),
+    }
+    r = abi.Results()
+    r.status = t["status"].data_ptr()
+    r.n_records = t["n_records"].data_ptr()
+    r.n_steps = t["n_steps"].data_ptr()
+    r.n_trials = t["n_trials"].data_ptr()
+    r.path_length = t["path_length"].data_ptr()
+    for i in range(8):
+        r.final_free[i] = t["final_free"][i].data_ptr()
+    if with_records and max_records > 0:
+        t["rec_barcode"] = torch.empty((max_records, n), dtype=torch.int64,
+                                       device=device)
+        t["rec_bound"] = torch.empty((6, max_records, n), **f32)
+        t["rec_path"] = torch.empty((max_records, n), **f32)
+        t["rec_flags"] = torch.empty((max_records, n), dtype=torch.uint8,
+                                     device=device)
+        r.rec_barcode = t["rec_barcode"].data_ptr()
+        for i in range(6):
+            r.rec_bound[i] = t["rec_bound"][i].data_ptr()
+        r.rec_path = t["rec_path"].data_ptr()
+        r.rec_flags = t["rec_flags"].data_ptr()
+        if with_cov:
+            t["rec_cov"] = torch.empty((21, max_records, n), **f32)
+            for i in range(21):
+                r.rec_cov[i] = t["rec_cov"][i].data_ptr()
+    return DeviceResults(t, r)
+
+
+def tracks_struct(trk) -> abi.Tracks:
+    """ABI track pointers for a (8, n) contiguous float32 CUDA tensor or a
+    (8, n) float64 host numpy array."""
+    ts = abi.Tracks()
+    if hasattr(trk, "data_ptr"):
+        rows = [trk[i].data_ptr() for i in range(8)]
+    else:
+        rows = [trk[i].ctypes.data for i in range(8)]
+    for i in range(3):
+        ts.pos[i] = rows[i]
+        ts.dir[i] = rows[4 + i]
+    ts.time = rows[3]
+    ts.qop = rows[7]
+    return ts
+
+
+def propagate(cfg: abi.Config, det: Detector, field: Field, tracks,
+              results: DeviceResults | None = None, launch: abi.Launch | None = None,
+              stream=None) -> DeviceResults:
+    """Propagate the tracks of a (8, n) float32 CUDA tensor; stream ordered
+    on ``stream`` (default: torch's current stream)."""
+    import torch
+    if not (hasattr(tracks, "is_cuda") and tracks.is_cuda):
+        raise PropagationError("propagate() needs a CUDA tensor of tracks")
+    if tracks.dtype != torch.float32 or tracks.dim() != 2 or tracks.shape[0] != 8:
+        raise PropagationError("tracks must be a (8, n) float32 tensor")
+    tracks = tracks.contiguous()
+    n = tracks.shape[1]
+    if results is None:
+        results = alloc_device_results(n, cfg.max_records, tracks.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(tracks.device)
+    ts = tracks_struct(tracks)
+    lc = launch if launch is not None else make_launch()
+    _check(load_library().dprop_propagate(
+        C.byref(cfg), C.byref(lc), det.handle, field.handle, C.byref(ts),
+        C.byref(results.struct), n, C.c_void_p(stream.cuda_stream)))
+    return results
+
+
+def alloc_host_results(n: int, max_records: int, pinned: bool = False,
+                       with_cov: bool = True) -> tuple[dict, abi.Results]:
+    """Host result buffers for propagate_host (float fields as float32)."""
+    if pinned:
+        import torch
+
+        def empty(shape, dtype):
+            return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+        import torch as _t
+        u8, i32, f32, i64 = _t.uint8, _t.int32, _t.float32, _t.int64
+    else:
+        def empty(shape, dtype):
+            return np.empty(shape, dtype=dtype)
+        u8, i32, f32, i64 = np.uint8, np.int32, np.float32, np.int64
+    res = {
+        "status": empty((n,), u8),
+        "n_records": empty((n,), i32),
+        "n_steps": empty((n,), i32),
+        "n_trials": empty((n,), i32),
+        "path_length": empty((n,), f32),
+        "final_free": empty((8, n), f32),
+        "rec_barcode": empty((max_records, n), i64),
+        "rec_bound": empty((6, max_records, n), f32),
+        "rec_path": empty((max_records, n), f32),
+        "rec_flags": empty((max_records, n), u8),
+    }
+    if with_cov:
+        res["rec_cov"] = empty((21, max_records, n), f32)
+    r = abi.Results()
+    r.status = res["status"].ctypes.data
+    r.n_records = res["n_records"].ctypes.data
+    r.n_steps = res["n_steps"].ctypes.data
+    r.n_trials = res["n_trials"].ctypes.data
+    r.path_length = res["path_length"].ctypes.data
+    for i in range(8):
+        r.final_free[i] = res["final_free"][i].ctypes.data
+    r.rec_barcode = res["rec_barcode"].ctypes.data
+    for i in range(6):
+        r.rec_bound[i] = res["rec_bound"][i].ctypes.data
+    if with_cov:
+        for i in range(21):
+            r.rec_cov[i] = res["rec_cov"][i].ctypes.data
+    r.rec_path = res["rec_path"].ctypes.data
+    r.rec_flags = res["rec_flags"].ctypes.data
+    return res, r
+
+
+def propagate_host(cfg: abi.Config, det: Detector, field: Field,
+                   tracks: np.ndarray, launch: abi.Launch | None = None,
+                   out: tuple | None = None) -> dict:
+    """Propagate host tracks ((8, n) float64); host-to-device copies,
+    propagation and device-to-host copies happen inside the call."""
+    trk = np.ascontiguousarray(tracks, dtype=np.float64)
+    n = trk.shape[1]
+    res, r = out if out is not None else alloc_host_results(n, cfg.max_records)
+    ts = tracks_struct(trk)
+    lc = launch if launch is not None else make_launch()
+    _check(load_library().dprop_propagate_host(
+        C.byref(cfg), C.byref(lc), det.handle, field.handle, C.byref(ts),
+        C.byref(r), n))
+    return res

@@ -1,0 +1,81 @@
+"""CPU parity of the propagation core (test-only host build, tests/native)
+against the reference oracle.  In double precision the core follows the
+reference operation for operation: every surface sequence must match and the
+recorded parameters agree to ~1e-7.  In float precision at most 0.1 % of the
+tracks may cross a different surface (grazing a mask edge)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tests.parity import compare
+
+T = 0.000299792458
+
+
+def run_core(core_host, oracle, det_desc, cfg, trk, precision_bytes):
+    n = trk.shape[1]
+    res, r = oracle.alloc_results(n, cfg.max_records)
+    trk = np.ascontiguousarray(trk)
+    ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    b = (C.c_double * 3)(0.0, 0.0, 2.0 * T)
+    rc = core_host.core_host_propagate(precision_bytes, C.byref(det_desc), 0,
+                                       b, None, None, None, None,
+                                       C.byref(cfg), ptrs, C.c_uint64(n),
+                                       C.byref(r))
+    assert rc == 0, core_host.core_host_last_error()
+    return res
+
+
+TIGHT = {"loc0": 1e-7, "loc1": 1e-7, "phi": 1e-9, "theta": 1e-9,
+         "qop": 1e-12, "time": 1e-12}
+FP32 = {"loc0": 2e-3, "loc1": 2e-3, "phi": 2e-5, "theta": 2e-5,
+        "qop": 1e-7, "time": 1e-6}
+
+
+@pytest.mark.parametrize("kind,n", [("telescope", 1000), ("toy", 3000)])
+def test_core_f64_matches_reference(core_host, oracle, kind, n):
+    from detray_b200 import abi, tracks
+    if kind == "telescope":
+        det = oracle.build_telescope()
+        cfg = abi.make_config(max_records=16)
+        trk = tracks.telescope_tracks(n, seed=3)
+    else:
+        det = oracle.build_toy()
+        cfg = abi.make_config(max_records=32, search_window=(3, 3))
+        trk = tracks.toy_tracks(n, seed=4)
+    ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)}, cfg, trk)
+    got = run_core(core_host, oracle, det.desc, cfg, trk, 8)
+    s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
+                tol_rel=1e-7, cov_rel=1e-5)
+    assert s["seq_mismatch"] == 0 and s["status_mismatch"] == 0
+
+
+def test_core_f32_within_tolerance(core_host, oracle):
+    from detray_b200 import abi, tracks
+    det = oracle.build_toy()
+    cfg = abi.make_config(max_records=32, search_window=(3, 3))
+    trk = tracks.toy_tracks(3000, seed=5)
+    ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)}, cfg, trk)
+    got = run_core(core_host, oracle, det.desc, cfg, trk, 4)
+    compare(ref, got, max_seq_mismatch_frac=1e-3, tol_abs=FP32, tol_rel=1e-4,
+            cov_rel=1e-3)
+
+
+def test_core_noise_estimation_and_no_material(core_host, oracle):
+    """Actor-chain switches: scattering-noise tolerance on (the reference
+    default) and the material interactor off."""
+    from detray_b200 import abi, tracks
+    det = oracle.build_toy()
+    trk = tracks.toy_tracks(1000, seed=6)
+    for kw in [dict(estimate_scattering_noise=1),
+               dict(estimate_scattering_noise=0, use_material_interactor=0),
+               dict(do_covariance_transport=0, estimate_scattering_noise=0)]:
+        cfg = abi.make_config(max_records=32, search_window=(3, 3), **kw)
+        ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)},
+                               cfg, trk)
+        got = run_core(core_host, oracle, det.desc, cfg, trk, 8)
+        tight_cov = 1e-5 if kw.get("do_covariance_transport", 1) else 1e9
+        s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
+                    tol_rel=1e-7, cov_rel=tight_cov)
+        assert s["seq_mismatch"] == 0, kw
