@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark: tracks/s of batched track propagation through the toy detector.
+
+Workload (one "step" = one propagation of the whole batch):
+  toy barrel + endcap detector from the reference's toy generator (4 barrel
+  layers, 7 endcap discs per side, 0.15 mm Si modules, beampipe), homogeneous
+  2 T field along z, 1 M muons per GPU from a Gaussian vertex spread
+  (sigma 0.1, 0.1, 50 mm), eta uniform in [-4, 4], phi uniform, pT
+  log-uniform in [1, 100] GeV; fp32 RKN4 with covariance transport, material
+  interaction, path-limit aborter, 3x3 grid search window, bound parameters
+  and covariance recorded at every sensitive / material surface.
+  Data: synthetic, seeded.
+
+Lines printed by rank 0 (one JSON line):
+  value   tracks/s over all GPUs, inputs resident in HBM (device API);
+  e2e     the same through dprop_propagate_host: host inputs copied in and
+          all records copied out inside the timed region;
+  roofline  FP32 issue bound of the propagation kernel (algorithmic FLOPs
+          from device event counters x frozen per-event constants, see
+          detray_b200/flops.py);
+  cpu_baseline  the reference's own CPU propagator (fp32) on the host cores.
+
+--impl reference times the reference CPU implementation only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "tracks/s (toy det., RK4+cov. transport) on 1 B200 vs host CPU; adjoint/fwd cost"
+UNIT = "tracks/s"
+WORKLOAD = "toy_4brl_7edc_const2T_1M_muons_pt1-100_eta4"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--tracks", type=int, default=1_000_000,
+                   help="tracks per GPU per step")
+    p.add_argument("--method", choices=["plain", "persistent", "auto"],
+                   default="auto")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--seed", type=int, default=20241203)
+    return p.parse_args()
+
+
+def workload_config():
+    from detray_b200 import abi
+    # the reference CUDA benchmark settings (tests/benchmarks/cuda/
+    # propagation.cpp:56-74): window 3x3, no scattering-noise tolerance
+    return abi.make_config(max_records=32, search_window=(3, 3),
+                           estimate_scattering_noise=0)
+
+
+def make_tracks(n, seed):
+    from detray_b200 import tracks
+    return tracks.toy_tracks(n, seed=seed, pt_range=(1.0, 100.0),
+                             eta_range=(-4.0, 4.0),
+                             vertex_sigma=(0.1, 0.1, 50.0))
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv",
+                                                   delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.tmp.read().splitlines()
+                if ln.strip()]
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                if int(r[0]) != self.gpu_index:
+                    continue
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------- CPU baseline
+def cpu_reference_rate(n_target_seconds: float, cfg, seed: int,
+                       max_tracks: int, threads: int) -> dict:
+    """Reference CPU propagator (fp32 build, OpenMP over tracks, dynamic
+    schedule chunk 1 as in the reference benchmark) on a bounded sample."""
+    from oracle import ref_oracle
+    from detray_b200.units import T
+    det = ref_oracle.build_toy(precision="f32")
+    field = {"kind": "const", "b": (0.0, 0.0, 2.0 * T)}
+    probe = make_tracks(20_000, seed + 7)
+    ref_oracle.propagate(det, field, cfg, probe[:, :2000], n_threads=threads,
+                         abort_reasons=False)  # warm-up
+    t0 = time.perf_counter()
+    ref_oracle.propagate(det, field, cfg, probe, n_threads=threads,
+                         abort_reasons=False)
+    rate = probe.shape[1] / (time.perf_counter() - t0)
+    n = int(min(max_tracks, max(20_000, rate * n_target_seconds)))
+    sample = make_tracks(n, seed + 11)
+    t0 = time.perf_counter()
+    ref_oracle.propagate(det, field, cfg, sample, n_threads=threads,
+                         abort_reasons=False)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": threads,
+            "kind": "reference",
+            "sample": f"{n} tracks of the same workload (seed {seed + 11}), "
+                      f"{dt:.1f} s wall, fp32 reference build, OpenMP "
+                      f"dynamic,1 over tracks"}
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------ our impl
+def run_ours(args):
+    import torch
+
+    from detray_b200 import abi, flops, geometry, propagator
+    from detray_b200.units import T
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.tracks
+    cfg = workload_config()
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"), local)
+    field = propagator.Field.constant((0.0, 0.0, 2.0 * T), local)
+    host_trk = make_tracks(n, args.seed + rank)
+    trk = torch.tensor(host_trk, dtype=torch.float32, device=dev)
+    res = propagator.alloc_device_results(n, cfg.max_records, dev)
+    method = {"plain": abi.METHOD_PLAIN, "persistent": abi.METHOD_PERSISTENT,
+              "auto": abi.METHOD_PLAIN}[args.method]
+    lc = propagator.make_launch(method=method)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        propagator.propagate(cfg, det, field, trk, results=res, launch=lc,
+                             stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms_local = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms_local, world)
+    total_tracks = n * world
+    value = total_tracks / (ms / 1e3)
+
+    # algorithmic work of one launch from the device event counters
+    t = res.tensors
+    fl = flops.algorithmic_flops(t["n_trials"].cpu().numpy(),
+                                 t["n_steps"].cpu().numpy(),
+                                 t["n_intersections"].cpu().numpy(),
+                                 t["n_transports"].cpu().numpy(),
+                                 t["n_material"].cpu().numpy())
+    status = np.bincount(t["status"].cpu().numpy(), minlength=7)
+    mean_steps = float(t["n_steps"].float().mean().item())
+    achieved = fl / (ms_local / 1e3) / 1e12
+    peak_mhz = 1965.0
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+        peak_mhz = float(peaks.get("sm_max_mhz", peak_mhz))
+    except (OSError, ValueError):
+        pass
+    peak = flops.nominal_fp32_tflops(sm_count, peak_mhz)
+    traffic = None
+    prof = REPO / "profiles" / "propagate_toy_traffic.json"
+    if prof.exists():
+        try:
+            per_track = json.loads(prof.read_text())["dram_bytes_per_track"]
+            traffic = per_track * n
+        except (OSError, ValueError, KeyError):
+            traffic = None
+    roofline = {"bound": "fp32", "achieved": round(achieved, 4),
+                "peak": round(peak, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 5), "traffic": traffic,
+                "peak_source": f"nominal FP32 ({sm_count} SMs x 128 lanes x "
+                               f"2 x {peak_mhz:.0f} MHz; no measured FP32 "
+                               "peak on this pool)",
+                "flops_per_launch": fl, "kernel_ms": round(ms_local, 4)}
+
+    # ---- end to end through the host-buffer API
+    e2e = None
+    if not args.no_e2e:
+        pinned_trk = torch.tensor(host_trk, dtype=torch.float64).pin_memory()
+        host_in = pinned_trk.numpy()
+        out = propagator.alloc_host_results(n, cfg.max_records, pinned=True)
+        for _ in range(max(1, args.warmup)):
+            propagator.propagate_host(cfg, det, field, host_in, launch=lc,
+                                      out=out)
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        k_e2e = max(1, min(args.steps, 5))
+        for _ in range(k_e2e):
+            propagator.propagate_host(cfg, det, field, host_in, launch=lc,
+                                      out=out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        wall = (time.perf_counter() - t0) / k_e2e
+        ms_e2e = max(e0.elapsed_time(e1) / k_e2e, wall * 1e3)
+        ms_e2e = max_over_ranks(ms_e2e, world)
+        h2d = 8 * n * 8
+        rec = cfg.max_records * n * (8 + 6 * 4 + 21 * 4 + 4 + 1)
+        d2h = n * (1 + 6 * 4 + 4 + 8 * 4) + rec
+        e2e = {"value": total_tracks / (ms_e2e / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": round(ms_e2e, 3), "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_rate(15.0, cfg, args.seed, 2_000_000,
+                                     host_threads())
+        except (FileNotFoundError, OSError) as exc:
+            cpu = {"value": None, "unit": UNIT, "cores": host_threads(),
+                   "kind": "reference", "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded toy-detector muon sample)",
+            "config": {"workload": WORKLOAD, "tracks_per_gpu": n,
+                       "global_batch": total_tracks,
+                       "method": {abi.METHOD_PLAIN: "plain",
+                                  abi.METHOD_PERSISTENT: "persistent"}[method],
+                       "parallelism": f"tracks sharded over {world} GPU(s)",
+                       "l2": "per step ~1.5 GB of records written (> 126 MB "
+                             "L2): inputs are re-read from HBM"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "track_status": status.tolist(),
+            "mean_steps_per_track": round(mean_steps, 2),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------ reference arm
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref_oracle
+    from detray_b200.units import T
+    if not ref_oracle.available("f32"):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libdetray_ref_f32.so not "
+                                         "built (needs the reference checkout)"}))
+        return
+    cfg = workload_config()
+    threads = host_threads()
+    det = ref_oracle.build_toy(precision="f32")
+    field = {"kind": "const", "b": (0.0, 0.0, 2.0 * T)}
+    # size each step for ~2 s of wall time on this host
+    probe = make_tracks(20_000, args.seed + 3)
+    t0 = time.perf_counter()
+    ref_oracle.propagate(det, field, cfg, probe, n_threads=threads,
+                         abort_reasons=False)
+    rate = probe.shape[1] / (time.perf_counter() - t0)
+    n = int(min(args.tracks, max(10_000, rate * 2.0)))
+    sample = make_tracks(n, args.seed)
+    for _ in range(args.warmup):
+        ref_oracle.propagate(det, field, cfg, sample, n_threads=threads,
+                             abort_reasons=False)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref_oracle.propagate(det, field, cfg, sample, n_threads=threads,
+                             abort_reasons=False)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded toy-detector muon sample)",
+        "config": {"workload": WORKLOAD, "tracks_per_step": n,
+                   "parallelism": f"OpenMP over tracks, {threads} threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{n} tracks per step of the same workload"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,8 +1,8 @@
 """ctypes mirror of the C ABI declared in include/detray_b200/dprop.h.
 
-The structures here must match the header field by field; tests check the
-sizes against the library (``dprop_struct_sizes``).  This module only
-describes the boundary - it does not load anything by itself.
+The structures here must match the header field by field; a CPU test
+compiles the header and compares every struct size and field offset.  This
+module only describes the boundary - it does not load anything by itself.
 """
 from __future__ import annotations
 
@@ -202,6 +202,9 @@ class Results(C.Structure):
         ("rec_cov", C.c_void_p * 21),
         ("rec_path", C.c_void_p),
         ("rec_flags", C.c_void_p),
+        ("n_intersections", C.c_void_p),
+        ("n_transports", C.c_void_p),
+        ("n_material", C.c_void_p),
     ]
 
 

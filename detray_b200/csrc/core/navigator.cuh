@@ -65,6 +65,7 @@ struct nav_state {
     S external_tol;
     S direction;  // +1 forward, -1 backward
     uint8_t reason;
+    uint32_t n_isect;  // ray-surface intersections evaluated
 
     DPROP_HD void reset(uint32_t vol) {
         for (int i = 0; i < k_cache; ++i) {
@@ -78,6 +79,7 @@ struct nav_state {
         external_tol = S(0);
         direction = S(1);
         reason = e_reason_none;
+        n_isect = 0u;
     }
     DPROP_HD bool is_alive() const { return status > e_nav_unknown; }
     DPROP_HD bool finished() const { return status == e_nav_exit; }
@@ -209,6 +211,7 @@ DPROP_HD void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
     const dev_transform<S>& trf = det.transforms[sf.transform];
     const uint32_t m0 = sf.mask_begin;
     const uint32_t m1 = sf.mask_begin + sf.n_masks;
+    ++nav.n_isect;
     if (sf.shape == e_cylinder) {
         isect_point<S> ips[2];
         intersect_cylinder(ro, rd, trf, det.masks[m0].v[0], ips);
@@ -257,10 +260,11 @@ DPROP_HD void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
 template <typename S>
 DPROP_HD bool update_candidate(candidate<S>& c, const detector_view<S>& det,
                                vec3<S> ro, vec3<S> rd, const isect_cfg<S>& cfg,
-                               S external_tol) {
+                               S external_tol, uint32_t& n_isect) {
     if (c.sf == k_invalid) {
         return false;
     }
+    ++n_isect;
     const uint32_t sf_idx = c.sf;
     const dev_surface sf = det.surfaces[sf_idx];
     const dev_transform<S>& trf = det.transforms[sf.transform];
@@ -475,7 +479,7 @@ DPROP_HD bool navigator_update_impl(nav_state<S>& nav,
     const vec3<S> rd = nav.direction * trk.dir;
     if (nav.trust == e_high_trust) {
         if (!update_candidate(nav.target(), det, ro, rd, cfg.isect,
-                              nav.external_tol)) {
+                              nav.external_tol, nav.n_isect)) {
             nav.status = e_nav_unknown;
             nav.set_fair_trust();
         } else {
@@ -486,7 +490,7 @@ DPROP_HD bool navigator_update_impl(nav_state<S>& nav,
             }
             if (nav.trust == e_full_trust &&
                 update_candidate(nav.target(), det, ro, rd, cfg.isect,
-                                 nav.external_tol)) {
+                                 nav.external_tol, nav.n_isect)) {
                 return false;
             }
             nav.set_fair_trust();
@@ -497,7 +501,7 @@ DPROP_HD bool navigator_update_impl(nav_state<S>& nav,
         const int e = nav.end_index();
         for (int i = b; i < e; ++i) {
             if (!update_candidate(nav.cand[i], det, ro, rd, cfg.isect,
-                                  nav.external_tol)) {
+                                  nav.external_tol, nav.n_isect)) {
                 nav.cand[i].path = limits<S>::max();
             }
         }

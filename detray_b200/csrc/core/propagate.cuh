@@ -72,6 +72,8 @@ struct track_state {
     bound_state<S> bound;
     S q;        // particle charge (sign of q/p)
     bool heartbeat;
+    uint32_t n_transport;
+    uint32_t n_material;
 };
 
 template <typename S>
@@ -103,6 +105,8 @@ DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
     // particle hypothesis with the charge sign of the track
     ts.q = (qop < S(0)) ? S(-1) : S(1);
     ts.heartbeat = false;
+    ts.n_transport = 0u;
+    ts.n_material = 0u;
 }
 
 // Run the actor chain once (propagator.hpp:308).
@@ -144,6 +148,7 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
                 const dev_surface dep = det.surfaces[b.sf];
                 S G[4][5];
                 full_jacobian(det, b, dep, dst, st, current_dtds(st, field), G);
+                ++ts.n_transport;
                 if (fabs(st.path_length) > 0.) {
                     st.jac.reset();
                 }
@@ -165,6 +170,7 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
         bool success = false;
         if (cfg.act.use_interactor && has_material) {
             success = interact(det, dst, b, cfg.act, ts.q, nav.direction);
+            ts.n_material += success ? 1u : 0u;
         }
         // parameter_setter
         if (success) {

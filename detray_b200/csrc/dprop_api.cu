@@ -137,6 +137,9 @@ struct io_ptrs {
     float* rec_cov[21];
     float* rec_path;
     uint8_t* rec_flags;
+    uint32_t* n_isect;
+    uint32_t* n_transport;
+    uint32_t* n_material;
 };
 
 template <typename In>
@@ -165,6 +168,9 @@ io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
     }
     io.rec_path = static_cast<float*>(r.rec_path);
     io.rec_flags = r.rec_flags;
+    io.n_isect = r.n_intersections;
+    io.n_transport = r.n_transports;
+    io.n_material = r.n_material;
     return io;
 }
 
@@ -207,6 +213,9 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     if (io.n_records) io.n_records[t] = rec.count;
     if (io.n_steps) io.n_steps[t] = ts.step.n_steps;
     if (io.n_trials) io.n_trials[t] = ts.step.n_trials;
+    if (io.n_isect) io.n_isect[t] = ts.nav.n_isect;
+    if (io.n_transport) io.n_transport[t] = ts.n_transport;
+    if (io.n_material) io.n_material[t] = ts.n_material;
     if (io.path_length) io.path_length[t] = static_cast<float>(ts.step.path_length);
     const float fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
                           ts.step.time,  ts.step.dir.x, ts.step.dir.y,
@@ -517,7 +526,7 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
     const uint64_t cap = cfg->max_records;
     // device scratch: inputs (8 doubles), per-track outputs, records
     const size_t in_bytes = 8 * n * sizeof(double);
-    const size_t trk_bytes = n * (1 + 3 * 4 + 4 + 8 * 4);
+    const size_t trk_bytes = n * (1 + 6 * 4 + 4 + 8 * 4) + 16 * 256;
     const size_t rec_bytes = cap * n * (8 + 6 * 4 + 21 * 4 + 4 + 1);
     s = ensure_scratch(in_bytes + trk_bytes + rec_bytes + 4096);
     if (s != DPROP_OK) {
@@ -561,6 +570,9 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
     }
     dr.rec_path = results->rec_path ? take(4 * cap * n) : nullptr;
     dr.rec_flags = results->rec_flags ? reinterpret_cast<uint8_t*>(take(cap * n)) : nullptr;
+    dr.n_intersections = results->n_intersections ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
+    dr.n_transports = results->n_transports ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
+    dr.n_material = results->n_material ? reinterpret_cast<uint32_t*>(take(4 * n)) : nullptr;
 
     dprop_tracks dt{};
     for (int i = 0; i < 3; ++i) {
@@ -597,6 +609,9 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
     }
     if ((s = d2h(results->rec_path, dr.rec_path, 4 * cap * n)) != DPROP_OK) return s;
     if ((s = d2h(results->rec_flags, dr.rec_flags, cap * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_intersections, dr.n_intersections, 4 * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_transports, dr.n_transports, 4 * n)) != DPROP_OK) return s;
+    if ((s = d2h(results->n_material, dr.n_material, 4 * n)) != DPROP_OK) return s;
     DPROP_CUDA(cudaStreamSynchronize(0));
     return DPROP_OK;
 }

@@ -183,8 +183,14 @@ def alloc_device_results(n: int, max_records: int, device="cuda",
         "n_trials": torch.empty(n, dtype=torch.int32, device=device),
         "path_length": torch.empty(n, **f32),
         "final_free": torch.empty((8, n), **f32),
+        "n_intersections": torch.empty(n, dtype=torch.int32, device=device),
+        "n_transports": torch.empty(n, dtype=torch.int32, device=device),
+        "n_material": torch.empty(n, dtype=torch.int32, device=device),
     }
     r = abi.Results()
+    r.n_intersections = t["n_intersections"].data_ptr()
+    r.n_transports = t["n_transports"].data_ptr()
+    r.n_material = t["n_material"].data_ptr()
     r.status = t["status"].data_ptr()
     r.n_records = t["n_records"].data_ptr()
     r.n_steps = t["n_steps"].data_ptr()
@@ -276,6 +282,9 @@ def alloc_host_results(n: int, max_records: int, pinned: bool = False,
         "rec_bound": empty((6, max_records, n), f32),
         "rec_path": empty((max_records, n), f32),
         "rec_flags": empty((max_records, n), u8),
+        "n_intersections": empty((n,), i32),
+        "n_transports": empty((n,), i32),
+        "n_material": empty((n,), i32),
     }
     if with_cov:
         res["rec_cov"] = empty((21, max_records, n), f32)
@@ -295,6 +304,9 @@ def alloc_host_results(n: int, max_records: int, pinned: bool = False,
             r.rec_cov[i] = res["rec_cov"][i].ctypes.data
     r.rec_path = res["rec_path"].ctypes.data
     r.rec_flags = res["rec_flags"].ctypes.data
+    r.n_intersections = res["n_intersections"].ctypes.data
+    r.n_transports = res["n_transports"].ctypes.data
+    r.n_material = res["n_material"].ctypes.data
     return res, r
 
 

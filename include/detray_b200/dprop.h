@@ -254,6 +254,11 @@ typedef struct dprop_results {
     void* rec_path;           /* [max_records * n]; may be NULL                 */
     uint8_t* rec_flags;       /* [max_records * n]; bit0: transported (bound +
                                   cov valid), bit1: portal, bit2: material     */
+    uint32_t* n_intersections;/* [n] ray-surface intersections evaluated;
+                                  may be NULL                                  */
+    uint32_t* n_transports;   /* [n] covariance transports to a surface;
+                                  may be NULL                                  */
+    uint32_t* n_material;     /* [n] material interactions; may be NULL        */
 } dprop_results;
 
 /* Launch shape; zero fields pick the library defaults / autotuned values. */
@@ -306,9 +311,10 @@ dprop_status dprop_propagate(const dprop_config* cfg,
                              const dprop_results* results, uint64_t n_tracks,
                              void* stream);
 
-/* Same, with host double-precision inputs and host outputs (the result
- * pointers then point to host memory, float fields as double).  Copies in,
- * propagates, copies out and synchronises. */
+/* Same, with host inputs (double precision, as dprop_tracks) and host
+ * outputs (the result pointers then point to host memory, with the same
+ * element types as on the device).  Copies in, propagates, copies out and
+ * synchronises.  Uses library-owned device scratch, grown on demand. */
 dprop_status dprop_propagate_host(const dprop_config* cfg,
                                   const dprop_launch* launch,
                                   const dprop_detector* det,

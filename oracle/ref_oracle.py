@@ -232,6 +232,9 @@ def alloc_results(n: int, max_records: int) -> tuple[dict, abi.Results]:
         "rec_cov": np.zeros((21, max_records, n), dtype=np.float64),
         "rec_path": np.zeros((max_records, n), dtype=np.float64),
         "rec_flags": np.zeros((max_records, n), dtype=np.uint8),
+        "n_intersections": np.zeros(n, dtype=np.uint32),
+        "n_transports": np.zeros(n, dtype=np.uint32),
+        "n_material": np.zeros(n, dtype=np.uint32),
     }
     r = abi.Results()
     r.status = res["status"].ctypes.data
@@ -248,6 +251,9 @@ def alloc_results(n: int, max_records: int) -> tuple[dict, abi.Results]:
         r.rec_cov[i] = res["rec_cov"][i].ctypes.data
     r.rec_path = res["rec_path"].ctypes.data
     r.rec_flags = res["rec_flags"].ctypes.data
+    r.n_intersections = res["n_intersections"].ctypes.data
+    r.n_transports = res["n_transports"].ctypes.data
+    r.n_material = res["n_material"].ctypes.data
     return res, r
 
 

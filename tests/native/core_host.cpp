@@ -102,6 +102,9 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         if (out->n_records) out->n_records[t] = rec.count;
         if (out->n_steps) out->n_steps[t] = ts.step.n_steps;
         if (out->n_trials) out->n_trials[t] = ts.step.n_trials;
+        if (out->n_intersections) out->n_intersections[t] = ts.nav.n_isect;
+        if (out->n_transports) out->n_transports[t] = ts.n_transport;
+        if (out->n_material) out->n_material[t] = ts.n_material;
         if (out->path_length)
             static_cast<double*>(out->path_length)[t] = ts.step.path_length;
         const double fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
