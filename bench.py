@@ -54,6 +54,8 @@ def parse_args():
                    help="tracks per GPU per step")
     p.add_argument("--method", choices=["plain", "persistent", "auto"],
                    default="auto")
+    p.add_argument("--no-sort", action="store_true",
+                   help="propagate in input order instead of direction order")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--seed", type=int, default=20241203)
@@ -233,7 +235,7 @@ def run_ours(args):
     res = propagator.alloc_device_results(n, cfg.max_records, dev)
     method = {"plain": abi.METHOD_PLAIN, "persistent": abi.METHOD_PERSISTENT,
               "auto": abi.METHOD_PLAIN}[args.method]
-    lc = propagator.make_launch(method=method)
+    lc = propagator.make_launch(method=method, sort_tracks=int(not args.no_sort))
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -348,6 +350,7 @@ def run_ours(args):
                        "global_batch": total_tracks,
                        "method": {abi.METHOD_PLAIN: "plain",
                                   abi.METHOD_PERSISTENT: "persistent"}[method],
+                       "sort_tracks": int(not args.no_sort),
                        "parallelism": f"tracks sharded over {world} GPU(s)",
                        "l2": "per step ~1.5 GB of records written (> 126 MB "
                              "L2): inputs are re-read from HBM"},

@@ -213,7 +213,8 @@ class Launch(C.Structure):
         ("method", C.c_uint32),
         ("block_size", C.c_uint32),
         ("ctas_per_sm", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("sort_tracks", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 

@@ -19,9 +19,20 @@
 #if defined(__CUDACC__)
 #define DPROP_HD __host__ __device__ __forceinline__
 #define DPROP_D __device__ __forceinline__
+// Infrequently taken paths (volume re-initialisation, covariance transport,
+// material).  Inlined by default: measured on B200, keeping them out of line
+// forces the track state into the stack frame and costs more than the
+// instruction-cache locality it buys.  -DDPROP_OUTLINE_COLD keeps them out
+// of line.
+#if defined(DPROP_OUTLINE_COLD)
+#define DPROP_HD_COLD __host__ __device__ __noinline__
+#else
+#define DPROP_HD_COLD __host__ __device__ __forceinline__
+#endif
 #else
 #define DPROP_HD inline
 #define DPROP_D inline
+#define DPROP_HD_COLD inline
 #endif
 
 namespace dprop {

@@ -403,7 +403,7 @@ DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S>& det,
 
 // --------------------------------------------------- local_navigation
 template <typename S>
-DPROP_HD void local_navigation(nav_state<S>& nav, const detector_view<S>& det,
+DPROP_HD_COLD void local_navigation(nav_state<S>& nav, const detector_view<S>& det,
                                const track_view<S>& trk, const nav_cfg<S>& cfg,
                                bool resolve_overstepping) {
     const dev_volume vol = det.volumes[nav.volume];
@@ -450,7 +450,7 @@ DPROP_HD void volume_switch(nav_state<S>& nav, const detector_view<S>& det,
 
 // ------------------------------------------------------- init_loose_cfg
 template <typename S>
-DPROP_HD void init_loose(nav_state<S>& nav, const detector_view<S>& det,
+DPROP_HD_COLD void init_loose(nav_state<S>& nav, const detector_view<S>& det,
                          const track_view<S>& trk, nav_cfg<S> loose) {
     const S a = S(100) * loose.isect.overstep_tol;
     const S b = S(-10) * loose.isect.max_mask_tol;
@@ -468,34 +468,44 @@ DPROP_HD void navigator_init(nav_state<S>& nav, const detector_view<S>& det,
     local_navigation(nav, det, trk, cfg, false);
 }
 
-// caching_navigator::update_impl; returns whether the volume was
-// (re-)initialised
+// caching_navigator::update_impl, high-trust branch: re-intersect only the
+// target.  Returns true if the update is complete (update_impl returned
+// there); false if trust dropped to fair and the cache must be re-evaluated.
 template <typename S>
-DPROP_HD bool navigator_update_impl(nav_state<S>& nav,
-                                    const detector_view<S>& det,
-                                    const track_view<S>& trk,
-                                    const nav_cfg<S>& cfg) {
+DPROP_HD bool high_trust_update(nav_state<S>& nav, const detector_view<S>& det,
+                                const track_view<S>& trk,
+                                const nav_cfg<S>& cfg) {
     const vec3<S> ro = trk.pos;
     const vec3<S> rd = nav.direction * trk.dir;
-    if (nav.trust == e_high_trust) {
-        if (!update_candidate(nav.target(), det, ro, rd, cfg.isect,
-                              nav.external_tol, nav.n_isect)) {
-            nav.status = e_nav_unknown;
-            nav.set_fair_trust();
-        } else {
-            update_status(nav, cfg);
-            DPROP_NAV_TRACE(nav, "Update complete: high trust: ", trk.pos);
-            if (nav.status == e_towards_object || nav.is_on_portal()) {
-                return false;
-            }
-            if (nav.trust == e_full_trust &&
-                update_candidate(nav.target(), det, ro, rd, cfg.isect,
-                                 nav.external_tol, nav.n_isect)) {
-                return false;
-            }
-            nav.set_fair_trust();
-        }
+    if (!update_candidate(nav.target(), det, ro, rd, cfg.isect,
+                          nav.external_tol, nav.n_isect)) {
+        nav.status = e_nav_unknown;
+        nav.set_fair_trust();
+        return false;
     }
+    update_status(nav, cfg);
+    DPROP_NAV_TRACE(nav, "Update complete: high trust: ", trk.pos);
+    if (nav.status == e_towards_object || nav.is_on_portal()) {
+        return true;
+    }
+    if (nav.trust == e_full_trust &&
+        update_candidate(nav.target(), det, ro, rd, cfg.isect,
+                         nav.external_tol, nav.n_isect)) {
+        return true;
+    }
+    nav.set_fair_trust();
+    return false;
+}
+
+// caching_navigator::update_impl, fair- and no-trust branches.  Returns
+// whether the volume was (re-)initialised.
+template <typename S>
+DPROP_HD_COLD bool fair_or_no_trust_update(nav_state<S>& nav,
+                                           const detector_view<S>& det,
+                                           const track_view<S>& trk,
+                                           const nav_cfg<S>& cfg) {
+    const vec3<S> ro = trk.pos;
+    const vec3<S> rd = nav.direction * trk.dir;
     if (nav.trust == e_fair_trust && !nav.cache_exhausted()) {
         const int b = nav.begin_index();
         const int e = nav.end_index();
@@ -539,15 +549,12 @@ DPROP_HD bool navigator_update_impl(nav_state<S>& nav,
     return false;
 }
 
-// navigator_base::update
+// Volume switch and loose re-initialisation after the trust-level update
+// (navigator_base::update, navigator_base.hpp:121-140).
 template <typename S>
-DPROP_HD bool navigator_update(nav_state<S>& nav, const detector_view<S>& det,
-                               const track_view<S>& trk,
-                               const nav_cfg<S>& cfg) {
-    if (nav.trust == e_full_trust) {
-        return false;
-    }
-    bool is_init = navigator_update_impl(nav, det, trk, cfg);
+DPROP_HD_COLD bool finish_update(nav_state<S>& nav, const detector_view<S>& det,
+                                 const track_view<S>& trk,
+                                 const nav_cfg<S>& cfg, bool is_init) {
     if (nav.is_on_portal()) {
         volume_switch(nav, det, trk, cfg);
         is_init = true;
@@ -558,6 +565,27 @@ DPROP_HD bool navigator_update(nav_state<S>& nav, const detector_view<S>& det,
     if (nav.trust != e_full_trust || nav.cache_exhausted()) {
         is_init = true;
         init_loose(nav, det, trk, cfg);
+    }
+    return is_init;
+}
+
+// navigator_base::update
+template <typename S>
+DPROP_HD bool navigator_update(nav_state<S>& nav, const detector_view<S>& det,
+                               const track_view<S>& trk,
+                               const nav_cfg<S>& cfg) {
+    if (nav.trust == e_full_trust) {
+        return false;
+    }
+    bool is_init = false;
+    if (nav.trust == e_high_trust && high_trust_update(nav, det, trk, cfg)) {
+        is_init = false;
+    } else {
+        is_init = fair_or_no_trust_update(nav, det, trk, cfg);
+    }
+    if (nav.is_on_portal() || nav.trust != e_full_trust ||
+        nav.cache_exhausted()) {
+        return finish_update(nav, det, trk, cfg, is_init);
     }
     return is_init;
 }

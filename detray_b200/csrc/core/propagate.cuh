@@ -109,29 +109,16 @@ DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
     ts.n_material = 0u;
 }
 
-// Run the actor chain once (propagator.hpp:308).
+// The surface actors: parameter_transporter, its observers (material
+// interactor, parameter setter) and the surface recorder.
 template <typename S>
-DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
-                         const field_view<S>& field, const prop_cfg<S>& cfg,
-                         record_sink<S>& rec) {
+DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
+                                      const detector_view<S>& det,
+                                      const field_view<S>& field,
+                                      const prop_cfg<S>& cfg,
+                                      record_sink<S>& rec) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
-
-    // pathlimit_aborter
-    if (!nav.finished()) {
-        const S step_limit =
-            cfg.act.path_limit - static_cast<S>(fabs(st.abs_path_length));
-        if (step_limit <= S(0)) {
-            nav.abort(e_reason_path_limit);
-            ts.heartbeat = false;
-        }
-        st.constraint = min_(st.constraint, fabs(step_limit));
-    }
-
-    // parameter_transporter and its observers
-    if (!nav.is_on_surface()) {
-        return;
-    }
     const uint32_t cur_sf = nav.current().sf;
     const dev_surface dst = det.surfaces[cur_sf];
     const bool on_sensitive =
@@ -198,6 +185,30 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
         }
         rec.write(dst.barcode, ts.bound.v, ts.bound.cov,
                   static_cast<S>(st.path_length), fl);
+    }
+}
+
+// Run the actor chain once (propagator.hpp:308).
+template <typename S>
+DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
+                         const field_view<S>& field, const prop_cfg<S>& cfg,
+                         record_sink<S>& rec) {
+    step_state<S>& st = ts.step;
+    nav_state<S>& nav = ts.nav;
+
+    // pathlimit_aborter
+    if (!nav.finished()) {
+        const S step_limit =
+            cfg.act.path_limit - static_cast<S>(fabs(st.abs_path_length));
+        if (step_limit <= S(0)) {
+            nav.abort(e_reason_path_limit);
+            ts.heartbeat = false;
+        }
+        st.constraint = min_(st.constraint, fabs(step_limit));
+    }
+    // parameter_transporter and observers only act on surfaces
+    if (nav.is_on_surface()) {
+        run_surface_actors(ts, det, field, cfg, rec);
     }
 }
 

@@ -14,6 +14,8 @@
 // Both write the slot-major records of dprop_results.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -121,6 +123,80 @@ dprop_status ensure_scratch(size_t bytes) {
 }
 
 unsigned int* g_queue_counter = nullptr;
+
+// Library-owned device scratch of the direction sort (grow-only).
+struct sort_scratch {
+    void* buf{nullptr};
+    size_t bytes{0};
+};
+sort_scratch g_sort;
+
+// Key of the track direction: 10 bits of theta (major) and 10 bits of phi.
+template <typename In>
+__global__ void direction_key_kernel(const In* __restrict__ dx,
+                                     const In* __restrict__ dy,
+                                     const In* __restrict__ dz, uint64_t n,
+                                     uint32_t* __restrict__ keys,
+                                     uint32_t* __restrict__ idx) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const float x = static_cast<float>(dx[i]);
+    const float y = static_cast<float>(dy[i]);
+    const float z = static_cast<float>(dz[i]);
+    const float theta = atan2f(sqrtf(x * x + y * y), z);
+    const float phi = atan2f(y, x);
+    int tb = static_cast<int>(theta * (1024.f / 3.14159265f));
+    int pb = static_cast<int>((phi + 3.14159265f) * (1024.f / 6.2831853f));
+    tb = tb < 0 ? 0 : (tb > 1023 ? 1023 : tb);
+    pb = pb < 0 ? 0 : (pb > 1023 ? 1023 : pb);
+    keys[i] = (static_cast<uint32_t>(tb) << 10) | static_cast<uint32_t>(pb);
+    idx[i] = static_cast<uint32_t>(i);
+}
+
+// Sort track indices by direction key; returns the device order array.
+template <typename In>
+dprop_status direction_order(const In* dx, const In* dy, const In* dz,
+                             uint64_t n, cudaStream_t stream,
+                             const uint32_t** order) {
+    if (n > 0x7fffffffull) {
+        return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
+    }
+    const int ni = static_cast<int>(n);
+    size_t temp_bytes = 0;
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), ni, 0, 20, stream));
+    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
+    const size_t need = 4 * arr + temp_bytes + 256;
+    if (g_sort.bytes < need) {
+        if (g_sort.buf) {
+            DPROP_CUDA(cudaStreamSynchronize(stream));
+            cudaFree(g_sort.buf);
+            g_sort.buf = nullptr;
+            g_sort.bytes = 0;
+        }
+        DPROP_CUDA(cudaMalloc(&g_sort.buf, need));
+        g_sort.bytes = need;
+    }
+    char* p = static_cast<char*>(g_sort.buf);
+    uint32_t* keys_in = reinterpret_cast<uint32_t*>(p);
+    uint32_t* keys_out = reinterpret_cast<uint32_t*>(p + arr);
+    uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + 2 * arr);
+    uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
+    void* temp = p + 4 * arr;
+    const unsigned int grid = static_cast<unsigned int>((n + 255) / 256);
+    direction_key_kernel<In><<<grid, 256, 0, stream>>>(dx, dy, dz, n, keys_in,
+                                                       idx_in);
+    DPROP_CUDA(cudaGetLastError());
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in,
+                                               keys_out, idx_in, idx_out, ni,
+                                               0, 20, stream));
+    *order = idx_out;
+    return DPROP_OK;
+}
 
 // Device pointers of the inputs/outputs, by value into the kernels
 template <typename In>
@@ -232,11 +308,12 @@ __global__ void __launch_bounds__(k_plain_block)
     propagate_plain_kernel(const detector_view<float> det,
                            const field_view<float> field,
                            const prop_cfg<float> cfg, const io_ptrs<In> io,
-                           uint64_t n) {
-    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= n) {
+                           uint64_t n, const uint32_t* __restrict__ order) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
         return;
     }
+    const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
     run_one(t, n, det, field, cfg, io);
 }
 
@@ -245,14 +322,26 @@ __global__ void __launch_bounds__(k_plain_block)
     propagate_persistent_kernel(const detector_view<float> det,
                                 const field_view<float> field,
                                 const prop_cfg<float> cfg, const io_ptrs<In> io,
-                                uint64_t n, unsigned int* queue) {
-    // each thread pulls the next unprocessed track until the queue is empty
+                                uint64_t n, unsigned int* queue,
+                                const uint32_t* __restrict__ order) {
+    // each warp pulls the next 32 unprocessed tracks once all of its lanes
+    // are done, so that the lanes of a warp start their tracks together
+    const unsigned int lane = threadIdx.x & 31u;
     while (true) {
-        const unsigned int t = atomicAdd(queue, 1u);
-        if (t >= n) {
+        unsigned int base = 0u;
+        if (lane == 0u) {
+            base = atomicAdd(queue, 32u);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) {
             break;
         }
-        run_one(static_cast<uint64_t>(t), n, det, field, cfg, io);
+        const uint64_t i = static_cast<uint64_t>(base) + lane;
+        if (i < n) {
+            const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
+            run_one(t, n, det, field, cfg, io);
+        }
+        __syncwarp();
     }
 }
 
@@ -265,6 +354,14 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     }
     const prop_cfg<float> cfg = make_prop_cfg<float>(c);
     const uint32_t method = launch_cfg ? launch_cfg->method : DPROP_METHOD_PLAIN;
+    const uint32_t* order = nullptr;
+    if (launch_cfg && launch_cfg->sort_tracks) {
+        const dprop_status s = direction_order<In>(io.trk[4], io.trk[5],
+                                                   io.trk[6], n, stream, &order);
+        if (s != DPROP_OK) {
+            return s;
+        }
+    }
     if (method == DPROP_METHOD_PERSISTENT) {
         if (n > 0xffffff00ull) {
             return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
@@ -287,12 +384,12 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
         }
         propagate_persistent_kernel<In><<<static_cast<unsigned int>(grid),
                                           k_plain_block, 0, stream>>>(
-            det->view(), field->view, cfg, io, n, g_queue_counter);
+            det->view(), field->view, cfg, io, n, g_queue_counter, order);
     } else {
         const uint64_t grid = (n + k_plain_block - 1) / k_plain_block;
         propagate_plain_kernel<In><<<static_cast<unsigned int>(grid),
                                      k_plain_block, 0, stream>>>(
-            det->view(), field->view, cfg, io, n);
+            det->view(), field->view, cfg, io, n, order);
     }
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;

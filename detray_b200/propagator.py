@@ -156,11 +156,12 @@ class Field:
 
 
 def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
-                ctas_per_sm: int = 0) -> abi.Launch:
+                ctas_per_sm: int = 0, sort_tracks: int = 0) -> abi.Launch:
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
     lc.ctas_per_sm = ctas_per_sm
+    lc.sort_tracks = sort_tracks
     return lc
 
 

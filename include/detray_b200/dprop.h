@@ -270,9 +270,13 @@ typedef enum dprop_method {
 
 typedef struct dprop_launch {
     uint32_t method;             /* dprop_method                               */
-    uint32_t block_size;         /* threads per CTA                            */
+    uint32_t block_size;         /* threads per CTA (0: default)               */
     uint32_t ctas_per_sm;        /* persistent grid = SMs * ctas_per_sm         */
-    uint32_t reserved[5];
+    uint32_t sort_tracks;        /* 1: process tracks ordered by direction
+                                    (theta, phi) so that the lanes of a warp
+                                    follow similar paths; results are still
+                                    written at each track's input position    */
+    uint32_t reserved[4];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */

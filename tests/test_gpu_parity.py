@@ -94,3 +94,51 @@ def test_host_api_equals_device_api(torch_cuda):
     m = int(a["n_records"].max())
     assert np.array_equal(a["rec_barcode"][:m], b["rec_barcode"][:m].view(np.uint64))
     assert np.allclose(a["rec_bound"][:, :m], b["rec_bound"][:, :m], atol=0, rtol=0)
+
+
+def test_sorted_order_equals_input_order(torch_cuda):
+    """Processing tracks in direction order changes only which tracks share
+    a warp; every track's result, written at its input position, is
+    bit-identical."""
+    det, field, cfg, trk = _setup("toy")
+    a = _run_device(torch_cuda, det, field, cfg, trk, method=0)
+    from detray_b200 import propagator
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+    for method in (0, 1):
+        lc = propagator.make_launch(method=method, sort_tracks=1)
+        res = propagator.propagate(cfg, det, field, dev, launch=lc)
+        torch_cuda.cuda.synchronize()
+        b = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+        for key in ["status", "n_records", "n_trials", "path_length",
+                    "final_free"]:
+            assert np.array_equal(a[key], b[key]), (method, key)
+        m = int(a["n_records"].max())
+        valid = np.arange(m)[:, None] < a["n_records"][None, :]
+        assert np.array_equal(a["rec_bound"][:, :m][:, valid],
+                              b["rec_bound"][:, :m][:, valid])
+        assert np.array_equal(a["rec_cov"][:, :m][:, valid],
+                              b["rec_cov"][:, :m][:, valid])
+
+
+def test_empty_batch_and_invalid_arguments(torch_cuda):
+    """n = 0 is a no-op; NULL detector / bad config are rejected with an
+    error status, nothing is launched."""
+    import ctypes as C
+
+    from detray_b200 import abi, propagator
+    det, field, cfg, trk = _setup("telescope")
+    dev = torch_cuda.zeros((8, 0), dtype=torch_cuda.float32, device="cuda")
+    res = propagator.alloc_device_results(0, cfg.max_records, "cuda")
+    lib = propagator.load_library()
+    ts = propagator.tracks_struct(torch_cuda.zeros((8, 1), device="cuda"))
+    rc = lib.dprop_propagate(C.byref(cfg), None, det.handle, field.handle,
+                             C.byref(ts), C.byref(res.struct), 0, None)
+    assert rc == abi.DPROP_OK
+    rc = lib.dprop_propagate(C.byref(cfg), None, None, field.handle,
+                             C.byref(ts), C.byref(res.struct), 1, None)
+    assert rc == abi.DPROP_E_INVALID
+    bad = abi.make_config(use_field_gradient=1)
+    rc = lib.dprop_propagate(C.byref(bad), None, det.handle, field.handle,
+                             C.byref(ts), C.byref(res.struct), 1, None)
+    assert rc == abi.DPROP_E_UNSUPPORTED
+    assert "gradient" in lib.dprop_last_error().decode()
