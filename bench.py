@@ -355,7 +355,9 @@ def run_ours(args):
                        "l2": "per step ~1.5 GB of records written (> 126 MB "
                              "L2): inputs are re-read from HBM"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-            "gpu_launches": args.steps,
+            # our kernels per step: the propagation kernel, plus the direction
+            # key kernel when sorting (the radix sort itself is CUB's)
+            "gpu_launches": args.steps * (1 + int(not args.no_sort)),
             "clocks": clk,
             "track_status": status.tolist(),
             "mean_steps_per_track": round(mean_steps, 2),

@@ -591,6 +591,9 @@ dprop_status dprop_propagate(const dprop_config* cfg, const dprop_launch* lc,
     if (!det || !field || !tracks || !results) {
         return fail(DPROP_E_INVALID, "propagate: NULL argument");
     }
+    if (n == 0) {
+        return DPROP_OK;
+    }
     for (int i = 0; i < 3; ++i) {
         if (!tracks->pos[i] || !tracks->dir[i]) {
             return fail(DPROP_E_INVALID, "propagate: missing track array");
@@ -714,3 +717,4 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
 }
 
 }  // extern "C"
+
