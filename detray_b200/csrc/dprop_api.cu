@@ -18,6 +18,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -718,3 +719,123 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
 
 }  // extern "C"
 
+// ===================================================== allocation-free path
+// dprop_propagate_noalloc: the direction-sorted plain propagation with its
+// sort scratch in a fixed device array instead of library allocations.
+namespace {
+
+// Layout of the fixed scratch: four track-index-sized arrays (sort keys and
+// indices, in and out) followed by the radix-sort temporary storage.
+constexpr size_t k_noalloc_array_bytes =
+    static_cast<size_t>(DPROP_NOALLOC_MAX_TRACKS) * sizeof(uint32_t);
+constexpr size_t k_noalloc_temp_offset = 4 * k_noalloc_array_bytes;
+constexpr size_t k_noalloc_temp_bytes =
+    static_cast<size_t>(DPROP_NOALLOC_SCRATCH_BYTES) - k_noalloc_temp_offset;
+static_assert(k_noalloc_temp_offset < DPROP_NOALLOC_SCRATCH_BYTES,
+              "no-alloc scratch too small for the sort arrays");
+
+// The scratch itself.  In host code this name is only a stand-in for the
+// symbol: its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char
+    g_noalloc_scratch[DPROP_NOALLOC_SCRATCH_BYTES];
+
+constexpr int k_noalloc_max_devices = 64;
+void* g_noalloc_device_ptr[k_noalloc_max_devices] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch on the current device, looked up once per
+// device (the lookup may load the module, so it must not run inside a
+// stream capture).
+dprop_status noalloc_scratch(void** out) {
+    int dev = 0;
+    DPROP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= k_noalloc_max_devices) {
+        return fail(DPROP_E_INVALID, "propagate_noalloc: device index out of range");
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_device_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        }
+        g_noalloc_device_ptr[dev] = p;
+    }
+    *out = g_noalloc_device_ptr[dev];
+    return DPROP_OK;
+}
+
+}  // namespace
+
+extern "C" dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
+                                                const dprop_detector* det,
+                                                const dprop_field* field,
+                                                const dprop_tracks* tracks,
+                                                const dprop_results* results,
+                                                uint64_t n, void* stream_ptr) {
+    dprop_status s = check_config(cfg);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    if (!det || !field || !tracks || !results) {
+        return fail(DPROP_E_INVALID, "propagate_noalloc: NULL argument");
+    }
+    if (n > DPROP_NOALLOC_MAX_TRACKS) {
+        return fail(DPROP_E_INVALID,
+                    "propagate_noalloc: " + std::to_string(n) +
+                        " tracks exceed the fixed scratch capacity of " +
+                        std::to_string(DPROP_NOALLOC_MAX_TRACKS) +
+                        " tracks per call; split the batch");
+    }
+    if (n == 0) {
+        return DPROP_OK;
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (!tracks->pos[i] || !tracks->dir[i]) {
+            return fail(DPROP_E_INVALID, "propagate_noalloc: missing track array");
+        }
+    }
+    if (!tracks->time || !tracks->qop || !results->status) {
+        return fail(DPROP_E_INVALID,
+                    "propagate_noalloc: missing track/status array");
+    }
+    void* scratch = nullptr;
+    s = noalloc_scratch(&scratch);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const int ni = static_cast<int>(n);
+    size_t temp_bytes = 0;
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), ni, 0, 20, stream));
+    if (temp_bytes > k_noalloc_temp_bytes) {
+        return fail(DPROP_E_INVALID,
+                    "propagate_noalloc: radix-sort storage exceeds the fixed "
+                    "scratch");
+    }
+    char* base = static_cast<char*>(scratch);
+    uint32_t* keys_in = reinterpret_cast<uint32_t*>(base);
+    uint32_t* keys_out = reinterpret_cast<uint32_t*>(base + k_noalloc_array_bytes);
+    uint32_t* idx_in = reinterpret_cast<uint32_t*>(base + 2 * k_noalloc_array_bytes);
+    uint32_t* idx_out = reinterpret_cast<uint32_t*>(base + 3 * k_noalloc_array_bytes);
+    void* temp = base + k_noalloc_temp_offset;
+
+    const io_ptrs<float> io = make_io<float>(*tracks, *results);
+    const unsigned int key_grid = static_cast<unsigned int>((n + 255) / 256);
+    direction_key_kernel<float><<<key_grid, 256, 0, stream>>>(
+        io.trk[4], io.trk[5], io.trk[6], n, keys_in, idx_in);
+    DPROP_CUDA(cudaGetLastError());
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in,
+                                               keys_out, idx_in, idx_out, ni,
+                                               0, 20, stream));
+    const prop_cfg<float> pc = make_prop_cfg<float>(*cfg);
+    const unsigned int grid =
+        static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
+    propagate_plain_kernel<float><<<grid, k_plain_block, 0, stream>>>(
+        det->view(), field->view, pc, io, n, idx_out);
+    DPROP_CUDA(cudaGetLastError());
+    return DPROP_OK;
+}

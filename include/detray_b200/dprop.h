@@ -327,6 +327,38 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
                                   const dprop_results* results,
                                   uint64_t n_tracks);
 
+/* ------------------------------------------------- allocation-free variant
+ * dprop_propagate_noalloc has no counterpart in the reference.
+ *
+ * It is for callers that must not have the library allocate device memory
+ * while they run: an event-processing framework that hands all device memory
+ * to its own pool allocator, a trigger or other latency-bound loop in which a
+ * cudaMalloc or cudaFree (which can synchronise the whole device) is not
+ * acceptable, or an application that fixes its device-memory budget up
+ * front.  It does what dprop_propagate does with sort_tracks = 1 and the
+ * plain one-thread-per-track kernel, but the scratch the direction sort needs
+ * (keys, indices, radix-sort temporary storage) lives in one fixed array
+ * compiled into the library: DPROP_NOALLOC_SCRATCH_BYTES on every GPU that
+ * loads the library, held until the process exits.  Inputs and outputs are
+ * device buffers passed by the caller, as for dprop_propagate.
+ *
+ *  - At most DPROP_NOALLOC_MAX_TRACKS tracks per call; a larger batch is
+ *    rejected with DPROP_E_INVALID (split it into several calls).
+ *  - The first call on a device looks up that device's copy of the array;
+ *    make that first call before capturing any stream into a CUDA graph.
+ *  - Every call uses the same array: calls whose GPU work overlaps (for
+ *    instance on two streams at once) race on it, so the caller must order
+ *    them, e.g. by issuing them on one stream.
+ */
+#define DPROP_NOALLOC_MAX_TRACKS 262144u
+#define DPROP_NOALLOC_SCRATCH_BYTES (6u * 1024u * 1024u)
+dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
+                                     const dprop_detector* det,
+                                     const dprop_field* field,
+                                     const dprop_tracks* tracks,
+                                     const dprop_results* results,
+                                     uint64_t n_tracks, void* stream);
+
 /* Number of surfaces / volumes held by a detector (for callers sizing output). */
 dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
                                  uint32_t* n_surfaces);
