@@ -27,7 +27,7 @@ DPROP_HD void clamp_locate(S x, S lo, S step_inv, uint32_t n, uint32_t& i0,
     }
     S u = (x - lo) * step_inv;
     const S umax = static_cast<S>(n - 1u);
-    u = u < S(0) ? S(0) : u;
+    u = (u >= S(0)) ? u : S(0);  // also maps NaN onto the first node
     u = u > umax ? umax : u;
     S fl = floor(u);
     fl = fl > umax - S(1) ? umax - S(1) : fl;

@@ -46,6 +46,7 @@ enum abort_reason : uint8_t {
     e_reason_path_limit = 1,
     e_reason_stalled = 2,
     e_reason_no_surface = 3,
+    e_reason_nonfinite = 4,
 };
 
 template <typename S>
@@ -56,7 +57,11 @@ struct nav_cfg {
 
 template <typename S>
 struct nav_state {
-    candidate<S> cand[k_cache];
+    // k_cache candidates plus one sentinel slot: when the last cached
+    // candidate is reached the next index points one past the cache, and a
+    // read there (which the reference does on its fixed-size array) finds
+    // an unreachable candidate instead of leaving the state.
+    candidate<S> cand[k_cache + 1];
     int8_t next;
     int8_t last;
     int8_t status;
@@ -68,7 +73,7 @@ struct nav_state {
     uint32_t n_isect;  // ray-surface intersections evaluated
 
     DPROP_HD void reset(uint32_t vol) {
-        for (int i = 0; i < k_cache; ++i) {
+        for (int i = 0; i <= k_cache; ++i) {
             cand[i] = invalid_candidate<S>();
         }
         next = 0;

@@ -265,6 +265,15 @@ DPROP_HD uint8_t propagate_track(track_state<S>& ts,
             if (i > 0u) {
                 is_init = false;
             }
+            // A state that is no longer finite (a particle stopped in
+            // material gets q/p = max, after which the reference computes with
+            // inf/NaN) cannot be propagated further: end the track.
+            if (!(fabs(st.path_length) < 1e30) || !(fabs(st.qop) < S(1e30)) ||
+                !(fabs(st.pos.x) + fabs(st.pos.y) + fabs(st.pos.z) < S(1e30))) {
+                ts.heartbeat = false;
+                nav.abort(e_reason_nonfinite);
+                continue;
+            }
             if (fabs(st.path_length) <=
                 fabs(path_prev) + static_cast<double>(cfg.nav.isect.path_tol)) {
                 if (stall >= 10u) {
@@ -293,6 +302,8 @@ DPROP_HD uint8_t propagate_track(track_state<S>& ts,
             return 1u;
         case e_reason_stalled:
             return 2u;
+        case e_reason_nonfinite:
+            return 6u;  // DPROP_TRK_NONFINITE
         default:
             return 3u;
     }

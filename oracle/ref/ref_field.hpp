@@ -86,6 +86,12 @@ struct field {
             out[2] = b[2];
             return;
         }
+        if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(z)) {
+            // a non-finite position (the reference continues after a
+            // particle stopped in material): no node lookup
+            out[0] = out[1] = out[2] = std::nan("");
+            return;
+        }
         const double r = std::sqrt(x * x + y * y);
         const double phi = std::atan2(y, x);
         uint32_t ir, iz;

@@ -140,8 +140,19 @@ struct surface_recorder : public base_actor {
 
     template <typename propagator_state_t>
     void operator()(state& st, propagator_state_t& prop) const {
+        // A particle that stopped in material gets q/p = the invalid maximum
+        // from the interactor (pointwise_material_interactor.hpp:271-276);
+        // the reference would go on stepping with inf/NaN into undefined
+        // behaviour (out-of-range table reads, segfaults).  End the track
+        // here, after this actor phase's record, as the device path does.
+        const bool stopped =
+            std::fabs(static_cast<double>(prop.stepping()().qop())) > 1e30;
         const auto& nav = prop.navigation();
         if (!nav.is_on_surface()) {
+            if (stopped) {
+                prop.navigation().abort("particle stopped in material");
+                prop.heartbeat(false);
+            }
             return;
         }
         const auto sf = nav.current_surface();
@@ -179,6 +190,10 @@ struct surface_recorder : public base_actor {
             st.buf->recs.push_back(r);
         }
         ++st.buf->n;
+        if (stopped) {
+            prop.navigation().abort("particle stopped in material");
+            prop.heartbeat(false);
+        }
     }
 };
 
@@ -291,16 +306,32 @@ int propagate_impl(const det_t& det, const oracle_field::field& field,
         state.set_particle(update_particle_hypothesis(ptc, track));
 
         bool ok = false;
-        if constexpr (with_interactor) {
-            auto refs = detray::tie(pl, us, is, rs);
-            ok = p.propagate(state, refs);
-        } else {
-            auto refs = detray::tie(pl, us, rs);
-            ok = p.propagate(state, refs);
+        bool failed = false;
+        try {
+            if constexpr (with_interactor) {
+                auto refs = detray::tie(pl, us, is, rs);
+                ok = p.propagate(state, refs);
+            } else {
+                auto refs = detray::tie(pl, us, rs);
+                ok = p.propagate(state, refs);
+            }
+        } catch (const std::exception&) {
+            // the reference ran into invalid state (e.g. it keeps stepping a
+            // particle that stopped in material and then indexes a table
+            // with garbage): report the track as non-finite
+            failed = true;
+        }
+        const auto& fstate = state.stepping()();
+        if (!std::isfinite(static_cast<double>(fstate.qop())) ||
+            std::fabs(static_cast<double>(fstate.qop())) > 1e30 ||
+            !std::isfinite(static_cast<double>(state.stepping().path_length()))) {
+            failed = true;
         }
 
         uint8_t status = DPROP_TRK_EXITED;
-        if (!ok) {
+        if (failed) {
+            status = DPROP_TRK_NONFINITE;
+        } else if (!ok) {
             const auto& nav = state.navigation();
             const scalar apl = state.stepping().abs_path_length();
             if (apl >= path_limit) {

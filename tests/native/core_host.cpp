@@ -145,3 +145,43 @@ int core_host_propagate(int precision_bytes, const dprop_detector_desc* desc,
     return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
 }
 }
+
+extern "C" int core_host_field_eval(int precision_bytes, const double* lo,
+                                    const double* hi, const uint32_t* nn,
+                                    const float* values, const double* xyz,
+                                    uint64_t count, double* out) {
+    const uint64_t n_all = static_cast<uint64_t>(nn[0]) * nn[1] * nn[2];
+    std::vector<float4> nodes(n_all);
+    for (uint64_t i = 0; i < n_all; ++i) {
+        nodes[i] = float4{values[3 * i], values[3 * i + 1], values[3 * i + 2], 0.f};
+    }
+    auto run = [&](auto zero) {
+        using S = decltype(zero);
+        field_view<S> f{};
+        f.kind = 1u;
+        f.n_r = nn[0];
+        f.n_phi = nn[1];
+        f.n_z = nn[2];
+        f.r_lo = static_cast<S>(lo[0]);
+        f.r_step_inv = nn[0] > 1 ? static_cast<S>((nn[0] - 1) / (hi[0] - lo[0])) : S(0);
+        f.phi_lo = static_cast<S>(lo[1]);
+        f.phi_step_inv = static_cast<S>(nn[1] / (2.0 * constant::pi));
+        f.z_lo = static_cast<S>(lo[2]);
+        f.z_step_inv = nn[2] > 1 ? static_cast<S>((nn[2] - 1) / (hi[2] - lo[2])) : S(0);
+        f.nodes = nodes.data();
+        for (uint64_t i = 0; i < count; ++i) {
+            const vec3<S> b = field_at(f, vec3<S>{static_cast<S>(xyz[3 * i]),
+                                                  static_cast<S>(xyz[3 * i + 1]),
+                                                  static_cast<S>(xyz[3 * i + 2])});
+            out[3 * i] = b.x;
+            out[3 * i + 1] = b.y;
+            out[3 * i + 2] = b.z;
+        }
+    };
+    if (precision_bytes == 8) {
+        run(0.0);
+    } else {
+        run(0.0f);
+    }
+    return 0;
+}
