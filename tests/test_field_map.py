@@ -150,7 +150,7 @@ def test_loopers_reach_path_limit(core_host, oracle, solenoid):
     this is a robustness check of the core, in double and float.)"""
     from detray_b200 import abi, tracks
     det = oracle.build_toy()
-    cfg = abi.make_config(max_records=48, search_window=(3, 3),
+    cfg = abi.make_config(max_records=8, search_window=(3, 3),
                           estimate_scattering_noise=0,
                           use_material_interactor=0)
     trk = tracks.toy_tracks(200, seed=22, pt_range=(0.02, 0.06),
