@@ -205,6 +205,7 @@ class Results(C.Structure):
         ("n_intersections", C.c_void_p),
         ("n_transports", C.c_void_p),
         ("n_material", C.c_void_p),
+        ("rec_offsets", C.c_void_p),
     ]
 
 
@@ -214,7 +215,8 @@ class Launch(C.Structure):
         ("block_size", C.c_uint32),
         ("ctas_per_sm", C.c_uint32),
         ("sort_tracks", C.c_uint32),
-        ("reserved", C.c_uint32 * 4),
+        ("use_graph", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 

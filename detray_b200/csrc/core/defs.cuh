@@ -29,10 +29,19 @@
 #else
 #define DPROP_HD_COLD __host__ __device__ __forceinline__
 #endif
+// Leaf functions with small interfaces (one surface intersection + mask
+// check) that are called from several places; -DDPROP_OUTLINE_LEAF keeps a
+// single out-of-line copy of each to shrink the kernel's code footprint.
+#if defined(DPROP_OUTLINE_LEAF)
+#define DPROP_HD_LEAF __host__ __device__ __noinline__
+#else
+#define DPROP_HD_LEAF __host__ __device__ __forceinline__
+#endif
 #else
 #define DPROP_HD inline
 #define DPROP_D inline
 #define DPROP_HD_COLD inline
+#define DPROP_HD_LEAF inline
 #endif
 
 namespace dprop {

@@ -209,7 +209,7 @@ DPROP_HD void nav_insert(nav_state<S>& nav, const candidate<S>& nc) {
 // -------------------------------------------- intersection_initialize
 // Intersect one surface with the tangential ray and insert the result(s).
 template <typename S>
-DPROP_HD void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
+DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
                                uint32_t sf_idx, vec3<S> ro, vec3<S> rd,
                                const isect_cfg<S>& cfg) {
     const dev_surface sf = det.surfaces[sf_idx];
@@ -263,7 +263,7 @@ DPROP_HD void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
 
 // ------------------------------------------------- intersection_update
 template <typename S>
-DPROP_HD bool update_candidate(candidate<S>& c, const detector_view<S>& det,
+DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S>& det,
                                vec3<S> ro, vec3<S> rd, const isect_cfg<S>& cfg,
                                S external_tol, uint32_t& n_isect) {
     if (c.sf == k_invalid) {

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <cstdio>
 #include <cstring>
@@ -156,48 +157,6 @@ __global__ void direction_key_kernel(const In* __restrict__ dx,
     idx[i] = static_cast<uint32_t>(i);
 }
 
-// Sort track indices by direction key; returns the device order array.
-template <typename In>
-dprop_status direction_order(const In* dx, const In* dy, const In* dz,
-                             uint64_t n, cudaStream_t stream,
-                             const uint32_t** order) {
-    if (n > 0x7fffffffull) {
-        return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
-    }
-    const int ni = static_cast<int>(n);
-    size_t temp_bytes = 0;
-    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
-        nullptr, temp_bytes, static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), ni, 0, 20, stream));
-    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
-    const size_t need = 4 * arr + temp_bytes + 256;
-    if (g_sort.bytes < need) {
-        if (g_sort.buf) {
-            DPROP_CUDA(cudaStreamSynchronize(stream));
-            cudaFree(g_sort.buf);
-            g_sort.buf = nullptr;
-            g_sort.bytes = 0;
-        }
-        DPROP_CUDA(cudaMalloc(&g_sort.buf, need));
-        g_sort.bytes = need;
-    }
-    char* p = static_cast<char*>(g_sort.buf);
-    uint32_t* keys_in = reinterpret_cast<uint32_t*>(p);
-    uint32_t* keys_out = reinterpret_cast<uint32_t*>(p + arr);
-    uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + 2 * arr);
-    uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
-    void* temp = p + 4 * arr;
-    const unsigned int grid = static_cast<unsigned int>((n + 255) / 256);
-    direction_key_kernel<In><<<grid, 256, 0, stream>>>(dx, dy, dz, n, keys_in,
-                                                       idx_in);
-    DPROP_CUDA(cudaGetLastError());
-    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in,
-                                               keys_out, idx_in, idx_out, ni,
-                                               0, 20, stream));
-    *order = idx_out;
-    return DPROP_OK;
-}
 
 // Device pointers of the inputs/outputs, by value into the kernels
 template <typename In>
@@ -302,10 +261,27 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     }
 }
 
-constexpr int k_plain_block = 128;
+// Threads per CTA and the minimum resident CTAs per SM the register
+// allocation targets (__launch_bounds__); overridable at build time for
+// tuning sweeps.
+#ifndef DPROP_BLOCK
+#define DPROP_BLOCK 128
+#endif
+#ifndef DPROP_MIN_BLOCKS
+// 12 resident CTAs of 128 threads per SM (40 registers per thread): measured
+// on B200 to hide the latency of the divergent navigation better than fewer
+// warps with more registers, despite the extra spills to L1
+#define DPROP_MIN_BLOCKS 12
+#endif
+constexpr int k_plain_block = DPROP_BLOCK;
 
-template <typename In>
-__global__ void __launch_bounds__(k_plain_block)
+// One instantiation per register budget: MinBlocks resident CTAs of 128
+// threads per SM -> 8: 64 registers, 12: 40 registers, 16: 32 registers per
+// thread (the rest spills to L1).  More resident warps hide more of the
+// navigation's memory and instruction-fetch latency; the best budget depends
+// on the workload (constant field vs field map), so it is a launch choice.
+template <typename In, int MinBlocks = DPROP_MIN_BLOCKS>
+__global__ void __launch_bounds__(k_plain_block, MinBlocks)
     propagate_plain_kernel(const detector_view<float> det,
                            const field_view<float> field,
                            const prop_cfg<float> cfg, const io_ptrs<In> io,
@@ -318,8 +294,8 @@ __global__ void __launch_bounds__(k_plain_block)
     run_one(t, n, det, field, cfg, io);
 }
 
-template <typename In>
-__global__ void __launch_bounds__(k_plain_block)
+template <typename In, int MinBlocks = DPROP_MIN_BLOCKS>
+__global__ void __launch_bounds__(k_plain_block, MinBlocks)
     propagate_persistent_kernel(const detector_view<float> det,
                                 const field_view<float> field,
                                 const prop_cfg<float> cfg, const io_ptrs<In> io,
@@ -346,6 +322,146 @@ __global__ void __launch_bounds__(k_plain_block)
     }
 }
 
+// register budget of a launch: resident CTAs per SM in {8, 12, 16}
+int occupancy_of(const dprop_launch* lc) {
+    const uint32_t v = (lc && lc->ctas_per_sm) ? lc->ctas_per_sm
+                                               : static_cast<uint32_t>(DPROP_MIN_BLOCKS);
+    return v <= 8u ? 8 : (v <= 12u ? 12 : 16);
+}
+
+template <typename In, int MB>
+void launch_plain_mb(unsigned int grid, cudaStream_t st,
+                     const detector_view<float>& det,
+                     const field_view<float>& field, const prop_cfg<float>& cfg,
+                     const io_ptrs<In>& io, uint64_t n, const uint32_t* order) {
+    propagate_plain_kernel<In, MB><<<grid, k_plain_block, 0, st>>>(
+        det, field, cfg, io, n, order);
+}
+
+template <typename In, int MB>
+void launch_persistent_mb(unsigned int grid, cudaStream_t st,
+                          const detector_view<float>& det,
+                          const field_view<float>& field,
+                          const prop_cfg<float>& cfg, const io_ptrs<In>& io,
+                          uint64_t n, unsigned int* queue,
+                          const uint32_t* order) {
+    propagate_persistent_kernel<In, MB><<<grid, k_plain_block, 0, st>>>(
+        det, field, cfg, io, n, queue, order);
+}
+
+// Scratch one propagation launch needs besides inputs and outputs.
+struct launch_scratch {
+    void* sort{nullptr};        // sort keys/indices + radix-sort temp storage
+    size_t sort_bytes{0};
+    unsigned int* queue{nullptr};  // persistent work-queue counter
+};
+
+size_t sort_scratch_bytes(uint64_t n) {
+    size_t temp = 0;
+    cub::DeviceRadixSort::SortPairs(
+        nullptr, temp, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 20);
+    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
+    return 4 * arr + temp + 256;
+}
+
+// Enqueue one propagation on a stream using the given scratch; contains no
+// allocation and no synchronisation, so it can be captured into a graph.
+template <typename In>
+dprop_status enqueue_propagation(const dprop_config& c,
+                                 const dprop_launch* launch_cfg,
+                                 const dprop_detector* det,
+                                 const dprop_field* field,
+                                 const io_ptrs<In>& io, uint64_t n,
+                                 cudaStream_t stream,
+                                 const launch_scratch& scr) {
+    const prop_cfg<float> cfg = make_prop_cfg<float>(c);
+    const uint32_t method = launch_cfg ? launch_cfg->method : DPROP_METHOD_PLAIN;
+    const int mb = occupancy_of(launch_cfg);
+    const uint32_t* order = nullptr;
+    if (launch_cfg && launch_cfg->sort_tracks) {
+        if (n > 0x7fffffffull) {
+            return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
+        }
+        const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
+        char* p = static_cast<char*>(scr.sort);
+        uint32_t* keys_in = reinterpret_cast<uint32_t*>(p);
+        uint32_t* keys_out = reinterpret_cast<uint32_t*>(p + arr);
+        uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + 2 * arr);
+        uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
+        size_t temp = scr.sort_bytes - 4 * arr;
+        const unsigned int kg = static_cast<unsigned int>((n + 255) / 256);
+        direction_key_kernel<In><<<kg, 256, 0, stream>>>(
+            io.trk[4], io.trk[5], io.trk[6], n, keys_in, idx_in);
+        DPROP_CUDA(cudaGetLastError());
+        DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+            p + 4 * arr, temp, keys_in, keys_out, idx_in, idx_out,
+            static_cast<int>(n), 0, 20, stream));
+        order = idx_out;
+    }
+    const detector_view<float> dv = det->view();
+    if (method == DPROP_METHOD_PERSISTENT) {
+        if (n > 0xffffff00ull) {
+            return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
+        }
+        DPROP_CUDA(cudaMemsetAsync(scr.queue, 0, sizeof(unsigned int), stream));
+        int dev = 0, sms = 0;
+        DPROP_CUDA(cudaGetDevice(&dev));
+        DPROP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(mb);
+        const uint64_t need = (n + k_plain_block - 1) / k_plain_block;
+        grid = grid < need ? grid : need;
+        const unsigned int g = static_cast<unsigned int>(grid);
+        if (mb == 8) {
+            launch_persistent_mb<In, 8>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
+        } else if (mb == 12) {
+            launch_persistent_mb<In, 12>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
+        } else {
+            launch_persistent_mb<In, 16>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
+        }
+    } else {
+        const unsigned int g =
+            static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
+        if (mb == 8) {
+            launch_plain_mb<In, 8>(g, stream, dv, field->view, cfg, io, n, order);
+        } else if (mb == 12) {
+            launch_plain_mb<In, 12>(g, stream, dv, field->view, cfg, io, n, order);
+        } else {
+            launch_plain_mb<In, 16>(g, stream, dv, field->view, cfg, io, n, order);
+        }
+    }
+    DPROP_CUDA(cudaGetLastError());
+    return DPROP_OK;
+}
+
+// ------------------------------------------------------------ CUDA graphs
+// With dprop_launch.use_graph the whole propagate call (key kernel, radix
+// sort, propagation kernel) is captured once into a CUDA graph and replayed
+// on later calls with the same arguments.  Each cached graph owns its
+// scratch, so a replay never depends on the shared grow-only scratch.
+struct graph_entry {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec{nullptr};
+    void* scratch{nullptr};
+    uint64_t last_use{0};
+};
+constexpr size_t k_graph_cache = 8;
+std::vector<graph_entry> g_graphs;
+uint64_t g_graph_clock = 0;
+std::mutex g_graph_mutex;
+
+void destroy_entry(graph_entry& e) {
+    if (e.exec) {
+        cudaGraphExecDestroy(e.exec);
+    }
+    if (e.scratch) {
+        cudaFree(e.scratch);
+    }
+    e.exec = nullptr;
+    e.scratch = nullptr;
+}
+
 template <typename In>
 dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
                     const dprop_detector* det, const dprop_field* field,
@@ -353,46 +469,99 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     if (n == 0) {
         return DPROP_OK;
     }
-    const prop_cfg<float> cfg = make_prop_cfg<float>(c);
-    const uint32_t method = launch_cfg ? launch_cfg->method : DPROP_METHOD_PLAIN;
-    const uint32_t* order = nullptr;
-    if (launch_cfg && launch_cfg->sort_tracks) {
-        const dprop_status s = direction_order<In>(io.trk[4], io.trk[5],
-                                                   io.trk[6], n, stream, &order);
-        if (s != DPROP_OK) {
-            return s;
+    const bool sort = launch_cfg && launch_cfg->sort_tracks;
+    const bool persistent = launch_cfg && launch_cfg->method == DPROP_METHOD_PERSISTENT;
+    if (!(launch_cfg && launch_cfg->use_graph)) {
+        launch_scratch scr{};
+        if (sort) {
+            const size_t need = sort_scratch_bytes(n);
+            if (g_sort.bytes < need) {
+                if (g_sort.buf) {
+                    DPROP_CUDA(cudaStreamSynchronize(stream));
+                    cudaFree(g_sort.buf);
+                    g_sort.buf = nullptr;
+                    g_sort.bytes = 0;
+                }
+                DPROP_CUDA(cudaMalloc(&g_sort.buf, need));
+                g_sort.bytes = need;
+            }
+            scr.sort = g_sort.buf;
+            scr.sort_bytes = need;
+        }
+        if (persistent) {
+            if (!g_queue_counter) {
+                DPROP_CUDA(cudaMalloc(&g_queue_counter, sizeof(unsigned int)));
+            }
+            scr.queue = g_queue_counter;
+        }
+        return enqueue_propagation<In>(c, launch_cfg, det, field, io, n, stream,
+                                       scr);
+    }
+
+    // graph path: key = everything the captured work depends on
+    std::vector<unsigned char> key;
+    auto put = [&key](const void* p, size_t b) {
+        const unsigned char* q = static_cast<const unsigned char*>(p);
+        key.insert(key.end(), q, q + b);
+    };
+    const int in_bytes = sizeof(In);
+    put(&in_bytes, sizeof(in_bytes));
+    put(&c, sizeof(c));
+    put(launch_cfg, sizeof(*launch_cfg));
+    put(&det, sizeof(det));
+    put(&field, sizeof(field));
+    put(&io, sizeof(io));
+    put(&n, sizeof(n));
+    int dev = 0;
+    DPROP_CUDA(cudaGetDevice(&dev));
+    put(&dev, sizeof(dev));
+
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    for (graph_entry& e : g_graphs) {
+        if (e.key == key) {
+            e.last_use = ++g_graph_clock;
+            DPROP_CUDA(cudaGraphLaunch(e.exec, stream));
+            return DPROP_OK;
         }
     }
-    if (method == DPROP_METHOD_PERSISTENT) {
-        if (n > 0xffffff00ull) {
-            return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
-        }
-        if (!g_queue_counter) {
-            DPROP_CUDA(cudaMalloc(&g_queue_counter, sizeof(unsigned int)));
-        }
-        DPROP_CUDA(cudaMemsetAsync(g_queue_counter, 0, sizeof(unsigned int),
-                                   stream));
-        int dev = 0, sms = 0;
-        DPROP_CUDA(cudaGetDevice(&dev));
-        DPROP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        uint32_t per_sm = (launch_cfg && launch_cfg->ctas_per_sm)
-                              ? launch_cfg->ctas_per_sm
-                              : 8u;
-        uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
-        const uint64_t need = (n + k_plain_block - 1) / k_plain_block;
-        if (grid > need) {
-            grid = need;
-        }
-        propagate_persistent_kernel<In><<<static_cast<unsigned int>(grid),
-                                          k_plain_block, 0, stream>>>(
-            det->view(), field->view, cfg, io, n, g_queue_counter, order);
-    } else {
-        const uint64_t grid = (n + k_plain_block - 1) / k_plain_block;
-        propagate_plain_kernel<In><<<static_cast<unsigned int>(grid),
-                                     k_plain_block, 0, stream>>>(
-            det->view(), field->view, cfg, io, n, order);
+    graph_entry e;
+    e.key = key;
+    const size_t sort_bytes = sort ? sort_scratch_bytes(n) : 0;
+    DPROP_CUDA(cudaMalloc(&e.scratch, sort_bytes + 256));
+    launch_scratch scr{};
+    scr.sort = e.scratch;
+    scr.sort_bytes = sort_bytes;
+    scr.queue = reinterpret_cast<unsigned int*>(static_cast<char*>(e.scratch) + sort_bytes);
+    cudaStream_t cap = nullptr;
+    DPROP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    DPROP_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    const dprop_status es =
+        enqueue_propagation<In>(c, launch_cfg, det, field, io, n, cap, scr);
+    const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (es != DPROP_OK || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaFree(e.scratch);
+        return es != DPROP_OK ? es : cuda_fail(ce, "cudaStreamEndCapture");
     }
-    DPROP_CUDA(cudaGetLastError());
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        cudaFree(e.scratch);
+        return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    if (g_graphs.size() >= k_graph_cache) {
+        size_t oldest = 0;
+        for (size_t i = 1; i < g_graphs.size(); ++i) {
+            if (g_graphs[i].last_use < g_graphs[oldest].last_use) oldest = i;
+        }
+        destroy_entry(g_graphs[oldest]);
+        g_graphs.erase(g_graphs.begin() + static_cast<long>(oldest));
+    }
+    e.last_use = ++g_graph_clock;
+    g_graphs.push_back(e);
+    DPROP_CUDA(cudaGraphLaunch(g_graphs.back().exec, stream));
     return DPROP_OK;
 }
 
@@ -412,6 +581,334 @@ dprop_status check_config(const dprop_config* cfg) {
     if (cfg->max_iterations == 0u) {
         return fail(DPROP_E_INVALID, "max_iterations must be > 0");
     }
+    return DPROP_OK;
+}
+
+
+// ------------------------------------------------ host path, jagged records
+// dprop_propagate_host with results->rec_offsets: the batch is processed in
+// chunks on two streams so that the host-to-device copy of one chunk, the
+// propagation of another and the device-to-host copy of a third overlap.
+// Each chunk's records are packed track by track (offsets from an exclusive
+// scan of the per-track record counts) and only the stored records are
+// copied back.
+
+// per-track record count, clamped to the capacity; entry n is 0 so that an
+// exclusive scan over n + 1 entries ends with the total
+__global__ void clamp_counts_kernel(const uint32_t* __restrict__ n_rec,
+                                    uint32_t cap, uint32_t n,
+                                    uint32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const uint32_t c = n_rec[i];
+        counts[i] = c < cap ? c : cap;
+    } else if (i == n) {
+        counts[i] = 0u;
+    }
+}
+
+struct record_arrays {
+    uint64_t* barcode;
+    float* bound[6];
+    float* cov[21];
+    float* path;
+    uint8_t* flags;
+};
+
+// slot-major records (k * n + t) -> packed records (offset[t] + k)
+__global__ void pack_records_kernel(record_arrays src, record_arrays dst,
+                                    const uint32_t* __restrict__ counts,
+                                    const uint32_t* __restrict__ offsets,
+                                    uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) {
+        return;
+    }
+    const uint32_t m = counts[t];
+    const uint32_t o = offsets[t];
+    for (uint32_t k = 0; k < m; ++k) {
+        const uint64_t si = static_cast<uint64_t>(k) * n + t;
+        const uint64_t di = static_cast<uint64_t>(o) + k;
+        if (dst.barcode) dst.barcode[di] = src.barcode[si];
+        for (int i = 0; i < 6; ++i) {
+            if (dst.bound[i]) dst.bound[i][di] = src.bound[i][si];
+        }
+        for (int i = 0; i < 21; ++i) {
+            if (dst.cov[i]) dst.cov[i][di] = src.cov[i][si];
+        }
+        if (dst.path) dst.path[di] = src.path[si];
+        if (dst.flags) dst.flags[di] = src.flags[si];
+    }
+}
+
+struct pipe_slot {
+    cudaStream_t stream{nullptr};
+    cudaEvent_t counted{nullptr};
+    void* dev{nullptr};
+    size_t dev_bytes{0};
+    uint32_t* host_offsets{nullptr};  // pinned, chunk + 1 entries
+    size_t host_entries{0};
+};
+pipe_slot g_pipe[2];
+
+dprop_status ensure_pipe(pipe_slot& ps, size_t dev_bytes, size_t chunk) {
+    if (!ps.stream) {
+        DPROP_CUDA(cudaStreamCreateWithFlags(&ps.stream, cudaStreamNonBlocking));
+        DPROP_CUDA(cudaEventCreateWithFlags(&ps.counted, cudaEventDisableTiming));
+    }
+    if (ps.dev_bytes < dev_bytes) {
+        if (ps.dev) {
+            cudaFree(ps.dev);
+            ps.dev = nullptr;
+            ps.dev_bytes = 0;
+        }
+        DPROP_CUDA(cudaMalloc(&ps.dev, dev_bytes));
+        ps.dev_bytes = dev_bytes;
+    }
+    if (ps.host_entries < chunk + 1) {
+        if (ps.host_offsets) {
+            cudaFreeHost(ps.host_offsets);
+            ps.host_offsets = nullptr;
+        }
+        DPROP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ps.host_offsets),
+                                  (chunk + 1) * sizeof(uint32_t)));
+        ps.host_entries = chunk + 1;
+    }
+    return DPROP_OK;
+}
+
+dprop_status propagate_host_jagged(const dprop_config& c,
+                                   const dprop_launch* lc,
+                                   const dprop_detector* det,
+                                   const dprop_field* field,
+                                   const dprop_tracks& tracks,
+                                   const dprop_results& out, uint64_t n) {
+    const uint64_t cap = c.max_records;
+    const uint64_t chunk = n < 262144u ? n : 262144u;
+    const prop_cfg<float> pcfg = make_prop_cfg<float>(c);
+    const bool sort = (lc == nullptr) || lc->sort_tracks != 0u;
+    const void* h_trk[8] = {tracks.pos[0], tracks.pos[1], tracks.pos[2],
+                            tracks.time,   tracks.dir[0], tracks.dir[1],
+                            tracks.dir[2], tracks.qop};
+    for (int i = 0; i < 8; ++i) {
+        if (!h_trk[i]) {
+            return fail(DPROP_E_INVALID, "propagate_host: missing track array");
+        }
+    }
+
+    // device scratch layout of one pipeline slot
+    size_t sort_temp = 0, scan_temp = 0;
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+        nullptr, sort_temp, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<int>(chunk), 0, 20));
+    DPROP_CUDA(cub::DeviceScan::ExclusiveSum(
+        nullptr, scan_temp, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<int>(chunk + 1)));
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t rec_slot = cap * chunk;
+    size_t need = 0;
+    need += 8 * al(chunk * sizeof(double));                        // inputs
+    need += al(chunk) + 7 * al(chunk * 4) + 8 * al(chunk * 4);     // per-track
+    need += 2 * (al(rec_slot * 8) + 28 * al(rec_slot * 4) + al(rec_slot));
+    need += 6 * al((chunk + 1) * 4) + al(sort_temp) + al(scan_temp);
+    for (auto& ps : g_pipe) {
+        const dprop_status s = ensure_pipe(ps, need, chunk);
+        if (s != DPROP_OK) {
+            return s;
+        }
+    }
+    cudaEvent_t inputs_ready = nullptr;
+    DPROP_CUDA(cudaEventCreateWithFlags(&inputs_ready, cudaEventDisableTiming));
+    // make the pipeline streams wait for work already queued on the legacy
+    // stream (e.g. the caller's uploads)
+    DPROP_CUDA(cudaEventRecord(inputs_ready, 0));
+    for (auto& ps : g_pipe) {
+        DPROP_CUDA(cudaStreamWaitEvent(ps.stream, inputs_ready, 0));
+    }
+
+    struct chunk_info {
+        uint64_t begin;
+        uint64_t count;
+        record_arrays packed;
+    };
+    chunk_info prev{};
+    bool have_prev = false;
+    int prev_slot = 0;
+    uint64_t rec_base = 0;
+
+    // copy a finished chunk's packed records into the caller's arrays
+    auto drain = [&](const chunk_info& ci, int slot) -> dprop_status {
+        pipe_slot& ps = g_pipe[slot];
+        DPROP_CUDA(cudaEventSynchronize(ps.counted));
+        const uint32_t total = ps.host_offsets[ci.count];
+        for (uint64_t t = 0; t < ci.count; ++t) {
+            out.rec_offsets[ci.begin + t] = rec_base + ps.host_offsets[t];
+        }
+        auto d2h = [&](void* h, const void* d, size_t elem) -> dprop_status {
+            if (h && d && total) {
+                DPROP_CUDA(cudaMemcpyAsync(static_cast<char*>(h) + rec_base * elem,
+                                           d, total * elem,
+                                           cudaMemcpyDeviceToHost, ps.stream));
+            }
+            return DPROP_OK;
+        };
+        dprop_status s = DPROP_OK;
+        if ((s = d2h(out.rec_barcode, ci.packed.barcode, 8)) != DPROP_OK) return s;
+        for (int i = 0; i < 6; ++i) {
+            if ((s = d2h(out.rec_bound[i], ci.packed.bound[i], 4)) != DPROP_OK) return s;
+        }
+        for (int i = 0; i < 21; ++i) {
+            if ((s = d2h(out.rec_cov[i], ci.packed.cov[i], 4)) != DPROP_OK) return s;
+        }
+        if ((s = d2h(out.rec_path, ci.packed.path, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.rec_flags, ci.packed.flags, 1)) != DPROP_OK) return s;
+        rec_base += total;
+        return DPROP_OK;
+    };
+
+    int slot = 0;
+    for (uint64_t begin = 0; begin < n; begin += chunk, slot ^= 1) {
+        const uint64_t m = (n - begin) < chunk ? (n - begin) : chunk;
+        pipe_slot& ps = g_pipe[slot];
+        cudaStream_t st = ps.stream;
+        char* p = static_cast<char*>(ps.dev);
+        auto take = [&](size_t b) {
+            char* r = p;
+            p += al(b);
+            return r;
+        };
+        // inputs
+        const double* d_trk[8];
+        for (int i = 0; i < 8; ++i) {
+            double* d = reinterpret_cast<double*>(take(chunk * sizeof(double)));
+            DPROP_CUDA(cudaMemcpyAsync(d, static_cast<const double*>(h_trk[i]) + begin,
+                                       m * sizeof(double), cudaMemcpyHostToDevice, st));
+            d_trk[i] = d;
+        }
+        // per-track outputs and slot-major records (row stride m)
+        dprop_results dr{};
+        dr.status = reinterpret_cast<uint8_t*>(take(chunk));
+        dr.n_records = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        dr.n_steps = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        dr.n_trials = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        dr.path_length = take(chunk * 4);
+        dr.n_intersections = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        dr.n_transports = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        dr.n_material = reinterpret_cast<uint32_t*>(take(chunk * 4));
+        for (int i = 0; i < 8; ++i) {
+            dr.final_free[i] = take(chunk * 4);
+        }
+        record_arrays slotm{}, packed{};
+        slotm.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
+        packed.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
+        for (int i = 0; i < 6; ++i) {
+            slotm.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+            packed.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+        }
+        for (int i = 0; i < 21; ++i) {
+            if (out.rec_cov[i]) {
+                slotm.cov[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+                packed.cov[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+            } else {
+                take(rec_slot * 4);
+                take(rec_slot * 4);
+            }
+        }
+        slotm.path = reinterpret_cast<float*>(take(rec_slot * 4));
+        packed.path = reinterpret_cast<float*>(take(rec_slot * 4));
+        slotm.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
+        packed.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
+        dr.rec_barcode = slotm.barcode;
+        for (int i = 0; i < 6; ++i) dr.rec_bound[i] = slotm.bound[i];
+        for (int i = 0; i < 21; ++i) dr.rec_cov[i] = slotm.cov[i];
+        dr.rec_path = slotm.path;
+        dr.rec_flags = slotm.flags;
+        uint32_t* counts = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        uint32_t* offsets = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        uint32_t* keys_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        uint32_t* keys_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        uint32_t* idx_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        uint32_t* idx_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+        void* sort_tmp = take(sort_temp);
+        void* scan_tmp = take(scan_temp);
+
+        dprop_tracks dt{};
+        for (int i = 0; i < 3; ++i) {
+            dt.pos[i] = d_trk[i];
+            dt.dir[i] = d_trk[4 + i];
+        }
+        dt.time = d_trk[3];
+        dt.qop = d_trk[7];
+        const io_ptrs<double> io = make_io<double>(dt, dr);
+        const uint32_t* order = nullptr;
+        if (sort) {
+            const unsigned int kg = static_cast<unsigned int>((m + 255) / 256);
+            direction_key_kernel<double><<<kg, 256, 0, st>>>(
+                d_trk[4], d_trk[5], d_trk[6], m, keys_in, idx_in);
+            size_t tb = sort_temp;
+            DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+                sort_tmp, tb, keys_in, keys_out, idx_in, idx_out,
+                static_cast<int>(m), 0, 20, st));
+            order = idx_out;
+        }
+        const unsigned int grid =
+            static_cast<unsigned int>((m + k_plain_block - 1) / k_plain_block);
+        propagate_plain_kernel<double><<<grid, k_plain_block, 0, st>>>(
+            det->view(), field->view, pcfg, io, m, order);
+        DPROP_CUDA(cudaGetLastError());
+        // pack the records
+        const unsigned int cg = static_cast<unsigned int>((m + 1 + 255) / 256);
+        clamp_counts_kernel<<<cg, 256, 0, st>>>(dr.n_records,
+                                                static_cast<uint32_t>(cap),
+                                                static_cast<uint32_t>(m), counts);
+        size_t sb = scan_temp;
+        DPROP_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, sb, counts, offsets,
+                                                 static_cast<int>(m + 1), st));
+        const unsigned int pg = static_cast<unsigned int>((m + 127) / 128);
+        pack_records_kernel<<<pg, 128, 0, st>>>(slotm, packed, counts, offsets,
+                                                static_cast<uint32_t>(m));
+        DPROP_CUDA(cudaGetLastError());
+        // per-track outputs and the offsets back to the host
+        auto d2h = [&](void* h, const void* d, size_t elem) -> dprop_status {
+            if (h && d) {
+                DPROP_CUDA(cudaMemcpyAsync(static_cast<char*>(h) + begin * elem, d,
+                                           m * elem, cudaMemcpyDeviceToHost, st));
+            }
+            return DPROP_OK;
+        };
+        dprop_status s = DPROP_OK;
+        if ((s = d2h(out.status, dr.status, 1)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_records, dr.n_records, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_steps, dr.n_steps, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_trials, dr.n_trials, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.path_length, dr.path_length, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_intersections, dr.n_intersections, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_transports, dr.n_transports, 4)) != DPROP_OK) return s;
+        if ((s = d2h(out.n_material, dr.n_material, 4)) != DPROP_OK) return s;
+        for (int i = 0; i < 8; ++i) {
+            if ((s = d2h(out.final_free[i], dr.final_free[i], 4)) != DPROP_OK) return s;
+        }
+        DPROP_CUDA(cudaMemcpyAsync(ps.host_offsets, offsets, (m + 1) * 4,
+                                   cudaMemcpyDeviceToHost, st));
+        DPROP_CUDA(cudaEventRecord(ps.counted, st));
+        // drain the previous chunk while this one runs
+        if (have_prev) {
+            if ((s = drain(prev, prev_slot)) != DPROP_OK) return s;
+        }
+        prev = chunk_info{begin, m, packed};
+        prev_slot = slot;
+        have_prev = true;
+    }
+    if (have_prev) {
+        const dprop_status s = drain(prev, prev_slot);
+        if (s != DPROP_OK) return s;
+    }
+    out.rec_offsets[n] = rec_base;
+    for (auto& ps : g_pipe) {
+        DPROP_CUDA(cudaStreamSynchronize(ps.stream));
+    }
+    cudaEventDestroy(inputs_ready);
     return DPROP_OK;
 }
 
@@ -501,6 +998,99 @@ dprop_status dprop_detector_destroy(dprop_detector* det) {
     cudaFree(det->grids);
     cudaFree(det->grid_bins);
     delete det;
+    return DPROP_OK;
+}
+
+dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
+                            const dprop_field* field, const dprop_tracks* tracks,
+                            uint64_t n, dprop_launch* launch_out,
+                            float* timings_ms, void* stream_ptr) {
+    dprop_status s = check_config(cfg);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    if (!det || !field || !tracks || !launch_out) {
+        return fail(DPROP_E_INVALID, "autotune: NULL argument");
+    }
+    if (n == 0) {
+        return DPROP_OK;
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const uint64_t m = n < 262144u ? n : 262144u;
+    const uint64_t cap = cfg->max_records;
+    // temporary results for the trial runs
+    const size_t per_track = 1 + 6 * 4 + 8 * 4 + 16;
+    const size_t per_rec = 8 + 6 * 4 + 21 * 4 + 4 + 1;
+    void* buf = nullptr;
+    DPROP_CUDA(cudaMalloc(&buf, m * per_track + cap * m * per_rec + 4096));
+    char* p = static_cast<char*>(buf);
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += (b + 15) & ~size_t(15);
+        return r;
+    };
+    dprop_results r{};
+    r.status = reinterpret_cast<uint8_t*>(take(m));
+    r.n_records = reinterpret_cast<uint32_t*>(take(4 * m));
+    r.n_steps = reinterpret_cast<uint32_t*>(take(4 * m));
+    r.n_trials = reinterpret_cast<uint32_t*>(take(4 * m));
+    r.path_length = take(4 * m);
+    r.rec_barcode = reinterpret_cast<uint64_t*>(take(8 * cap * m));
+    for (int i = 0; i < 6; ++i) r.rec_bound[i] = take(4 * cap * m);
+    for (int i = 0; i < 21; ++i) r.rec_cov[i] = take(4 * cap * m);
+    r.rec_path = take(4 * cap * m);
+    r.rec_flags = reinterpret_cast<uint8_t*>(take(cap * m));
+    const io_ptrs<float> io = make_io<float>(*tracks, r);
+
+    struct cand {
+        uint32_t method, ctas, sort;
+    };
+    const cand cands[DPROP_AUTOTUNE_CANDIDATES] = {
+        {DPROP_METHOD_PLAIN, 8, 1},       {DPROP_METHOD_PLAIN, 12, 1},
+        {DPROP_METHOD_PLAIN, 16, 1},      {DPROP_METHOD_PERSISTENT, 8, 1},
+        {DPROP_METHOD_PERSISTENT, 12, 1}, {DPROP_METHOD_PERSISTENT, 16, 1},
+        {DPROP_METHOD_PLAIN, 8, 0},       {DPROP_METHOD_PLAIN, 12, 0},
+        {DPROP_METHOD_PLAIN, 16, 0},      {DPROP_METHOD_PERSISTENT, 16, 0}};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 3.4e38f;
+    int best_i = 1;
+    for (int i = 0; i < DPROP_AUTOTUNE_CANDIDATES && s == DPROP_OK; ++i) {
+        dprop_launch lc{};
+        lc.method = cands[i].method;
+        lc.ctas_per_sm = cands[i].ctas;
+        lc.sort_tracks = cands[i].sort;
+        s = launch<float>(*cfg, &lc, det, field, io, m, stream);  // warm-up
+        if (s != DPROP_OK) break;
+        cudaEventRecord(e0, stream);
+        for (int k = 0; k < 2 && s == DPROP_OK; ++k) {
+            s = launch<float>(*cfg, &lc, det, field, io, m, stream);
+        }
+        cudaEventRecord(e1, stream);
+        const cudaError_t ce = cudaEventSynchronize(e1);
+        if (ce != cudaSuccess) {
+            s = cuda_fail(ce, "autotune");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms *= 0.5f;
+        if (timings_ms) timings_ms[i] = ms;
+        if (ms < best) {
+            best = ms;
+            best_i = i;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    if (s != DPROP_OK) {
+        return s;
+    }
+    launch_out->method = cands[best_i].method;
+    launch_out->ctas_per_sm = cands[best_i].ctas;
+    launch_out->sort_tracks = cands[best_i].sort;
     return DPROP_OK;
 }
 
@@ -622,7 +1212,13 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
         return fail(DPROP_E_INVALID, "propagate_host: NULL argument");
     }
     if (n == 0) {
+        if (results->rec_offsets) {
+            results->rec_offsets[0] = 0u;
+        }
         return DPROP_OK;
+    }
+    if (results->rec_offsets) {
+        return propagate_host_jagged(*cfg, lc, det, field, *tracks, *results, n);
     }
     const uint64_t cap = cfg->max_records;
     // device scratch: inputs (8 doubles), per-track outputs, records

@@ -71,6 +71,9 @@ def load_library() -> C.CDLL:
     lib.dprop_propagate_host.argtypes = [
         C.POINTER(abi.Config), C.POINTER(abi.Launch), C.c_void_p, C.c_void_p,
         C.POINTER(abi.Tracks), C.POINTER(abi.Results), C.c_uint64]
+    lib.dprop_autotune.argtypes = [
+        C.POINTER(abi.Config), C.c_void_p, C.c_void_p, C.POINTER(abi.Tracks),
+        C.c_uint64, C.POINTER(abi.Launch), C.POINTER(C.c_float), C.c_void_p]
     if lib.dprop_abi_version() != abi.DPROP_ABI_VERSION:
         raise PropagationError("detray-b200 library ABI version mismatch")
     _lib = lib
@@ -156,12 +159,14 @@ class Field:
 
 
 def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
-                ctas_per_sm: int = 0, sort_tracks: int = 0) -> abi.Launch:
+                ctas_per_sm: int = 0, sort_tracks: int = 0,
+                use_graph: int = 0) -> abi.Launch:
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
     lc.ctas_per_sm = ctas_per_sm
     lc.sort_tracks = sort_tracks
+    lc.use_graph = use_graph
     return lc
 
 
@@ -259,8 +264,13 @@ def propagate(cfg: abi.Config, det: Detector, field: Field, tracks,
 
 
 def alloc_host_results(n: int, max_records: int, pinned: bool = False,
-                       with_cov: bool = True) -> tuple[dict, abi.Results]:
-    """Host result buffers for propagate_host (float fields as float32)."""
+                       with_cov: bool = True,
+                       jagged: bool = False) -> tuple[dict, abi.Results]:
+    """Host result buffers for propagate_host (float fields as float32).
+
+    jagged=True asks for the records as a jagged array: ``rec_offsets``
+    (n + 1 entries) indexes flat record arrays, and only the stored records
+    are copied back from the device."""
     if pinned:
         import torch
 
@@ -283,6 +293,7 @@ def alloc_host_results(n: int, max_records: int, pinned: bool = False,
         "rec_bound": empty((6, max_records, n), f32),
         "rec_path": empty((max_records, n), f32),
         "rec_flags": empty((max_records, n), u8),
+        "rec_offsets": empty((n + 1,), i64) if jagged else None,
         "n_intersections": empty((n,), i32),
         "n_transports": empty((n,), i32),
         "n_material": empty((n,), i32),
@@ -308,20 +319,55 @@ def alloc_host_results(n: int, max_records: int, pinned: bool = False,
     r.n_intersections = res["n_intersections"].ctypes.data
     r.n_transports = res["n_transports"].ctypes.data
     r.n_material = res["n_material"].ctypes.data
+    if jagged:
+        r.rec_offsets = res["rec_offsets"].ctypes.data
+        # flat views: record j of the jagged array is index j
+        for key in ("rec_barcode", "rec_path", "rec_flags"):
+            res[key] = res[key].reshape(-1)
+        for key in ("rec_bound", "rec_cov"):
+            if key in res:
+                res[key] = res[key].reshape(res[key].shape[0], -1)
+    else:
+        del res["rec_offsets"]
     return res, r
 
 
 def propagate_host(cfg: abi.Config, det: Detector, field: Field,
                    tracks: np.ndarray, launch: abi.Launch | None = None,
-                   out: tuple | None = None) -> dict:
+                   out: tuple | None = None, jagged: bool = False) -> dict:
     """Propagate host tracks ((8, n) float64); host-to-device copies,
     propagation and device-to-host copies happen inside the call."""
     trk = np.ascontiguousarray(tracks, dtype=np.float64)
     n = trk.shape[1]
-    res, r = out if out is not None else alloc_host_results(n, cfg.max_records)
+    res, r = out if out is not None else alloc_host_results(
+        n, cfg.max_records, jagged=jagged)
     ts = tracks_struct(trk)
     lc = launch if launch is not None else make_launch()
     _check(load_library().dprop_propagate_host(
         C.byref(cfg), C.byref(lc), det.handle, field.handle, C.byref(ts),
         C.byref(r), n))
     return res
+
+
+AUTOTUNE_CANDIDATES = [
+    ("plain", 8, 1), ("plain", 12, 1), ("plain", 16, 1),
+    ("persistent", 8, 1), ("persistent", 12, 1), ("persistent", 16, 1),
+    ("plain", 8, 0), ("plain", 12, 0), ("plain", 16, 0),
+    ("persistent", 16, 0)]
+
+
+def autotune(cfg: abi.Config, det: Detector, field: Field, tracks,
+             use_graph: int = 0, stream=None) -> tuple[abi.Launch, list]:
+    """Pick the fastest launch form for these tracks (dprop_autotune)."""
+    import torch
+    tracks = tracks.contiguous()
+    n = tracks.shape[1]
+    lc = make_launch(use_graph=use_graph)
+    times = (C.c_float * len(AUTOTUNE_CANDIDATES))()
+    if stream is None:
+        stream = torch.cuda.current_stream(tracks.device)
+    ts = tracks_struct(tracks)
+    _check(load_library().dprop_autotune(
+        C.byref(cfg), det.handle, field.handle, C.byref(ts), n, C.byref(lc),
+        times, C.c_void_p(stream.cuda_stream)))
+    return lc, list(times)

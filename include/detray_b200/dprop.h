@@ -259,6 +259,12 @@ typedef struct dprop_results {
     uint32_t* n_transports;   /* [n] covariance transports to a surface;
                                   may be NULL                                  */
     uint32_t* n_material;     /* [n] material interactions; may be NULL        */
+    uint64_t* rec_offsets;    /* host entry point only: if not NULL, records
+                                  are returned as a jagged array - the records
+                                  of track t are entries [rec_offsets[t],
+                                  rec_offsets[t+1]) of the rec_* arrays (at
+                                  most max_records per track, n + 1 offsets),
+                                  and only stored records are copied back     */
 } dprop_results;
 
 /* Launch shape; zero fields pick the library defaults / autotuned values. */
@@ -271,12 +277,19 @@ typedef enum dprop_method {
 typedef struct dprop_launch {
     uint32_t method;             /* dprop_method                               */
     uint32_t block_size;         /* threads per CTA (0: default)               */
-    uint32_t ctas_per_sm;        /* persistent grid = SMs * ctas_per_sm         */
+    uint32_t ctas_per_sm;        /* register budget: resident CTAs of 128
+                                    threads per SM the kernel is compiled for,
+                                    8 (64 registers), 12 (40) or 16 (32);
+                                    0 = 12.  The persistent grid is SMs times
+                                    this                                       */
     uint32_t sort_tracks;        /* 1: process tracks ordered by direction
                                     (theta, phi) so that the lanes of a warp
                                     follow similar paths; results are still
                                     written at each track's input position    */
-    uint32_t reserved[4];
+    uint32_t use_graph;          /* 1: capture the whole propagate call into a
+                                    CUDA graph on first use and replay it on
+                                    later calls with identical arguments       */
+    uint32_t reserved[3];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */
@@ -358,6 +371,20 @@ dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
                                      const dprop_tracks* tracks,
                                      const dprop_results* results,
                                      uint64_t n_tracks, void* stream);
+
+/* Autotuner: times candidate launch forms - plain and persistent kernels at
+ * the three register budgets (ctas_per_sm 8, 12, 16), with and without the
+ * direction sort - on the first min(n_tracks, 262144) of the given device
+ * tracks, and writes the fastest into *launch (method, ctas_per_sm,
+ * sort_tracks; use_graph is left as given).  If timings_ms is not NULL it
+ * receives one time per candidate (DPROP_AUTOTUNE_CANDIDATES entries).
+ * Allocates temporary device result buffers for the trial runs. */
+#define DPROP_AUTOTUNE_CANDIDATES 10
+dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
+                            const dprop_field* field,
+                            const dprop_tracks* tracks, uint64_t n_tracks,
+                            dprop_launch* launch, float* timings_ms,
+                            void* stream);
 
 /* Number of surfaces / volumes held by a detector (for callers sizing output). */
 dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,

@@ -142,3 +142,103 @@ def test_empty_batch_and_invalid_arguments(torch_cuda):
                              C.byref(ts), C.byref(res.struct), 1, None)
     assert rc == abi.DPROP_E_UNSUPPORTED
     assert "gradient" in lib.dprop_last_error().decode()
+
+
+def test_device_in_field_map_vs_oracle(torch_cuda, oracle):
+    """Config-3 style: toy detector in the finite-solenoid field map,
+    pT 0.1-100 GeV, direction-sorted launch."""
+    from detray_b200 import abi, fields, geometry, propagator, tracks
+    fmap = fields.solenoid_map()
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
+    field = propagator.Field.grid(fmap)
+    cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                          estimate_scattering_noise=0)
+    trk = tracks.toy_tracks(20000, seed=31, pt_range=(0.1, 100.0))
+    ref = oracle.propagate(oracle.build_toy(), fmap, cfg, trk)
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+    res = propagator.propagate(cfg, det, field, dev,
+                               launch=propagator.make_launch(sort_tracks=1))
+    torch_cuda.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+    got["rec_barcode"] = got["rec_barcode"].view(np.uint64)
+    s = compare(ref, got, max_seq_mismatch_frac=1e-3, tol_abs=TOL_ABS,
+                tol_rel=TOL_REL, cov_rel=COV_REL)
+    print("field map", s)
+
+
+def test_device_loopers_end_cleanly(torch_cuda):
+    """Low-pT loopers in the field map, with and without energy loss: every
+    track ends by the path limit, by leaving, by losing its surfaces or by
+    stopping (non-finite) - never by the iteration budget."""
+    from detray_b200 import abi, fields, geometry, propagator, tracks
+    fmap = fields.solenoid_map()
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
+    field = propagator.Field.grid(fmap)
+    trk = tracks.toy_tracks(4096, seed=22, pt_range=(0.02, 0.06),
+                            eta_range=(-1.0, 1.0))
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+    for material in (0, 1):
+        cfg = abi.make_config(max_records=16, search_window=(3, 3),
+                              estimate_scattering_noise=0,
+                              use_material_interactor=material)
+        res = propagator.propagate(cfg, det, field, dev,
+                                   launch=propagator.make_launch(sort_tracks=1))
+        torch_cuda.cuda.synchronize()
+        st = res.tensors["status"].cpu().numpy()
+        assert not (st == abi.TRK_MAX_ITER).any()
+        assert (st == abi.TRK_PATH_LIMIT).sum() > 0
+        if material:
+            assert (st == abi.TRK_NONFINITE).sum() > 0
+
+
+def test_host_api_jagged_equals_device_api(torch_cuda):
+    """The pipelined host path returning jagged records (several chunks, two
+    streams) gives the same records as the device API."""
+    from detray_b200 import abi, geometry, propagator, tracks
+    from detray_b200.units import T
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
+    field = propagator.Field.constant((0.0, 0.0, 2.0 * T))
+    cfg = abi.make_config(max_records=24, search_window=(3, 3))
+    trk = tracks.toy_tracks(600_000, seed=41)  # 3 chunks
+    a = _run_device(torch_cuda, det, field, cfg, trk)
+    lc = propagator.make_launch(sort_tracks=1)
+    b = propagator.propagate_host(cfg, det, field, trk, launch=lc, jagged=True)
+    for key in ["status", "n_records", "n_trials", "path_length"]:
+        assert np.array_equal(a[key], b[key]), key
+    off = b["rec_offsets"]
+    cnt = np.minimum(a["n_records"], cfg.max_records)
+    assert np.array_equal(np.diff(off), cnt)
+    k = np.arange(cfg.max_records)[:, None]
+    valid = k < cnt[None, :]
+    # slot-major (k, t) -> jagged index off[t] + k
+    idx = (off[:-1][None, :] + k)[valid]
+    assert np.array_equal(a["rec_barcode"][valid], b["rec_barcode"][idx].view(np.uint64))
+    for i in range(6):
+        assert np.array_equal(a["rec_bound"][i][valid], b["rec_bound"][i][idx])
+    for i in range(21):
+        assert np.array_equal(a["rec_cov"][i][valid], b["rec_cov"][i][idx])
+
+
+def test_graph_replay_and_autotune(torch_cuda):
+    """A propagate call captured into a CUDA graph and replayed gives the
+    same results as the direct launch; the autotuner returns one of its
+    candidates and times all of them."""
+    from detray_b200 import abi, propagator
+    det, field, cfg, trk = _setup("toy")
+    a = _run_device(torch_cuda, det, field, cfg, trk, method=0)
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+    res = propagator.alloc_device_results(dev.shape[1], cfg.max_records, "cuda")
+    for occ in (8, 16):
+        lc = propagator.make_launch(sort_tracks=1, use_graph=1, ctas_per_sm=occ)
+        for _ in range(3):  # capture, then replays
+            res.tensors["status"].fill_(255)
+            propagator.propagate(cfg, det, field, dev, results=res, launch=lc)
+            torch_cuda.cuda.synchronize()
+            b = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+            assert np.array_equal(a["status"], b["status"])
+            assert np.array_equal(a["n_records"], b["n_records"])
+            assert np.array_equal(a["path_length"], b["path_length"])
+    lc, times = propagator.autotune(cfg, det, field, dev)
+    assert lc.ctas_per_sm in (8, 12, 16)
+    assert lc.method in (abi.METHOD_PLAIN, abi.METHOD_PERSISTENT)
+    assert all(t > 0 for t in times)
