@@ -220,6 +220,26 @@ class Launch(C.Structure):
     ]
 
 
+# Adjoint-mode tape sizes in floats (dprop.h DPROP_TAPE_*_FLOATS)
+TAPE_RECORD_FLOATS = 27
+TAPE_TRACK_FLOATS = 35
+
+
+class Tape(C.Structure):
+    _fields_ = [
+        ("rec", C.c_void_p),
+        ("init", C.c_void_p),
+    ]
+
+
+class Gradients(C.Structure):
+    _fields_ = [
+        ("grad_bound", C.c_void_p * 6),
+        ("grad_free", C.c_void_p * 8),
+        ("grad_align", C.c_void_p),
+    ]
+
+
 def default_config_values() -> dict:
     """The reference defaults (stepping_config.hpp:27-77,
     navigation_config.hpp:23-56, intersection_config.hpp:20-33) plus the

@@ -34,9 +34,17 @@ def _newer(target: Path, sources) -> bool:
     return all(Path(s).stat().st_mtime <= t for s in sources)
 
 
-def _sources():
-    return ([CSRC / "dprop_api.cu"] + sorted((CSRC / "core").glob("*"))
+# translation units of the library, compiled in parallel
+UNITS = ["dprop_api.cu", "adjoint_api.cu"]
+
+
+def _headers():
+    return (sorted((CSRC / "core").glob("*")) + sorted(CSRC.glob("*.cuh"))
             + [REPO / "include" / "detray_b200" / "dprop.h"])
+
+
+def _sources():
+    return [CSRC / u for u in UNITS] + _headers()
 
 
 def nvcc() -> str:
@@ -50,11 +58,28 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     if not force and _newer(LIB, _sources()):
         return LIB
     LIB.parent.mkdir(parents=True, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{REPO / 'include'}", f"-I{CSRC}",
-           str(CSRC / "dprop_api.cu"), "-o", str(LIB)]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    obj_dir = LIB.parent / "obj"
+    obj_dir.mkdir(exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for unit in UNITS:
+        src = CSRC / unit
+        obj = obj_dir / (src.stem + ".o")
+        objs.append(obj)
+        if not force and _newer(obj, [src] + _headers()):
+            continue
+        cmd = [nvcc(), *flags, "-c", f"-I{REPO / 'include'}", f"-I{CSRC}",
+               str(src), "-o", str(obj)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((unit, subprocess.Popen(cmd)))
+    failed = [unit for unit, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-shared", *[str(o) for o in objs], "-o", str(LIB)],
+                   check=True)
     return LIB
 
 

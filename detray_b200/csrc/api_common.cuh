@@ -1,0 +1,76 @@
+// Pieces of the C ABI implementation shared by its translation units
+// (dprop_api.cu: propagation; adjoint_api.cu: adjoint mode and the reverse
+// sweep): error reporting, the detector and field handles, the direction
+// sort of the inputs and the register-budget choice of a launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "core/propagate.cuh"
+#include "detray_b200/dprop.h"
+
+namespace dprop::api {
+
+// Record msg as dprop_last_error() of this thread and return s.
+dprop_status fail(dprop_status s, const std::string& msg);
+dprop_status cuda_fail(cudaError_t e, const char* what);
+
+// Register budget of a launch: resident CTAs of 128 threads per SM, one of
+// 8 (64 registers), 12 (40) or 16 (32).
+int occupancy_of(const dprop_launch* lc);
+
+// Device scratch bytes of enqueue_direction_sort for n tracks.
+size_t sort_scratch_bytes(uint64_t n);
+
+// Enqueue the direction sort of n tracks (20-bit theta/phi key, CUB radix
+// sort) on stream; *order receives the device array of sorted track
+// indices, which lives in scratch.  No allocation, no synchronisation.
+dprop_status enqueue_direction_sort(const float* dx, const float* dy,
+                                    const float* dz, uint64_t n, void* scratch,
+                                    size_t scratch_bytes, cudaStream_t stream,
+                                    const uint32_t** order);
+
+}  // namespace dprop::api
+
+#define DPROP_CUDA(call)                                      \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) {                              \
+            return ::dprop::api::cuda_fail(e_, #call);        \
+        }                                                     \
+    } while (0)
+
+struct dprop_detector {
+    int device{0};
+    dprop::dev_volume* volumes{nullptr};
+    dprop::dev_surface* surfaces{nullptr};
+    dprop::dev_mask<float>* masks{nullptr};
+    dprop::dev_transform<float>* transforms{nullptr};
+    dprop::dev_slab<float>* slabs{nullptr};
+    uint32_t* bf_surfaces{nullptr};
+    dprop::dev_grid<float>* grids{nullptr};
+    uint32_t* grid_bins{nullptr};
+    uint32_t n_volumes{0}, n_surfaces{0};
+    dprop::detector_view<float> view() const {
+        dprop::detector_view<float> v;
+        v.volumes = volumes;
+        v.surfaces = surfaces;
+        v.masks = masks;
+        v.transforms = transforms;
+        v.slabs = slabs;
+        v.bf_surfaces = bf_surfaces;
+        v.grids = grids;
+        v.grid_bins = grid_bins;
+        v.n_volumes = n_volumes;
+        v.n_surfaces = n_surfaces;
+        return v;
+    }
+};
+
+struct dprop_field {
+    int device{0};
+    float4* nodes{nullptr};
+    dprop::field_view<float> view{};
+};

@@ -9,7 +9,7 @@
 // stepper_rk_policy (navigation/policies.hpp:98-139).
 #pragma once
 
-#include "actors.cuh"
+#include "adjoint.cuh"
 
 namespace dprop {
 
@@ -110,13 +110,16 @@ DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
 }
 
 // The surface actors: parameter_transporter, its observers (material
-// interactor, parameter setter) and the surface recorder.
-template <typename S>
+// interactor, parameter setter) and the surface recorder.  With an
+// adjoint_tape (adjoint mode) the derivative data of each transported record
+// goes to the tape, and the transport Jacobian restarts at the first
+// transported surface as well.
+template <typename S, typename Tape>
 DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
                                       const detector_view<S>& det,
                                       const field_view<S>& field,
                                       const prop_cfg<S>& cfg,
-                                      record_sink<S>& rec) {
+                                      record_sink<S>& rec, const Tape& tape) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
     const uint32_t cur_sf = nav.current().sf;
@@ -128,13 +131,27 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
     if (transported) {
         bound_state<S>& b = ts.bound;
         bool update_vector = true;
+        S G[4][5];
+        vec3<S> dtds_in;
+        if constexpr (Tape::enabled) {
+            dtds_in = current_dtds(st, field);
+            for (int r = 0; r < 4; ++r) {
+                for (int c = 0; c < 5; ++c) {
+                    G[r][c] = (r == c) ? S(1) : S(0);
+                }
+            }
+        }
         if (b.sf != k_invalid) {
             if (b.sf == cur_sf) {
                 update_vector = false;  // already on the departure surface
             } else {
                 const dev_surface dep = det.surfaces[b.sf];
-                S G[4][5];
-                full_jacobian(det, b, dep, dst, st, current_dtds(st, field), G);
+                if constexpr (Tape::enabled) {
+                    full_jacobian(det, b, dep, dst, st, dtds_in, G);
+                } else {
+                    full_jacobian(det, b, dep, dst, st, current_dtds(st, field),
+                                  G);
+                }
                 ++ts.n_transport;
                 if (fabs(st.path_length) > 0.) {
                     st.jac.reset();
@@ -148,6 +165,12 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
             for (int i = 0; i < 6; ++i) {
                 b.cov[tri6(i, i)] = S(1);
             }
+            if constexpr (Tape::enabled) {
+                S K[5][7];
+                initial_jacobian(det, dst, st, dtds_in, K);
+                tape.write_init(K);
+                st.jac.reset();
+            }
         }
         if (update_vector) {
             free_to_bound(det, dst, st, b.v);
@@ -155,9 +178,19 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
         }
         // pointwise_material_interactor
         bool success = false;
+        S tape_mq = S(1), tape_mc = S(0);
+        const S qop_in = b.v[4];
         if (cfg.act.use_interactor && has_material) {
+            if constexpr (Tape::enabled) {
+                kick_derivatives(det, dst, b.v, cfg.act.mass, ts.q,
+                                 nav.direction, tape_mq, tape_mc);
+            }
             success = interact(det, dst, b, cfg.act, ts.q, nav.direction);
             ts.n_material += success ? 1u : 0u;
+        }
+        if constexpr (Tape::enabled) {
+            tape.write_record(rec.count, G, tape_mq, tape_mc, dtds_in, qop_in,
+                              !update_vector);
         }
         // parameter_setter
         if (success) {
@@ -189,10 +222,10 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
 }
 
 // Run the actor chain once (propagator.hpp:308).
-template <typename S>
+template <typename S, typename Tape>
 DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
                          const field_view<S>& field, const prop_cfg<S>& cfg,
-                         record_sink<S>& rec) {
+                         record_sink<S>& rec, const Tape& tape) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
 
@@ -208,7 +241,7 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
     }
     // parameter_transporter and observers only act on surfaces
     if (nav.is_on_surface()) {
-        run_surface_actors(ts, det, field, cfg, rec);
+        run_surface_actors(ts, det, field, cfg, rec, tape);
     }
 }
 
@@ -231,11 +264,12 @@ DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
 }
 
 // Propagate one track to the end; returns a dprop_track_status code.
-template <typename S>
+template <typename S, typename Tape = no_tape>
 DPROP_HD uint8_t propagate_track(track_state<S>& ts,
                                  const detector_view<S>& det,
                                  const field_view<S>& field,
-                                 const prop_cfg<S>& cfg, record_sink<S>& rec) {
+                                 const prop_cfg<S>& cfg, record_sink<S>& rec,
+                                 const Tape& tape = Tape{}) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
 
@@ -252,7 +286,7 @@ DPROP_HD uint8_t propagate_track(track_state<S>& ts,
             break;
         }
         if (i % 2u == 0u) {
-            run_actors(ts, det, field, cfg, rec);
+            run_actors(ts, det, field, cfg, rec, tape);
             if (!ts.heartbeat) {
                 continue;
             }

@@ -23,16 +23,21 @@
 #include <string>
 #include <vector>
 
+#include "api_common.cuh"
 #include "core/config.hpp"
 #include "core/convert.hpp"
-#include "core/propagate.cuh"
-#include "detray_b200/dprop.h"
+#include "track_io.cuh"
 
 using namespace dprop;
+using dprop::api::io_ptrs;
+using dprop::api::make_io;
+using dprop::api::run_one;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace dprop::api {
 
 dprop_status fail(dprop_status s, const std::string& msg) {
     g_last_error = msg;
@@ -44,13 +49,12 @@ dprop_status cuda_fail(cudaError_t e, const char* what) {
     return (e == cudaErrorMemoryAllocation) ? DPROP_E_OOM : DPROP_E_CUDA;
 }
 
-#define DPROP_CUDA(call)                              \
-    do {                                              \
-        cudaError_t e_ = (call);                      \
-        if (e_ != cudaSuccess) {                      \
-            return cuda_fail(e_, #call);              \
-        }                                             \
-    } while (0)
+}  // namespace dprop::api
+
+using dprop::api::cuda_fail;
+using dprop::api::fail;
+
+namespace {
 
 template <typename T>
 dprop_status upload(const std::vector<T>& h, T** d) {
@@ -65,39 +69,6 @@ dprop_status upload(const std::vector<T>& h, T** d) {
 }
 
 }  // namespace
-
-struct dprop_detector {
-    int device{0};
-    dev_volume* volumes{nullptr};
-    dev_surface* surfaces{nullptr};
-    dev_mask<float>* masks{nullptr};
-    dev_transform<float>* transforms{nullptr};
-    dev_slab<float>* slabs{nullptr};
-    uint32_t* bf_surfaces{nullptr};
-    dev_grid<float>* grids{nullptr};
-    uint32_t* grid_bins{nullptr};
-    uint32_t n_volumes{0}, n_surfaces{0};
-    detector_view<float> view() const {
-        detector_view<float> v;
-        v.volumes = volumes;
-        v.surfaces = surfaces;
-        v.masks = masks;
-        v.transforms = transforms;
-        v.slabs = slabs;
-        v.bf_surfaces = bf_surfaces;
-        v.grids = grids;
-        v.grid_bins = grid_bins;
-        v.n_volumes = n_volumes;
-        v.n_surfaces = n_surfaces;
-        return v;
-    }
-};
-
-struct dprop_field {
-    int device{0};
-    float4* nodes{nullptr};
-    field_view<float> view{};
-};
 
 namespace {
 
@@ -157,109 +128,6 @@ __global__ void direction_key_kernel(const In* __restrict__ dx,
     idx[i] = static_cast<uint32_t>(i);
 }
 
-
-// Device pointers of the inputs/outputs, by value into the kernels
-template <typename In>
-struct io_ptrs {
-    const In* trk[8];
-    uint8_t* status;
-    uint32_t* n_records;
-    uint32_t* n_steps;
-    uint32_t* n_trials;
-    float* path_length;
-    float* final_free[8];
-    uint64_t* rec_barcode;
-    float* rec_bound[6];
-    float* rec_cov[21];
-    float* rec_path;
-    uint8_t* rec_flags;
-    uint32_t* n_isect;
-    uint32_t* n_transport;
-    uint32_t* n_material;
-};
-
-template <typename In>
-io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
-    io_ptrs<In> io{};
-    for (int i = 0; i < 3; ++i) {
-        io.trk[i] = static_cast<const In*>(t.pos[i]);
-        io.trk[4 + i] = static_cast<const In*>(t.dir[i]);
-    }
-    io.trk[3] = static_cast<const In*>(t.time);
-    io.trk[7] = static_cast<const In*>(t.qop);
-    io.status = r.status;
-    io.n_records = r.n_records;
-    io.n_steps = r.n_steps;
-    io.n_trials = r.n_trials;
-    io.path_length = static_cast<float*>(r.path_length);
-    for (int i = 0; i < 8; ++i) {
-        io.final_free[i] = static_cast<float*>(r.final_free[i]);
-    }
-    io.rec_barcode = r.rec_barcode;
-    for (int i = 0; i < 6; ++i) {
-        io.rec_bound[i] = static_cast<float*>(r.rec_bound[i]);
-    }
-    for (int i = 0; i < 21; ++i) {
-        io.rec_cov[i] = static_cast<float*>(r.rec_cov[i]);
-    }
-    io.rec_path = static_cast<float*>(r.rec_path);
-    io.rec_flags = r.rec_flags;
-    io.n_isect = r.n_intersections;
-    io.n_transport = r.n_transports;
-    io.n_material = r.n_material;
-    return io;
-}
-
-template <typename In>
-__device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
-                                        const detector_view<float>& det,
-                                        const field_view<float>& field,
-                                        const prop_cfg<float>& cfg,
-                                        const io_ptrs<In>& io) {
-    const vec3<float> pos{static_cast<float>(io.trk[0][t]),
-                          static_cast<float>(io.trk[1][t]),
-                          static_cast<float>(io.trk[2][t])};
-    const vec3<float> dir{static_cast<float>(io.trk[4][t]),
-                          static_cast<float>(io.trk[5][t]),
-                          static_cast<float>(io.trk[6][t])};
-    const float time = static_cast<float>(io.trk[3][t]);
-    const float qop = static_cast<float>(io.trk[7][t]);
-
-    track_state<float> ts;
-    init_track_state(ts, pos, time, dir, qop, cfg);
-
-    record_sink<float> rec;
-    rec.barcode = io.rec_barcode;
-    for (int i = 0; i < 6; ++i) {
-        rec.bound[i] = io.rec_bound[i];
-    }
-    for (int i = 0; i < 21; ++i) {
-        rec.cov[i] = io.rec_cov[i];
-    }
-    rec.path = io.rec_path;
-    rec.flags = io.rec_flags;
-    rec.n_tracks = n;
-    rec.track = t;
-    rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
-    rec.count = 0u;
-
-    const uint8_t status = propagate_track(ts, det, field, cfg, rec);
-
-    if (io.status) io.status[t] = status;
-    if (io.n_records) io.n_records[t] = rec.count;
-    if (io.n_steps) io.n_steps[t] = ts.step.n_steps;
-    if (io.n_trials) io.n_trials[t] = ts.step.n_trials;
-    if (io.n_isect) io.n_isect[t] = ts.nav.n_isect;
-    if (io.n_transport) io.n_transport[t] = ts.n_transport;
-    if (io.n_material) io.n_material[t] = ts.n_material;
-    if (io.path_length) io.path_length[t] = static_cast<float>(ts.step.path_length);
-    const float fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
-                          ts.step.time,  ts.step.dir.x, ts.step.dir.y,
-                          ts.step.dir.z, ts.step.qop};
-    for (int i = 0; i < 8; ++i) {
-        if (io.final_free[i]) io.final_free[i][t] = fin[i];
-    }
-}
 
 // Threads per CTA and the minimum resident CTAs per SM the register
 // allocation targets (__launch_bounds__); overridable at build time for
@@ -322,12 +190,66 @@ __global__ void __launch_bounds__(k_plain_block, MinBlocks)
     }
 }
 
+}  // namespace
+
+namespace dprop::api {
+
 // register budget of a launch: resident CTAs per SM in {8, 12, 16}
 int occupancy_of(const dprop_launch* lc) {
     const uint32_t v = (lc && lc->ctas_per_sm) ? lc->ctas_per_sm
                                                : static_cast<uint32_t>(DPROP_MIN_BLOCKS);
     return v <= 8u ? 8 : (v <= 12u ? 12 : 16);
 }
+
+size_t sort_scratch_bytes(uint64_t n) {
+    size_t temp = 0;
+    cub::DeviceRadixSort::SortPairs(
+        nullptr, temp, static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 20);
+    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
+    return 4 * arr + temp + 256;
+}
+
+template <typename In>
+dprop_status enqueue_sort(const In* dx, const In* dy, const In* dz,
+                          uint64_t n, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream, const uint32_t** order) {
+    if (n > 0x7fffffffull) {
+        return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
+    }
+    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
+    char* p = static_cast<char*>(scratch);
+    uint32_t* keys_in = reinterpret_cast<uint32_t*>(p);
+    uint32_t* keys_out = reinterpret_cast<uint32_t*>(p + arr);
+    uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + 2 * arr);
+    uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
+    size_t temp = scratch_bytes - 4 * arr;
+    const unsigned int kg = static_cast<unsigned int>((n + 255) / 256);
+    direction_key_kernel<In><<<kg, 256, 0, stream>>>(dx, dy, dz, n, keys_in,
+                                                     idx_in);
+    DPROP_CUDA(cudaGetLastError());
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+        p + 4 * arr, temp, keys_in, keys_out, idx_in, idx_out,
+        static_cast<int>(n), 0, 20, stream));
+    *order = idx_out;
+    return DPROP_OK;
+}
+
+dprop_status enqueue_direction_sort(const float* dx, const float* dy,
+                                    const float* dz, uint64_t n, void* scratch,
+                                    size_t scratch_bytes, cudaStream_t stream,
+                                    const uint32_t** order) {
+    return enqueue_sort<float>(dx, dy, dz, n, scratch, scratch_bytes, stream,
+                               order);
+}
+
+}  // namespace dprop::api
+
+using dprop::api::occupancy_of;
+using dprop::api::sort_scratch_bytes;
+
+namespace {
 
 template <typename In, int MB>
 void launch_plain_mb(unsigned int grid, cudaStream_t st,
@@ -356,16 +278,6 @@ struct launch_scratch {
     unsigned int* queue{nullptr};  // persistent work-queue counter
 };
 
-size_t sort_scratch_bytes(uint64_t n) {
-    size_t temp = 0;
-    cub::DeviceRadixSort::SortPairs(
-        nullptr, temp, static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 20);
-    const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
-    return 4 * arr + temp + 256;
-}
-
 // Enqueue one propagation on a stream using the given scratch; contains no
 // allocation and no synchronisation, so it can be captured into a graph.
 template <typename In>
@@ -381,24 +293,12 @@ dprop_status enqueue_propagation(const dprop_config& c,
     const int mb = occupancy_of(launch_cfg);
     const uint32_t* order = nullptr;
     if (launch_cfg && launch_cfg->sort_tracks) {
-        if (n > 0x7fffffffull) {
-            return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
+        const dprop_status s = dprop::api::enqueue_sort<In>(
+            io.trk[4], io.trk[5], io.trk[6], n, scr.sort, scr.sort_bytes,
+            stream, &order);
+        if (s != DPROP_OK) {
+            return s;
         }
-        const size_t arr = ((n * sizeof(uint32_t)) + 255) & ~size_t(255);
-        char* p = static_cast<char*>(scr.sort);
-        uint32_t* keys_in = reinterpret_cast<uint32_t*>(p);
-        uint32_t* keys_out = reinterpret_cast<uint32_t*>(p + arr);
-        uint32_t* idx_in = reinterpret_cast<uint32_t*>(p + 2 * arr);
-        uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
-        size_t temp = scr.sort_bytes - 4 * arr;
-        const unsigned int kg = static_cast<unsigned int>((n + 255) / 256);
-        direction_key_kernel<In><<<kg, 256, 0, stream>>>(
-            io.trk[4], io.trk[5], io.trk[6], n, keys_in, idx_in);
-        DPROP_CUDA(cudaGetLastError());
-        DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
-            p + 4 * arr, temp, keys_in, keys_out, idx_in, idx_out,
-            static_cast<int>(n), 0, 20, stream));
-        order = idx_out;
     }
     const detector_view<float> dv = det->view();
     if (method == DPROP_METHOD_PERSISTENT) {

@@ -33,6 +33,8 @@ ABI_SYMBOLS = [
     "dprop_detector_create", "dprop_detector_destroy", "dprop_detector_info",
     "dprop_field_create_const", "dprop_field_create_grid",
     "dprop_field_destroy", "dprop_propagate", "dprop_propagate_host",
+    "dprop_propagate_noalloc", "dprop_autotune", "dprop_propagate_adjoint",
+    "dprop_backward",
 ]
 
 
@@ -74,6 +76,14 @@ def load_library() -> C.CDLL:
     lib.dprop_autotune.argtypes = [
         C.POINTER(abi.Config), C.c_void_p, C.c_void_p, C.POINTER(abi.Tracks),
         C.c_uint64, C.POINTER(abi.Launch), C.POINTER(C.c_float), C.c_void_p]
+    lib.dprop_propagate_adjoint.argtypes = [
+        C.POINTER(abi.Config), C.POINTER(abi.Launch), C.c_void_p, C.c_void_p,
+        C.POINTER(abi.Tracks), C.POINTER(abi.Results), C.POINTER(abi.Tape),
+        C.c_uint64, C.c_void_p]
+    lib.dprop_backward.argtypes = [
+        C.POINTER(abi.Config), C.c_void_p, C.POINTER(abi.Tracks),
+        C.POINTER(abi.Results), C.POINTER(abi.Tape),
+        C.POINTER(abi.Gradients), C.c_uint64, C.c_void_p]
     if lib.dprop_abi_version() != abi.DPROP_ABI_VERSION:
         raise PropagationError("detray-b200 library ABI version mismatch")
     _lib = lib

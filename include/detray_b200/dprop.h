@@ -390,6 +390,73 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
 dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
                                  uint32_t* n_surfaces);
 
+/* ------------------------------------------------------------- adjoint mode
+ * dprop_propagate_adjoint and dprop_backward have no counterpart in the
+ * reference.  They give reverse-mode derivatives of a loss L(b_1 .. b_K) of
+ * the recorded bound parameters b_k of each track: dL/d(initial free
+ * parameters) and dL/d(alignment) of the surfaces the records lie on.  The
+ * factors of the chain are the surface-to-surface Jacobians the reference's
+ * parameter transporter forms for its covariance transport
+ * (core/include/detray/propagator/actors/parameter_updater.hpp:422-572), the
+ * start-to-first-surface Jacobian and the derivative of the material
+ * interaction's q/p kick.
+ *
+ * dprop_propagate_adjoint is dprop_propagate (plain kernel; launch->method and
+ * use_graph are ignored) plus a tape of derivative data:
+ *   tape->rec:  float [DPROP_TAPE_RECORD_FLOATS][max_records][n]
+ *   tape->init: float [DPROP_TAPE_TRACK_FLOATS][n]
+ * (device memory, written for every stored transported record and every
+ * track with one).  Unlike dprop_propagate it restarts the transport
+ * Jacobian at the first transported surface too, so the covariance it
+ * records at the second transported surface follows the clean chain rather
+ * than the reference's (which integrates that step's Jacobian from the track
+ * start).  All other results are the same.  The results' rec_bound,
+ * rec_barcode, rec_flags and n_records are required.
+ *
+ * dprop_backward runs the reverse sweep (one thread per track):
+ *   grads->grad_bound[6]: float [max_records][n] (slot-major like rec_bound)
+ *       dL/db_k; NULL entries are zero.
+ *   grads->grad_free[8]: float [n] each, written: dL/d(x, y, z, t, tx, ty,
+ *       tz, q/p) at the start; the direction part is tangent to the unit
+ *       sphere (inputs are unit directions).  NULL entries are skipped.
+ *   grads->grad_align: double [n_surfaces][6], ACCUMULATED (zero it first):
+ *       dL/d(dt_x, dt_y, dt_z, w_x, w_y, w_z) of each planar or ring
+ *       surface, a translation dt and a small rotation w (global axes) about
+ *       the surface centre.  NULL: skipped.
+ * The q/p row and time column of the Jacobians are identity (the reference's
+ * convention), so time derivatives pass straight through.  Step sizes and
+ * navigation decisions are constants of the derivative; the field map's
+ * gradient is not differentiated (as in the reference's Jacobian). */
+#define DPROP_TAPE_RECORD_FLOATS 27u
+#define DPROP_TAPE_TRACK_FLOATS 35u
+
+typedef struct dprop_tape {
+    void* rec;
+    void* init;
+} dprop_tape;
+
+typedef struct dprop_gradients {
+    const void* grad_bound[6];
+    void* grad_free[8];
+    double* grad_align;
+} dprop_gradients;
+
+dprop_status dprop_propagate_adjoint(const dprop_config* cfg,
+                                     const dprop_launch* launch,
+                                     const dprop_detector* det,
+                                     const dprop_field* field,
+                                     const dprop_tracks* tracks,
+                                     const dprop_results* results,
+                                     const dprop_tape* tape, uint64_t n_tracks,
+                                     void* stream);
+
+dprop_status dprop_backward(const dprop_config* cfg, const dprop_detector* det,
+                            const dprop_tracks* tracks,
+                            const dprop_results* results,
+                            const dprop_tape* tape,
+                            const dprop_gradients* grads, uint64_t n_tracks,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif

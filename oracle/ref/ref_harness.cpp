@@ -126,6 +126,7 @@ struct record_buffer {
         uint64_t barcode;
         std::array<double, 6> bound;
         std::array<double, 21> cov;
+        std::array<double, 36> jac;  // accumulated full Jacobian (row-major)
         double path;
         uint8_t flags;
     };
@@ -183,6 +184,17 @@ struct surface_recorder : public base_actor {
                 for (unsigned int j = i; j < 6u; ++j) {
                     r.cov[k++] =
                         static_cast<double>(getter::element(cov, i, j));
+                }
+            }
+            // the reference's product of the surface-to-surface Jacobians
+            // (parameter_transporter, parameter_updater.hpp:373-381)
+            if (st.updater->has_full_jacobian()) {
+                const auto& fj = st.updater->full_jacobian();
+                for (unsigned int i = 0; i < 6u; ++i) {
+                    for (unsigned int j = 0; j < 6u; ++j) {
+                        r.jac[6u * i + j] =
+                            static_cast<double>(getter::element(fj, i, j));
+                    }
                 }
             }
         }
@@ -252,7 +264,7 @@ template <typename det_t, bool with_interactor, typename insp_t>
 int propagate_impl(const det_t& det, const oracle_field::field& field,
                    const dprop_config& cfg, const double* const trk[8],
                    uint64_t n, const dprop_results* out, int n_threads,
-                   int chunk) {
+                   int chunk, double* rec_jac) {
     using types = prop_types<det_t, with_interactor, insp_t>;
     using propagator_t = typename types::propagator_t;
     const propagation::config pcfg = to_ref_config(cfg);
@@ -288,7 +300,10 @@ int propagate_impl(const det_t& det, const oracle_field::field& field,
         buf.recs.reserve(cap);
 
         typename actor::pathlimit_aborter<scalar>::state pl{path_limit};
-        actor::parameter_updater_state<algebra_t> us{pcfg};
+        bound_matrix<algebra_t> full_jac =
+            matrix::identity<bound_matrix<algebra_t>>();
+        actor::parameter_updater_state<algebra_t> us{
+            pcfg, rec_jac != nullptr ? &full_jac : nullptr};
         actor::pointwise_material_interactor<algebra_t>::state is{};
         surface_recorder::state rs{&buf, &us};
 
@@ -392,6 +407,12 @@ int propagate_impl(const det_t& det, const oracle_field::field& field,
             for (unsigned int i = 0; i < 21u; ++i) {
                 host_results::put(out->rec_cov[i], o, r.cov[i]);
             }
+            if (rec_jac != nullptr) {
+                for (unsigned int i = 0; i < 36u; ++i) {
+                    rec_jac[(static_cast<uint64_t>(i) * cap + k) * n + t] =
+                        r.jac[i];
+                }
+            }
         }
     }
     return 0;
@@ -401,21 +422,21 @@ template <typename det_t>
 int dispatch(const det_t& det, const oracle_field::field& f,
              const dprop_config& cfg, const double* const trk[8], uint64_t n,
              const dprop_results* out, int n_threads, int chunk,
-             int with_abort_reasons) {
+             int with_abort_reasons, double* rec_jac) {
     if (cfg.use_material_interactor) {
         if (with_abort_reasons) {
             return propagate_impl<det_t, true, abort_inspector>(
-                det, f, cfg, trk, n, out, n_threads, chunk);
+                det, f, cfg, trk, n, out, n_threads, chunk, rec_jac);
         }
         return propagate_impl<det_t, true, navigation::void_inspector>(
-            det, f, cfg, trk, n, out, n_threads, chunk);
+            det, f, cfg, trk, n, out, n_threads, chunk, rec_jac);
     }
     if (with_abort_reasons) {
         return propagate_impl<det_t, false, abort_inspector>(
-            det, f, cfg, trk, n, out, n_threads, chunk);
+            det, f, cfg, trk, n, out, n_threads, chunk, rec_jac);
     }
     return propagate_impl<det_t, false, navigation::void_inspector>(
-        det, f, cfg, trk, n, out, n_threads, chunk);
+        det, f, cfg, trk, n, out, n_threads, chunk, rec_jac);
 }
 
 }  // namespace
@@ -532,10 +553,25 @@ typedef struct ref_field_desc {
     const float* values;
 } ref_field_desc;
 
+int ref_propagate_jac(void* handle, const ref_field_desc* fd,
+                      const dprop_config* cfg, const double* const* tracks,
+                      uint64_t n, const dprop_results* out, int n_threads,
+                      int chunk, int with_abort_reasons, double* rec_jac);
+
 int ref_propagate(void* handle, const ref_field_desc* fd,
                   const dprop_config* cfg, const double* const* tracks,
                   uint64_t n, const dprop_results* out, int n_threads,
                   int chunk, int with_abort_reasons) {
+    return ref_propagate_jac(handle, fd, cfg, tracks, n, out, n_threads, chunk,
+                             with_abort_reasons, nullptr);
+}
+
+/// ref_propagate plus, per transported record, the reference's accumulated
+/// full Jacobian (rec_jac: [36][max_records][n], row-major 6 x 6 elements).
+int ref_propagate_jac(void* handle, const ref_field_desc* fd,
+                      const dprop_config* cfg, const double* const* tracks,
+                      uint64_t n, const dprop_results* out, int n_threads,
+                      int chunk, int with_abort_reasons, double* rec_jac) {
     try {
         auto* h = static_cast<det_handle*>(handle);
         oracle_field::field f;
@@ -546,13 +582,13 @@ int ref_propagate(void* handle, const ref_field_desc* fd,
         }
         if (auto* toy = std::get_if<std::unique_ptr<toy_det_t>>(&h->det)) {
             return dispatch(**toy, f, *cfg, tracks, n, out, n_threads, chunk,
-                            with_abort_reasons);
+                            with_abort_reasons, rec_jac);
         }
         if (auto* tel = std::get_if<std::unique_ptr<tel_det_t>>(&h->det)) {
             return dispatch(**tel, f, *cfg, tracks, n, out, n_threads, chunk,
-                            with_abort_reasons);
+                            with_abort_reasons, rec_jac);
         }
-        g_error = "ref_propagate: empty detector handle";
+        g_error = "ref_propagate_jac: empty detector handle";
         return 1;
     } catch (const std::exception& e) {
         g_error = e.what();

@@ -89,6 +89,10 @@ def load(precision: str = "f64") -> C.CDLL:
         C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
         C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
         C.c_int, C.c_int]
+    lib.ref_propagate_jac.argtypes = [
+        C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
+        C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
+        C.c_int, C.c_int, C.c_void_p]
     lib.ref_field_eval.argtypes = [C.POINTER(RefFieldDesc),
                                    C.POINTER(C.c_double), C.c_uint64,
                                    C.POINTER(C.c_double)]
@@ -259,9 +263,12 @@ def alloc_results(n: int, max_records: int) -> tuple[dict, abi.Results]:
 
 def propagate(det: RefDetector, field: dict, cfg: abi.Config,
               tracks: np.ndarray, n_threads: int = 0, chunk: int = 1,
-              abort_reasons: bool = True) -> dict:
+              abort_reasons: bool = True, full_jacobian: bool = False) -> dict:
     """Run the reference propagator on ``tracks`` (shape (8, n) float64, the
-    free vector rows [x, y, z, t, tx, ty, tz, q/p])."""
+    free vector rows [x, y, z, t, tx, ty, tz, q/p]).  With ``full_jacobian``
+    the result also holds "rec_jac" [36][max_records][n]: the reference's
+    accumulated full Jacobian (row-major 6 x 6) after each transported
+    record."""
     lib = det._lib
     trk = np.ascontiguousarray(tracks, dtype=np.float64)
     n = trk.shape[1]
@@ -270,8 +277,13 @@ def propagate(det: RefDetector, field: dict, cfg: abi.Config,
     fd, keep = field_desc(field)
     if n_threads <= 0:
         n_threads = os.cpu_count() or 1
-    _check(lib, lib.ref_propagate(det.handle, C.byref(fd), C.byref(cfg), ptrs,
-                                  n, C.byref(r), n_threads, chunk,
-                                  int(abort_reasons)))
+    jac = None
+    if full_jacobian:
+        jac = np.zeros((36, cfg.max_records, n), dtype=np.float64)
+        res["rec_jac"] = jac
+    _check(lib, lib.ref_propagate_jac(
+        det.handle, C.byref(fd), C.byref(cfg), ptrs, n, C.byref(r), n_threads,
+        chunk, int(abort_reasons),
+        jac.ctypes.data_as(C.c_void_p) if jac is not None else None))
     del keep
     return res

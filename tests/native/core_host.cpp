@@ -30,7 +30,8 @@ template <typename S>
 int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         const double* lo, const double* hi, const uint32_t* nn,
         const float* values, const dprop_config* c, const double* const* trk,
-        uint64_t n, const dprop_results* out) {
+        uint64_t n, const dprop_results* out, double* tape_rec = nullptr,
+        double* tape_init = nullptr) {
     const std::string problem = validate_desc(desc);
     if (!problem.empty()) {
         g_err = problem;
@@ -97,7 +98,31 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         rec.track = 0u;
         rec.capacity = cap;
         rec.count = 0u;
-        const uint8_t status = propagate_track(ts, det, f, cfg, rec);
+        uint8_t status;
+        std::vector<S> trec, tinit;
+        if (tape_rec != nullptr) {
+            // adjoint mode: per-track tape scratch, widened below
+            trec.assign(static_cast<size_t>(k_tape_rec) * cap, S(0));
+            tinit.assign(k_tape_init, S(0));
+            adjoint_tape<S> tape{};
+            tape.v.rec = trec.data();
+            tape.v.init = tinit.data();
+            tape.v.n = 1u;
+            tape.v.capacity = cap;
+            tape.track = 0u;
+            status = propagate_track(ts, det, f, cfg, rec, tape);
+            for (int i = 0; i < k_tape_init; ++i) {
+                tape_init[static_cast<uint64_t>(i) * n + t] = tinit[i];
+            }
+            for (int comp = 0; comp < k_tape_rec; ++comp) {
+                for (uint32_t k = 0; k < cap; ++k) {
+                    tape_rec[(static_cast<uint64_t>(comp) * cap + k) * n + t] =
+                        trec[static_cast<size_t>(comp) * cap + k];
+                }
+            }
+        } else {
+            status = propagate_track(ts, det, f, cfg, rec);
+        }
         out->status[t] = status;
         if (out->n_records) out->n_records[t] = rec.count;
         if (out->n_steps) out->n_steps[t] = ts.step.n_steps;
@@ -143,6 +168,73 @@ int core_host_propagate(int precision_bytes, const dprop_detector_desc* desc,
         return run<double>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
     }
     return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
+}
+
+// Adjoint-mode propagation: as core_host_propagate, plus the tape
+// (tape_rec: [k_tape_rec][max_records][n], tape_init: [k_tape_init][n]).
+int core_host_propagate_adjoint(int precision_bytes,
+                                const dprop_detector_desc* desc,
+                                uint32_t field_kind, const double* b,
+                                const double* lo, const double* hi,
+                                const uint32_t* nn, const float* values,
+                                const dprop_config* cfg,
+                                const double* const* trk, uint64_t n,
+                                const dprop_results* out, double* tape_rec,
+                                double* tape_init) {
+    if (tape_rec == nullptr || tape_init == nullptr) {
+        g_err = "tape arrays are required";
+        return 1;
+    }
+    if (precision_bytes == 8) {
+        return run<double>(desc, field_kind, b, lo, hi, nn, values, cfg, trk,
+                           n, out, tape_rec, tape_init);
+    }
+    return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n,
+                      out, tape_rec, tape_init);
+}
+
+// Reverse sweep over the records of core_host_propagate_adjoint (double
+// precision).  grad_bound: 6 slot-major arrays (entries may be NULL);
+// grad_free: 8 arrays of n; grad_align: n_surfaces x 6 (accumulated) or NULL.
+int core_host_backward(const dprop_detector_desc* desc, uint32_t capacity,
+                       const double* const* trk, uint64_t n,
+                       const uint32_t* n_records, const uint64_t* rec_barcode,
+                       const uint8_t* rec_flags,
+                       const double* const* rec_bound, const double* tape_rec,
+                       const double* tape_init,
+                       const double* const* grad_bound,
+                       double* const* grad_free, double* grad_align) {
+    const std::string problem = validate_desc(desc);
+    if (!problem.empty()) {
+        g_err = problem;
+        return 1;
+    }
+    const host_tables<double> tables = convert_desc<double>(desc);
+    const detector_view<double> det = tables.view();
+    tape_view<double> tp{};
+    tp.rec = const_cast<double*>(tape_rec);
+    tp.init = const_cast<double*>(tape_init);
+    tp.n = n;
+    tp.capacity = capacity;
+    for (uint64_t t = 0; t < n; ++t) {
+        double g[8];
+        const vec3<double> dir0{trk[4][t], trk[5][t], trk[6][t]};
+        backward_track(det, tp, t, n_records[t], rec_barcode, rec_flags,
+                       rec_bound, grad_bound, dir0, g,
+                       [&](uint32_t sf, const double* v) {
+                           if (grad_align != nullptr) {
+                               for (int j = 0; j < 6; ++j) {
+                                   grad_align[6u * sf + j] += v[j];
+                               }
+                           }
+                       });
+        for (int i = 0; i < 8; ++i) {
+            if (grad_free[i] != nullptr) {
+                grad_free[i][t] = g[i];
+            }
+        }
+    }
+    return 0;
 }
 }
 
