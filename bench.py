@@ -58,6 +58,9 @@ def parse_args():
                    help="propagate in input order instead of direction order")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true",
+                   help="skip the adjoint/forward cost measurement")
+    p.add_argument("--adjoint-tracks", type=int, default=262_144)
     p.add_argument("--seed", type=int, default=20241203)
     return p.parse_args()
 
@@ -75,6 +78,123 @@ def make_tracks(n, seed):
     return tracks.toy_tracks(n, seed=seed, pt_range=(1.0, 100.0),
                              eta_range=(-4.0, 4.0),
                              vertex_sigma=(0.1, 0.1, 50.0))
+
+
+# ---------------------------------------------------- adjoint workload
+ADJOINT_WORKLOAD = ("toy_4brl_7edc_solenoid_map_262k_muons_pt0.5-50_"
+                    "residual_loss_vs_aligned_targets")
+
+
+def adjoint_cost(args, dev, stream, steps=10, warmup=3):
+    """Adjoint / forward time ratio on the alignment workload: toy detector
+    in the solenoid field map, muons with pT uniform in [0.5, 50] GeV; targets
+    are the local positions recorded by a propagation of perturbed tracks
+    (position +- 10 um, angles +- 0.1 mrad, q/p +- 0.1 %) through the
+    detector with every sensitive module shifted by N(0, 10 um) per axis
+    (seed 12345); loss = sum over matching sensitive records of the squared
+    local residuals.  One adjoint step = adjoint-mode propagation, the
+    residual and its gradient, and the reverse sweep (gradients for the
+    initial free parameters and 6 alignment values per surface); one
+    forward step = the plain propagation of the same tracks.  Each side is
+    timed at its best register budget."""
+    import torch
+
+    from detray_b200 import adjoint, alignment, fields, geometry, propagator
+    from detray_b200 import tracks as tracks_mod
+
+    n = args.adjoint_tracks
+    tables = geometry.load_geometry("toy_4brl_7edc")
+    rng = np.random.default_rng(12345)
+    sens = np.nonzero(tables["surfaces"]["kind"] == 1)[0]
+    shifts = {int(s): np.concatenate([rng.normal(0.0, 0.010, 3), np.zeros(3)])
+              for s in sens}
+    det0 = propagator.Detector(tables, dev.index)
+    det1 = propagator.Detector(alignment.apply_alignment(tables, shifts),
+                               dev.index)
+    field = propagator.Field.grid(fields.solenoid_map(), dev.index)
+    cfg = workload_config()
+    trk0 = tracks_mod.toy_tracks(n, seed=args.seed + 4, pt_range=(0.5, 50.0),
+                                 eta_range=(-4.0, 4.0), pt_log_uniform=False)
+    trk1 = trk0.copy()
+    trk1[0:3] += rng.normal(0.0, 0.010, (3, n))
+    phi = np.arctan2(trk0[5], trk0[4]) + rng.normal(0.0, 1e-4, n)
+    th = np.arccos(np.clip(trk0[6], -1, 1)) + rng.normal(0.0, 1e-4, n)
+    trk1[4:7] = np.stack([np.cos(phi) * np.sin(th), np.sin(phi) * np.sin(th),
+                          np.cos(th)])
+    trk1[7] *= 1.0 + rng.normal(0.0, 1e-3, n)
+    t0 = torch.tensor(trk0, dtype=torch.float32, device=dev)
+    t1 = torch.tensor(trk1, dtype=torch.float32, device=dev)
+    tgt = propagator.propagate(cfg, det1, field, t1,
+                               launch=propagator.make_launch(sort_tracks=1),
+                               stream=stream)
+    tgt_bound = tgt.tensors["rec_bound"][:2].clone()
+    tgt_bc = tgt.tensors["rec_barcode"].clone()
+    slot = torch.arange(cfg.max_records, device=dev)[:, None]
+    tgt_ok = ((slot < tgt.tensors["n_records"].clamp(max=cfg.max_records)[None])
+              & ((tgt.tensors["rec_flags"] & 1) != 0))
+    sens_lut = torch.zeros(det0.n_surfaces, dtype=torch.bool, device=dev)
+    sens_lut[torch.as_tensor(sens, device=dev)] = True
+
+    def residual_grad(rec):
+        t = rec.results.tensors
+        bc = t["rec_barcode"]
+        sf = (bc >> 27) & 0x1FFFFF
+        m = adjoint.rec_mask(rec) & tgt_ok & (bc == tgt_bc)
+        m &= sens_lut[sf.clamp(max=det0.n_surfaces - 1)]
+        r = (t["rec_bound"][:2] - tgt_bound) * m[None]
+        g = torch.zeros_like(t["rec_bound"])
+        g[:2] = 2.0 * r
+        return (r * r).sum(), g, m
+
+    def time_it(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    res = propagator.alloc_device_results(n, cfg.max_records, dev)
+    fwd_ms, adj_ms = {}, {}
+    out = {}
+    for ctas in (12, 16):
+        lc = propagator.make_launch(sort_tracks=1, ctas_per_sm=ctas)
+        fwd_ms[ctas] = time_it(lambda: propagator.propagate(
+            cfg, det0, field, t0, results=res, launch=lc, stream=stream))
+
+        def adj_step():
+            rec = adjoint.propagate_adjoint(cfg, det0, field, t0, launch=lc,
+                                            stream=stream)
+            loss, g, m = residual_grad(rec)
+            gf, ga = adjoint.backward(cfg, det0, rec, g, stream=stream)
+            out.update(loss=loss, gf=gf, ga=ga, m=m)
+
+        adj_ms[ctas] = time_it(adj_step)
+    best_f = min(fwd_ms.values())
+    best_a = min(adj_ms.values())
+    ga = out["ga"]
+    # the alignment gradient of the loss should point along the true shifts
+    g_sens = ga[torch.as_tensor(sens, device=dev), :3].cpu().numpy()
+    true = np.stack([shifts[int(s)][:3] for s in sens])
+    hit = np.abs(g_sens).sum(axis=1) > 0
+    cos = float(-(g_sens[hit] * true[hit]).sum() /
+                (np.linalg.norm(g_sens[hit]) * np.linalg.norm(true[hit]) + 1e-30))
+    return {"workload": ADJOINT_WORKLOAD, "tracks": n,
+            "forward_ms": round(best_f, 3), "adjoint_ms": round(best_a, 3),
+            "ratio": round(best_a / best_f, 3),
+            "forward_ms_by_ctas": {k: round(v, 3) for k, v in fwd_ms.items()},
+            "adjoint_ms_by_ctas": {k: round(v, 3) for k, v in adj_ms.items()},
+            "loss": float(out["loss"]),
+            "residual_records": int(out["m"].sum()),
+            "surfaces_with_gradient": int(hit.sum()),
+            "cos_grad_vs_true_shift": round(cos, 4),
+            "adjoint_includes": "adjoint-mode propagation + residual + "
+                                "reverse sweep (fp64 alignment atomics)"}
 
 
 # ----------------------------------------------------------------- clocks
@@ -345,6 +465,10 @@ def run_ours(args):
                "api": "dprop_propagate_host, jagged records, 2-stream "
                       "chunked pipeline, pinned host buffers"}
 
+    adj = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adj = adjoint_cost(args, dev, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -374,6 +498,7 @@ def run_ours(args):
                        "l2": "per step ~1.5 GB of records written (> 126 MB "
                              "L2): inputs are re-read from HBM"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "adjoint": adj,
             # our kernels per step: the propagation kernel, plus the direction
             # key kernel when sorting (the radix sort itself is CUB's)
             "gpu_launches": args.steps * (1 + int(lc.sort_tracks)),

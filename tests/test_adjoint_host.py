@@ -156,6 +156,41 @@ def test_toy_gradients_match_finite_differences(core_host):
     assert len(arel) >= 12 and max(arel) < 1e-3 and np.median(arel) < 1e-4
 
 
+@pytest.fixture(scope="module")
+def solenoid():
+    from detray_b200 import fields
+    return fields.solenoid_map()
+
+
+def test_field_map_gradients_match_finite_differences(core_host, solenoid):
+    """Toy detector in the solenoid field map.  The Jacobians, like the
+    reference's without use_field_gradient, do not differentiate the field
+    map; inside the toy detector the map varies slowly enough that the
+    finite differences still agree to < 5e-3 (median ~3e-6)."""
+    tables = geometry.load_geometry("toy_4brl_7edc")
+    cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                          step_constraint=2.0)
+    trk = tracks.toy_tracks(24, seed=12, pt_range=(0.5, 50.0),
+                            eta_range=(-2.5, 2.5), pt_log_uniform=False)
+    res, tape = ah.forward(core_host, tables, cfg, trk, field=solenoid)
+    W = ah.random_weights(res, cfg.max_records, seed=3)
+    gfree, _ = ah.backward(core_host, tables, cfg, trk, res, tape, W)
+    rels = []
+    for which in (0, 1, 2, "phi", "theta", 7):
+        h = STEPS[which]
+        rp, _ = ah.forward(core_host, tables, cfg, _perturbed(trk, which, h),
+                           field=solenoid, adjoint=False)
+        rm, _ = ah.forward(core_host, tables, cfg, _perturbed(trk, which, -h),
+                           field=solenoid, adjoint=False)
+        same = ah.same_records(rp, rm)
+        fd = ah.loss_difference(rp, rm, W) / (2 * h)
+        an = _analytic(gfree, trk, which)
+        rel = _rel(fd, an, 1e-6 * np.abs(an).max() + 1e-12)[same]
+        assert same.sum() >= 20 and rel.max() < 5e-3, (which, rel)
+        rels.append(rel)
+    assert np.median(np.concatenate(rels)) < 2e-5
+
+
 def test_loss_on_one_record_component(core_host):
     """d(b_k)/d(x0) for single records equals the finite difference of the
     recorded parameter (telescope, q/p row and time: identity through the
@@ -187,25 +222,28 @@ def test_loss_on_one_record_component(core_host):
     np.testing.assert_array_equal(g[3], np.ones(trk.shape[1]))
 
 
-@pytest.mark.parametrize("kind", ["toy", "telescope"])
-def test_tape_jacobians_match_reference(core_host, oracle, kind):
+@pytest.mark.parametrize("kind", ["toy", "telescope", "toy_map"])
+def test_tape_jacobians_match_reference(core_host, oracle, solenoid, kind):
     """Every surface-to-surface Jacobian on the tape equals the reference's:
     its accumulated full Jacobian P_k after record k gives the step factor
     P_k P_{k-1}^-1 (from the third transported surface on: the reference
     does not restart the transport Jacobian at the first surface, so its
     second factor integrates from the track start)."""
-    if kind == "toy":
+    field = {"kind": "const", "b": (0, 0, 2 * T)}
+    if kind.startswith("toy"):
         det = oracle.build_toy()
         cfg = abi.make_config(max_records=32, search_window=(3, 3))
         trk = tracks.toy_tracks(300, seed=4)
+        if kind == "toy_map":
+            field = solenoid
     else:
         det = oracle.build_telescope()
         cfg = abi.make_config(max_records=16)
         trk = tracks.telescope_tracks(200, seed=3)
     tables = det.tables()
-    ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)}, cfg,
-                           trk, full_jacobian=True)
-    res, tape = ah.forward(core_host, tables, cfg, trk)
+    ref = oracle.propagate(det, field, cfg, trk, full_jacobian=True)
+    res, tape = ah.forward(core_host, tables, cfg, trk,
+                           field=None if field.get("kind") == "const" else field)
     np.testing.assert_array_equal(ref["rec_barcode"], res["rec_barcode"])
     mask = ah.transported_mask(res, cfg.max_records)
     compared = 0
