@@ -85,7 +85,7 @@ ADJOINT_WORKLOAD = ("toy_4brl_7edc_solenoid_map_262k_muons_pt0.5-50_"
                     "residual_loss_vs_aligned_targets")
 
 
-def adjoint_cost(args, dev, stream, steps=10, warmup=3):
+def adjoint_cost(args, dev, stream, world=1, rank=0, steps=10, warmup=3):
     """Adjoint / forward time ratio on the alignment workload: toy detector
     in the solenoid field map, muons with pT uniform in [0.5, 50] GeV; targets
     are the local positions recorded by a propagation of perturbed tracks
@@ -96,10 +96,14 @@ def adjoint_cost(args, dev, stream, steps=10, warmup=3):
     residual and its gradient, and the reverse sweep (gradients for the
     initial free parameters and 6 alignment values per surface); one
     forward step = the plain propagation of the same tracks.  Each side is
-    timed at its best register budget."""
+    timed at its best register budget.  With several GPUs every rank runs
+    its own tracks and the adjoint step ends with the all-reduce of the
+    alignment gradient and the loss over NCCL; times are the max over
+    ranks."""
     import torch
 
-    from detray_b200 import adjoint, alignment, fields, geometry, propagator
+    from detray_b200 import (adjoint, alignment, fields, geometry, propagator,
+                             sharding)
     from detray_b200 import tracks as tracks_mod
 
     n = args.adjoint_tracks
@@ -113,7 +117,8 @@ def adjoint_cost(args, dev, stream, steps=10, warmup=3):
                                dev.index)
     field = propagator.Field.grid(fields.solenoid_map(), dev.index)
     cfg = workload_config()
-    trk0 = tracks_mod.toy_tracks(n, seed=args.seed + 4, pt_range=(0.5, 50.0),
+    trk0 = tracks_mod.toy_tracks(n, seed=args.seed + 4 + 1000 * rank,
+                                 pt_range=(0.5, 50.0),
                                  eta_range=(-4.0, 4.0), pt_log_uniform=False)
     trk1 = trk0.copy()
     trk1[0:3] += rng.normal(0.0, 0.010, (3, n))
@@ -172,9 +177,13 @@ def adjoint_cost(args, dev, stream, steps=10, warmup=3):
                                             stream=stream)
             loss, g, m = residual_grad(rec)
             gf, ga = adjoint.backward(cfg, det0, rec, g, stream=stream)
+            if world > 1:
+                ga, loss = sharding.allreduce_alignment(ga, loss)
             out.update(loss=loss, gf=gf, ga=ga, m=m)
 
         adj_ms[ctas] = time_it(adj_step)
+    fwd_ms = {k: max_over_ranks(v, world) for k, v in fwd_ms.items()}
+    adj_ms = {k: max_over_ranks(v, world) for k, v in adj_ms.items()}
     best_f = min(fwd_ms.values())
     best_a = min(adj_ms.values())
     ga = out["ga"]
@@ -184,7 +193,8 @@ def adjoint_cost(args, dev, stream, steps=10, warmup=3):
     hit = np.abs(g_sens).sum(axis=1) > 0
     cos = float(-(g_sens[hit] * true[hit]).sum() /
                 (np.linalg.norm(g_sens[hit]) * np.linalg.norm(true[hit]) + 1e-30))
-    return {"workload": ADJOINT_WORKLOAD, "tracks": n,
+    return {"workload": ADJOINT_WORKLOAD, "tracks_per_gpu": n,
+            "n_gpus": world,
             "forward_ms": round(best_f, 3), "adjoint_ms": round(best_a, 3),
             "ratio": round(best_a / best_f, 3),
             "forward_ms_by_ctas": {k: round(v, 3) for k, v in fwd_ms.items()},
@@ -466,8 +476,8 @@ def run_ours(args):
                       "chunked pipeline, pinned host buffers"}
 
     adj = None
-    if rank == 0 and world == 1 and not args.no_adjoint:
-        adj = adjoint_cost(args, dev, stream)
+    if not args.no_adjoint:
+        adj = adjoint_cost(args, dev, stream, world, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

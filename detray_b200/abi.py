@@ -8,6 +8,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 DPROP_ABI_VERSION = 1
 DPROP_INVALID_INDEX = 0xFFFFFFFF
 DPROP_INVALID_LINK = 0xFFFF
@@ -267,7 +269,9 @@ def default_config_values() -> dict:
         use_path_limit_aborter=1,
         use_material_interactor=1,
         record_all_surfaces=0,
-        mass=0.1056583755,
+        # the reference's muon mass, a float product
+        # (definitions/pdg_particle.hpp:84: 105.6583755f * unit<float>::MeV)
+        mass=float(np.float32(np.float32(105.6583755) * np.float32(1e-3))),
         pdg=13,
         max_records=32,
         max_iterations=200000,

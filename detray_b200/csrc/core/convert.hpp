@@ -110,6 +110,23 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
     return {};
 }
 
+// One material slab descriptor -> the device slab.
+template <typename S>
+dev_slab<S> convert_slab(const dprop_slab_desc& s) {
+    dev_slab<S> o{};
+    o.thickness = static_cast<S>(s.thickness);
+    o.thickness_in_X0 = static_cast<S>(s.thickness_in_X0);
+    o.molar_electron_density = static_cast<S>(s.molar_electron_density);
+    o.mean_excitation_energy = static_cast<S>(s.mean_excitation_energy);
+    o.density_a = static_cast<S>(s.density_a);
+    o.density_m = static_cast<S>(s.density_m);
+    o.density_x0 = static_cast<S>(s.density_x0);
+    o.density_x1 = static_cast<S>(s.density_x1);
+    o.density_c = static_cast<S>(s.density_c);
+    o.has_density_effect = s.has_density_effect ? S(1) : S(0);
+    return o;
+}
+
 template <typename S>
 host_tables<S> convert_desc(const dprop_detector_desc* d) {
     host_tables<S> t;
@@ -157,19 +174,7 @@ host_tables<S> convert_desc(const dprop_detector_desc* d) {
     }
     t.slabs.resize(d->n_slabs);
     for (uint32_t i = 0; i < d->n_slabs; ++i) {
-        const dprop_slab_desc& s = d->slabs[i];
-        dev_slab<S> o{};
-        o.thickness = static_cast<S>(s.thickness);
-        o.thickness_in_X0 = static_cast<S>(s.thickness_in_X0);
-        o.molar_electron_density = static_cast<S>(s.molar_electron_density);
-        o.mean_excitation_energy = static_cast<S>(s.mean_excitation_energy);
-        o.density_a = static_cast<S>(s.density_a);
-        o.density_m = static_cast<S>(s.density_m);
-        o.density_x0 = static_cast<S>(s.density_x0);
-        o.density_x1 = static_cast<S>(s.density_x1);
-        o.density_c = static_cast<S>(s.density_c);
-        o.has_density_effect = s.has_density_effect ? S(1) : S(0);
-        t.slabs[i] = o;
+        t.slabs[i] = convert_slab<S>(d->slabs[i]);
     }
     t.bf_surfaces.assign(d->bf_surfaces, d->bf_surfaces + d->n_bf_surfaces);
     t.grids.resize(d->n_grids);

@@ -845,7 +845,9 @@ void dprop_config_default(dprop_config* c) {
     c->use_path_limit_aborter = 1;
     c->use_material_interactor = 1;
     c->record_all_surfaces = 0;
-    c->mass = 0.1056583755f;
+    // the reference's muon mass, a float product
+    // (definitions/pdg_particle.hpp:84: 105.6583755f * unit<float>::MeV)
+    c->mass = 105.6583755f * 1e-3f;
     c->pdg = 13;
     c->max_records = 32u;
     c->max_iterations = 200000u;

@@ -8,3 +8,5 @@ m = 1000.0
 MeV = 1e-3
 GeV = 1.0
 T = 0.000299792458
+cm2 = cm * cm
+g = 1.0 / 1.782662e-24  # GeV / c^2

@@ -129,6 +129,30 @@ struct mask_copier {
     }
 };
 
+/// One homogeneous detray material slab as a dprop_slab_desc.
+template <typename slab_t>
+dprop_slab_desc to_slab_desc(const slab_t& slab) {
+    const auto& mat = slab.get_material();
+    dprop_slab_desc d{};
+    d.thickness = static_cast<double>(slab.thickness());
+    d.thickness_in_X0 = static_cast<double>(slab.thickness_in_X0());
+    d.X0 = static_cast<double>(mat.X0());
+    d.molar_electron_density =
+        static_cast<double>(mat.molar_electron_density());
+    d.mean_excitation_energy =
+        static_cast<double>(mat.mean_excitation_energy());
+    d.has_density_effect = mat.has_density_effect_data() ? 1u : 0u;
+    if (mat.has_density_effect_data()) {
+        const auto& de = mat.density_effect_data();
+        d.density_a = static_cast<double>(de.get_A_density());
+        d.density_m = static_cast<double>(de.get_M_density());
+        d.density_x0 = static_cast<double>(de.get_X0_density());
+        d.density_x1 = static_cast<double>(de.get_X1_density());
+        d.density_c = static_cast<double>(de.get_C_density());
+    }
+    return d;
+}
+
 /// Material-store visitor: homogeneous slabs only.
 struct slab_copier {
     template <typename mat_group_t, typename index_t>
@@ -139,25 +163,7 @@ struct slab_copier {
                           s.thickness_in_X0();
                           s.get_material();
                       }) {
-            const auto& slab = group[idx];
-            const auto& mat = slab.get_material();
-            dprop_slab_desc d{};
-            d.thickness = static_cast<double>(slab.thickness());
-            d.thickness_in_X0 = static_cast<double>(slab.thickness_in_X0());
-            d.X0 = static_cast<double>(mat.X0());
-            d.molar_electron_density =
-                static_cast<double>(mat.molar_electron_density());
-            d.mean_excitation_energy =
-                static_cast<double>(mat.mean_excitation_energy());
-            d.has_density_effect = mat.has_density_effect_data() ? 1u : 0u;
-            if (mat.has_density_effect_data()) {
-                const auto& de = mat.density_effect_data();
-                d.density_a = static_cast<double>(de.get_A_density());
-                d.density_m = static_cast<double>(de.get_M_density());
-                d.density_x0 = static_cast<double>(de.get_X0_density());
-                d.density_x1 = static_cast<double>(de.get_X1_density());
-                d.density_c = static_cast<double>(de.get_C_density());
-            }
+            const dprop_slab_desc d = to_slab_desc(group[idx]);
             sf.material = static_cast<uint32_t>(out.slabs.size());
             out.slabs.push_back(d);
         } else {

@@ -25,6 +25,9 @@
  */
 #include "detray/definitions/algebra.hpp"
 #include "detray/definitions/pdg_particle.hpp"
+#include "detray/material/interaction.hpp"
+#include "detray/material/material_slab.hpp"
+#include "detray/material/predefined_materials.hpp"
 #include "detray/navigation/caching_navigator.hpp"
 #include "detray/propagator/actor_chain.hpp"
 #include "detray/propagator/actors/aborters.hpp"
@@ -441,6 +444,56 @@ int dispatch(const det_t& det, const oracle_field::field& f,
 
 }  // namespace
 
+namespace {
+
+/// A predefined reference material by name (material/predefined_materials.hpp);
+/// false for an unknown name.
+template <typename F>
+bool with_material(const std::string& name, F&& f) {
+#define DPROP_REF_MATERIAL(m)      \
+    if (name == #m) {              \
+        f(m<scalar>());            \
+        return true;               \
+    }
+    DPROP_REF_MATERIAL(hydrogen_liquid)
+    DPROP_REF_MATERIAL(hydrogen_gas)
+    DPROP_REF_MATERIAL(helium_gas)
+    DPROP_REF_MATERIAL(beryllium)
+    DPROP_REF_MATERIAL(aluminium)
+    DPROP_REF_MATERIAL(silicon)
+    DPROP_REF_MATERIAL(silicon_with_ded)
+    DPROP_REF_MATERIAL(argon_gas)
+    DPROP_REF_MATERIAL(argon_liquid)
+    DPROP_REF_MATERIAL(iron)
+    DPROP_REF_MATERIAL(iron_with_ded)
+    DPROP_REF_MATERIAL(copper)
+    DPROP_REF_MATERIAL(copper_with_ded)
+    DPROP_REF_MATERIAL(tungsten)
+    DPROP_REF_MATERIAL(gold)
+    DPROP_REF_MATERIAL(cesium_iodide)
+    DPROP_REF_MATERIAL(cesium_iodide_with_ded)
+#undef DPROP_REF_MATERIAL
+    return false;
+}
+
+pdg_particle<scalar> particle_of(int pdg) {
+    if (pdg == 11) {
+        return electron<scalar>();
+    }
+    if (pdg == -11) {
+        return positron<scalar>();
+    }
+    if (pdg == 211) {
+        return pion_plus<scalar>();
+    }
+    if (pdg == -13) {
+        return antimuon<scalar>();
+    }
+    return muon<scalar>();
+}
+
+}  // namespace
+
 // ======================================================================
 extern "C" {
 
@@ -594,6 +647,43 @@ int ref_propagate_jac(void* handle, const ref_field_desc* fd,
         g_error = e.what();
         return 1;
     }
+}
+
+/// A slab of `thickness` mm of a predefined material as the product's slab
+/// descriptor, plus the material's mass density.
+int ref_material_slab(const char* name, double thickness,
+                      dprop_slab_desc* out, double* mass_density) {
+    const bool ok = with_material(name, [&](const auto& mat) {
+        const material_slab<scalar> slab(mat, static_cast<scalar>(thickness));
+        *out = dprop::adapter_detail::to_slab_desc(slab);
+        *mass_density = static_cast<double>(mat.mass_density());
+    });
+    if (!ok) {
+        g_error = std::string("unknown material ") + name;
+        return 1;
+    }
+    return 0;
+}
+
+/// The reference's mean Bethe-Bloch stopping power of a particle with
+/// momentum p (GeV, detray units) in a predefined material, and its q/p
+/// derivative (interaction::compute_bethe_bloch / derive_bethe_bloch,
+/// material/interaction.hpp:44-153).  dedx: detray units (energy / length).
+int ref_bethe(const char* name, int pdg, double p, double* dedx,
+              double* ddedx_dqop) {
+    const pdg_particle<scalar> ptc = particle_of(pdg);
+    const bool ok = with_material(name, [&](const auto& mat) {
+        const scalar qop = ptc.charge() / static_cast<scalar>(p);
+        const interaction<scalar> I;
+        const detail::relativistic_quantities<scalar> rq(ptc, qop);
+        *dedx = static_cast<double>(I.compute_bethe_bloch(mat, ptc, rq));
+        *ddedx_dqop = static_cast<double>(I.derive_bethe_bloch(mat, ptc, rq));
+    });
+    if (!ok) {
+        g_error = std::string("unknown material ") + name;
+        return 1;
+    }
+    return 0;
 }
 
 /// Evaluate the oracle field at n points (for field-map tests).

@@ -93,6 +93,11 @@ def load(precision: str = "f64") -> C.CDLL:
         C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
         C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
         C.c_int, C.c_int, C.c_void_p]
+    lib.ref_material_slab.argtypes = [C.c_char_p, C.c_double,
+                                      C.POINTER(abi.SlabDesc),
+                                      C.POINTER(C.c_double)]
+    lib.ref_bethe.argtypes = [C.c_char_p, C.c_int, C.c_double,
+                              C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.ref_field_eval.argtypes = [C.POINTER(RefFieldDesc),
                                    C.POINTER(C.c_double), C.c_uint64,
                                    C.POINTER(C.c_double)]
@@ -287,3 +292,23 @@ def propagate(det: RefDetector, field: dict, cfg: abi.Config,
         jac.ctypes.data_as(C.c_void_p) if jac is not None else None))
     del keep
     return res
+
+
+def material_slab(name: str, thickness: float, precision="f64"):
+    """(slab descriptor, mass density) of a predefined reference material."""
+    lib = load(precision)
+    d = abi.SlabDesc()
+    rho = C.c_double()
+    _check(lib, lib.ref_material_slab(name.encode(), thickness, C.byref(d),
+                                      C.byref(rho)))
+    return d, rho.value
+
+
+def bethe(name: str, pdg: int, p: float, precision="f64"):
+    """The reference's mean stopping power (detray units) and its q/p
+    derivative for a particle of momentum p in a predefined material."""
+    lib = load(precision)
+    v = C.c_double()
+    dv = C.c_double()
+    _check(lib, lib.ref_bethe(name.encode(), pdg, p, C.byref(v), C.byref(dv)))
+    return v.value, dv.value

@@ -1,0 +1,56 @@
+"""Extract the reference's known-answer vectors for the propagation path
+into JSON fixtures (run where the reference checkout exists; the fixtures
+are committed so the tests do not need it):
+
+  bethe_pdg.json  muon mean dE/dx against the PDG tables, the cases of
+                  tests/unit_tests/cpu/material/bethe_equation.cpp (the
+                  instantiations that are commented out there are skipped:
+                  the reference does not meet its 5 % bound on them).
+
+Usage: python tests/golden/make_golden.py [reference checkout]
+"""
+from __future__ import annotations
+
+import json
+import re
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+
+def strip_comments_keep_lines(text: str) -> str:
+    """Blank out /* */ and // comments, keeping line numbers."""
+    def blank(m):
+        return re.sub(r"[^\n]", " ", m.group(0))
+    text = re.sub(r"/\*.*?\*/", blank, text, flags=re.S)
+    return re.sub(r"//[^\n]*", blank, text)
+
+
+def bethe_cases(ref: Path) -> list[dict]:
+    rel = "tests/unit_tests/cpu/material/bethe_equation.cpp"
+    text = strip_comments_keep_lines((ref / rel).read_text())
+    pat = re.compile(
+        r"make_tuple\(\s*(\w+)<scalar>\(\)\s*,\s*(\w+)<scalar>\(\)\s*,\s*"
+        r"([0-9.eE+-]+)f\s*\*\s*unit<scalar>::GeV\s*,\s*([0-9.eE+-]+)f\s*\)",
+        re.S)
+    out = []
+    for m in pat.finditer(text):
+        line = text.count("\n", 0, m.start()) + 1
+        out.append({"material": m.group(1), "particle": m.group(2),
+                    "p_gev": float(m.group(3)),
+                    "dedx_mev_cm2_per_g": float(m.group(4)),
+                    "source": f"{rel}:{line}"})
+    return out
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    ref = Path(argv[0]) if argv else Path("/root/reference")
+    cases = bethe_cases(ref)
+    (HERE / "bethe_pdg.json").write_text(json.dumps(cases, indent=1) + "\n")
+    print(f"bethe_pdg.json: {len(cases)} cases")
+
+
+if __name__ == "__main__":
+    main()

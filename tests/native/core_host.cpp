@@ -277,3 +277,16 @@ extern "C" int core_host_field_eval(int precision_bytes, const double* lo,
     }
     return 0;
 }
+
+// Mean Bethe-Bloch stopping power (energy per length) and its q/p
+// derivative of the core's material physics for one slab, in double.
+extern "C" int core_host_bethe(const dprop_slab_desc* slab, double mass,
+                               double qop, double q, double* dedx,
+                               double* ddedx_dqop) {
+    const dev_slab<double> s = convert_slab<double>(*slab);
+    const rel_quantities<double> rq = make_rq(mass, qop, q);
+    const double bb = bethe_bloch(s, rq);
+    *dedx = bb;
+    *ddedx_dqop = bethe_bloch_dqop(s, rq, bb);
+    return 0;
+}
