@@ -104,7 +104,7 @@ class SlabDesc(C.Structure):
         ("density_x1", C.c_double),
         ("density_c", C.c_double),
         ("has_density_effect", C.c_uint32),
-        ("pad", C.c_uint32),
+        ("kind", C.c_uint32),
     ]
 
 
@@ -114,7 +114,7 @@ class GridDesc(C.Structure):
         ("n_bins", C.c_uint32 * 2),
         ("bin_offset", C.c_uint32),
         ("transform", C.c_uint32),
-        ("pad", C.c_uint32),
+        ("multi", C.c_uint32),
         ("axis_min", C.c_double * 2),
         ("axis_max", C.c_double * 2),
         ("radius", C.c_double),

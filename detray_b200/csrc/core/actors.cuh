@@ -12,12 +12,15 @@
 //                                (J C J^T with the identity q/p row and time
 //                                column the generator assumes)
 //   frame Jacobians              propagator/detail/jacobian_{cartesian,polar,
-//                                concentric_cylindrical}.hpp, jacobian_engine.hpp
+//                                concentric_cylindrical,line}.hpp,
+//                                jacobian_engine.hpp
 //   parameter_setter             parameter_updater.hpp:577-627
 //   external mask tolerance      propagator/detail/noise_estimation.hpp:22-107
 //   material interactor          propagator/actors/pointwise_material_interactor.hpp:59-326
 //   interaction formulas         material/interaction.hpp:28-310,
 //                                material/detail/relativistic_quantities.hpp
+//   slab / rod path segments     material/material_slab.hpp,
+//                                material/material_rod.hpp
 #pragma once
 
 #include "navigator.cuh"
@@ -58,11 +61,23 @@ DPROP_HD vec3<S> bound_dir(S phi, S theta) {
     return {cos(phi) * st, sin(phi) * st, cos(theta)};
 }
 
+// The line frame's axes at a track direction (jacobian_line.hpp
+// reference_frame): y along the wire, x = normalize(z x dir), z = x x y.
+template <typename S>
+DPROP_HD void line_frame(const dev_transform<S>& trf, vec3<S> dir,
+                         vec3<S>& nx, vec3<S>& ny, vec3<S>& nz) {
+    ny = trf.z();
+    nx = normalize(cross(ny, dir));
+    nz = cross(nx, ny);
+}
+
 // bound -> free position for the surface frame (bound_to_free_vector,
-// tracks/detail/transform_track_parameters.hpp:43-74)
+// tracks/detail/transform_track_parameters.hpp:43-74); the line frame needs
+// the track direction (line2D::local_to_global)
 template <typename S>
 DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S>& det,
-                                   const dev_surface& sf, S l0, S l1) {
+                                   const dev_surface& sf, S l0, S l1,
+                                   vec3<S> dir) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
     switch (sf.shape) {
         case e_ring:
@@ -70,6 +85,10 @@ DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S>& det,
         case e_concentric_cylinder: {
             const S r = det.masks[sf.mask_begin].v[0];
             return {r * cos(l0), r * sin(l0), l1};
+        }
+        case e_line: {
+            const vec3<S> on_wire = trf.point_to_global({S(0), S(0), l1});
+            return on_wire + l0 * normalize(cross(trf.z(), dir));
         }
         default:
             return trf.point_to_global({l0, l1, S(0)});
@@ -81,7 +100,11 @@ template <typename S>
 DPROP_HD void free_to_bound(const detector_view<S>& det, const dev_surface& sf,
                             const step_state<S>& st, S out[6]) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
-    global_to_bound_local(sf.shape, trf, st.pos, out[0], out[1]);
+    if (sf.shape == e_line) {
+        line_bound_local(trf, st.pos, st.dir, out[0], out[1]);
+    } else {
+        global_to_bound_local(sf.shape, trf, st.pos, out[0], out[1]);
+    }
     out[2] = phi_of(st.dir);
     out[3] = theta_of(st.dir);
     out[4] = st.qop;
@@ -91,9 +114,14 @@ DPROP_HD void free_to_bound(const detector_view<S>& det, const dev_surface& sf,
 // columns d(pos)/d(loc0), d(pos)/d(loc1) (get_derivative_dpos_dloc)
 template <typename S>
 DPROP_HD void dpos_dloc(const detector_view<S>& det, const dev_surface& sf,
-                        vec3<S> pos, vec3<S>& c0, vec3<S>& c1) {
+                        vec3<S> pos, vec3<S> dir, vec3<S>& c0, vec3<S>& c1) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
     switch (sf.shape) {
+        case e_line: {
+            vec3<S> nz;
+            line_frame(trf, dir, c0, c1, nz);
+            return;
+        }
         case e_ring: {
             const vec3<S> l = trf.point_to_local(pos);
             const S lrad = perp(l);
@@ -123,9 +151,14 @@ DPROP_HD void dpos_dloc(const detector_view<S>& det, const dev_surface& sf,
 // rows d(loc0)/d(pos), d(loc1)/d(pos) (get_derivative_dloc_dpos)
 template <typename S>
 DPROP_HD void dloc_dpos(const detector_view<S>& det, const dev_surface& sf,
-                        vec3<S> pos, vec3<S>& r0, vec3<S>& r1) {
+                        vec3<S> pos, vec3<S> dir, vec3<S>& r0, vec3<S>& r1) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
     switch (sf.shape) {
+        case e_line: {
+            vec3<S> nz;
+            line_frame(trf, dir, r0, r1, nz);
+            return;
+        }
         case e_ring: {
             const vec3<S> l = trf.point_to_local(pos);
             const S lrad = perp(l);
@@ -172,6 +205,50 @@ DPROP_HD vec3<S> surface_normal_at_bound(const detector_view<S>& det,
     return det.transforms[sf.transform].z();
 }
 
+// d(path)/d(free position), d(path)/d(free direction) to reach the surface
+// (jacobian<frame>::path_derivative): -n / (n . dir) for surfaces with a
+// normal; for a line (jacobian_line.hpp path_derivative) the closest
+// approach also moves with the direction and the track's curvature.
+template <typename S>
+DPROP_HD void path_derivative(const detector_view<S>& det,
+                              const dev_surface& sf, vec3<S> pos, vec3<S> dir,
+                              vec3<S> dtds, vec3<S>& f_pos, vec3<S>& f_dir) {
+    if (sf.shape == e_line) {
+        const dev_transform<S>& trf = det.transforms[sf.transform];
+        const vec3<S> pc = pos - trf.translation();
+        const vec3<S> z = trf.z();
+        const S pz = dot(pc, z);
+        const S dz = dot(z, dir);
+        const vec3<S> pc_x = pc - pz * z;
+        const S norm = S(-1) / (S(1) - dz * dz + dot(pc_x, dtds));
+        f_pos = norm * (dir - dz * z);
+        f_dir = norm * pc_x;
+        return;
+    }
+    const vec3<S> n = surface_normal_at_pos(det, sf, pos);
+    const S inv_nd = S(-1) / dot(n, dir);
+    f_pos = {inv_nd * n.x, inv_nd * n.y, inv_nd * n.z};
+    f_dir = {S(0), S(0), S(0)};
+}
+
+// d(pos)/d(phi), d(pos)/d(theta) of the line frame at fixed local position
+// (jacobian_line.hpp get_derivative_dpos_dangle); zero for the other frames.
+template <typename S>
+DPROP_HD void line_dpos_dangle(const dev_transform<S>& trf, vec3<S> pos,
+                               vec3<S> dir, vec3<S> dd_phi, vec3<S> dd_th,
+                               vec3<S>& c_phi, vec3<S>& c_th) {
+    S l0, l1;
+    line_bound_local(trf, pos, dir, l0, l1);
+    vec3<S> nx, ny, nz;
+    line_frame(trf, dir, nx, ny, nz);
+    const S ipdn = S(1) / dot(dir, nz);
+    const S C = ipdn * l0;
+    const vec3<S> y_phi = cross(ny, dd_phi);
+    const vec3<S> y_th = cross(ny, dd_th);
+    c_phi = C * (y_phi - nx * dot(nx, y_phi));
+    c_th = C * (y_th - nx * dot(nx, y_th));
+}
+
 // ---------------------------------------------------- full Jacobian
 // J_full (6x6) from the departure bound state, the transport Jacobian and
 // the current (destination) free state.  Only rows 0..3 x cols 0..4 are
@@ -183,12 +260,14 @@ DPROP_HD void full_jacobian(const detector_view<S>& det,
                             const dev_surface& dst_sf, const step_state<S>& st,
                             vec3<S> dtds, S G[4][5]) {
     // bound -> free at the departure surface
-    const vec3<S> dep_pos = bound_to_free_pos(det, dep_sf, dep.v[0], dep.v[1]);
-    vec3<S> p0, p1;
-    dpos_dloc(det, dep_sf, dep_pos, p0, p1);
     const S ph = dep.v[2];
     const S th = dep.v[3];
     const S ct = cos(th), st_ = sin(th), cp = cos(ph), sp = sin(ph);
+    const vec3<S> dep_dir{cp * st_, sp * st_, ct};
+    const vec3<S> dep_pos =
+        bound_to_free_pos(det, dep_sf, dep.v[0], dep.v[1], dep_dir);
+    vec3<S> p0, p1;
+    dpos_dloc(det, dep_sf, dep_pos, dep_dir, p0, p1);
     // ddir/dphi, ddir/dtheta
     const vec3<S> dd_phi{-st_ * sp, st_ * cp, S(0)};
     const vec3<S> dd_th{ct * cp, ct * sp, -st_};
@@ -224,14 +303,32 @@ DPROP_HD void full_jacobian(const detector_view<S>& det,
         m1d[r][3] = b3;
         m1d[r][4] = da[r];
     }
+    if (dep_sf.shape == e_line) {
+        // the line frame's position also moves with the angles
+        vec3<S> c_phi, c_th;
+        line_dpos_dangle(det.transforms[dep_sf.transform], dep_pos, dep_dir,
+                         dd_phi, dd_th, c_phi, c_th);
+        const S cpa[3] = {c_phi.x, c_phi.y, c_phi.z};
+        const S cta[3] = {c_th.x, c_th.y, c_th.z};
+        for (int r = 0; r < 3; ++r) {
+            m1p[r][2] += cpa[r];
+            m1p[r][3] += cta[r];
+        }
+    }
 
-    // path correction: M2 = M1 + P2F (F2P M1), F2P has position terms only
-    const vec3<S> n = surface_normal_at_pos(det, dst_sf, st.pos);
-    const S inv_nd = S(-1) / dot(n, st.dir);
-    const S f[3] = {inv_nd * n.x, inv_nd * n.y, inv_nd * n.z};
+    // path correction: M2 = M1 + P2F (F2P M1)
+    vec3<S> f_pos, f_dir;
+    path_derivative(det, dst_sf, st.pos, st.dir, dtds, f_pos, f_dir);
+    const S f[3] = {f_pos.x, f_pos.y, f_pos.z};
     S s[5];
     for (int c = 0; c < 5; ++c) {
         s[c] = f[0] * m1p[0][c] + f[1] * m1p[1][c] + f[2] * m1p[2][c];
+    }
+    if (dst_sf.shape == e_line) {
+        for (int c = 0; c < 5; ++c) {
+            s[c] += f_dir.x * m1d[0][c] + f_dir.y * m1d[1][c] +
+                    f_dir.z * m1d[2][c];
+        }
     }
     const S dir_a[3] = {st.dir.x, st.dir.y, st.dir.z};
     const S dtds_a[3] = {dtds.x, dtds.y, dtds.z};
@@ -244,7 +341,7 @@ DPROP_HD void full_jacobian(const detector_view<S>& det,
 
     // free -> bound at the destination
     vec3<S> r0, r1;
-    dloc_dpos(det, dst_sf, st.pos, r0, r1);
+    dloc_dpos(det, dst_sf, st.pos, st.dir, r0, r1);
     const S dth = theta_of(st.dir);
     const S dph = phi_of(st.dir);
     const S cth = cos(dth), sth = sin(dth), cph = cos(dph), sph = sin(dph);
@@ -388,6 +485,17 @@ DPROP_HD S scattering_theta0(S x_over_x0, const rel_quantities<S>& rq, S q,
            (S(1) + S(0.038) * S(2) * log(t));
 }
 
+// Path through a rod of radius r around a line surface at closest approach
+// d (material_rod::path_segment)
+template <typename S>
+DPROP_HD S rod_path(S r, S cos_inc, S d) {
+    if (fabs(d) > r) {
+        return S(0);
+    }
+    const S sin_inc_2 = S(1) - cos_inc * cos_inc;
+    return S(2) * sqrt((r * r - d * d) / sin_inc_2);
+}
+
 // pointwise_material_interactor::update on the bound state
 template <typename S>
 DPROP_HD bool interact(const detector_view<S>& det, const dev_surface& sf,
@@ -407,12 +515,18 @@ DPROP_HD bool interact(const detector_view<S>& det, const dev_surface& sf,
     if (qop == S(0)) {
         return false;
     }
-    const S path_segment = mat.thickness / cos_inc;
+    S path_segment, x_over_x0;
+    if (mat.is_rod != S(0)) {
+        path_segment = rod_path(mat.thickness, cos_inc, b.v[0]);
+        x_over_x0 = path_segment / mat.X0;
+    } else {
+        path_segment = mat.thickness / cos_inc;
+        x_over_x0 = mat.thickness_in_X0 / cos_inc;
+    }
     const rel_quantities<S> rq = make_rq(cfg.mass, qop, q);
     const S e_loss = path_segment * bethe_bloch(mat, rq);
     const S sigma_qop = landau_sigma_qop(path_segment, mat, rq, q);
-    const S theta0 = scattering_theta0(mat.thickness_in_X0 / cos_inc, rq, q,
-                                       cfg.electron);
+    const S theta0 = scattering_theta0(x_over_x0, rq, q, cfg.electron);
     // energy loss
     const S m = cfg.mass;
     const S p = q / qop;

@@ -149,13 +149,14 @@ DPROP_HD void initial_jacobian(const detector_view<S>& det,
     md[1][6] = J.d.y;
     md[2][6] = J.d.z;
     // path correction onto the destination surface
-    const vec3<S> nrm = surface_normal_at_pos(det, dst_sf, st.pos);
-    const S inv_nd = S(-1) / dot(nrm, st.dir);
-    const S f[3] = {inv_nd * nrm.x, inv_nd * nrm.y, inv_nd * nrm.z};
+    vec3<S> f_pos, f_dir;
+    path_derivative(det, dst_sf, st.pos, st.dir, dtds, f_pos, f_dir);
     const S dir_a[3] = {st.dir.x, st.dir.y, st.dir.z};
     const S dtds_a[3] = {dtds.x, dtds.y, dtds.z};
     for (int c = 0; c < 7; ++c) {
-        const S s = f[0] * mp[0][c] + f[1] * mp[1][c] + f[2] * mp[2][c];
+        const S s = f_pos.x * mp[0][c] + f_pos.y * mp[1][c] +
+                    f_pos.z * mp[2][c] + f_dir.x * md[0][c] +
+                    f_dir.y * md[1][c] + f_dir.z * md[2][c];
         for (int r = 0; r < 3; ++r) {
             mp[r][c] += dir_a[r] * s;
             md[r][c] += dtds_a[r] * s;
@@ -163,7 +164,7 @@ DPROP_HD void initial_jacobian(const detector_view<S>& det,
     }
     // free -> bound at the destination
     vec3<S> r0, r1;
-    dloc_dpos(det, dst_sf, st.pos, r0, r1);
+    dloc_dpos(det, dst_sf, st.pos, st.dir, r0, r1);
     const S th = theta_of(st.dir);
     const S ph = phi_of(st.dir);
     const S cth = cos(th), sth = sin(th), cph = cos(ph), sph = sin(ph);
@@ -217,7 +218,9 @@ DPROP_HD S bethe_bloch_dqop(const dev_slab<S>& mat, const rel_quantities<S>& rq,
 // Derivatives of the q/p after the kick of interact() with respect to the
 // q/p before it (mq) and to the incidence d.n (mc), for the bound state b
 // before the kick.  (1, 0) where interact() leaves q/p alone; (0, 0) where
-// the particle stops (q/p becomes the invalid maximum).
+// the particle stops (q/p becomes the invalid maximum).  For a material rod
+// around a wire the dependence of the path on the closest approach (loc0)
+// is not included.
 template <typename S>
 DPROP_HD void kick_derivatives(const detector_view<S>& det,
                                const dev_surface& sf, const S* b, S mass, S q,
@@ -236,7 +239,16 @@ DPROP_HD void kick_derivatives(const detector_view<S>& det,
     const vec3<S> n = surface_normal_at_bound(det, sf, b[0]);
     const S dn = dot(dir, n);
     const S cos_inc = fabs(dn);
-    const S path = mat.thickness / cos_inc;
+    // path through the material and its derivative by |d.n| (the closest
+    // approach of a rod is held fixed)
+    S path, dpath_dcos;
+    if (mat.is_rod != S(0)) {
+        path = rod_path(mat.thickness, cos_inc, b[0]);
+        dpath_dcos = path * cos_inc / (S(1) - cos_inc * cos_inc);
+    } else {
+        path = mat.thickness / cos_inc;
+        dpath_dcos = -path / cos_inc;
+    }
     const rel_quantities<S> rq = make_rq(mass, qop, q);
     const S bb = bethe_bloch(mat, rq);
     const S dbb = bethe_bloch_dqop(mat, rq, bb);
@@ -253,9 +265,8 @@ DPROP_HD void kick_derivatives(const detector_view<S>& det,
     const S dq_de1 = -q / (p1 * p1) * (e1 / p1);
     // dE/dq = (p / E) dp/dq with dp/dq = -p^2 / q
     const S de1_dq = (p / E) * (-p * p / q) - sgn * path * dbb;
-    // d(path)/d(d.n) = -path / |d.n| * sign(d.n)
     const S sdn = (dn < S(0)) ? S(-1) : S(1);
-    const S de1_ddn = sgn * bb * path / cos_inc * sdn;
+    const S de1_ddn = -sgn * bb * dpath_dcos * sdn;
     mq = dq_de1 * de1_dq;
     mc = dq_de1 * de1_ddn;
 }
@@ -274,10 +285,10 @@ DPROP_HD bool alignment_contribution(const detector_view<S>& det,
         return false;
     }
     const dev_transform<S>& trf = det.transforms[sf.transform];
-    const vec3<S> x = bound_to_free_pos(det, sf, b[0], b[1]);
     const S cph = cos(b[2]), sph = sin(b[2]);
     const S cth = cos(b[3]), sth = sin(b[3]);
     const vec3<S> d{cph * sth, sph * sth, cth};
+    const vec3<S> x = bound_to_free_pos(det, sf, b[0], b[1], d);
     const vec3<S> u = trf.x(), v = trf.y(), n = trf.z();
     const vec3<S> r = x - trf.translation();
     const S inv_nd = S(1) / dot(n, d);

@@ -67,9 +67,6 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
             (s.material != DPROP_INVALID_INDEX && s.material >= d->n_slabs)) {
             return "surface " + std::to_string(i) + " has an out-of-range index";
         }
-        if (s.shape == DPROP_SHAPE_LINE) {
-            return "line (wire) surfaces are not supported on the device path";
-        }
     }
     for (uint32_t i = 0; i < d->n_masks; ++i) {
         const uint32_t vl = d->masks[i].volume_link;
@@ -90,19 +87,39 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
             return "brute-force entry " + std::to_string(i) + " out of range";
         }
     }
+    for (uint32_t i = 0; i < d->n_slabs; ++i) {
+        if (d->slabs[i].kind > DPROP_MATERIAL_ROD) {
+            return "material " + std::to_string(i) + " has an unknown kind";
+        }
+    }
+    // grid_bins entries that are bin ranges of multi-entry grids (the rest
+    // are surface indices)
+    std::vector<bool> is_range(d->n_grid_bins, false);
     for (uint32_t i = 0; i < d->n_grids; ++i) {
         const dprop_grid_desc& g = d->grids[i];
         const uint64_t nb = static_cast<uint64_t>(g.n_bins[0]) * g.n_bins[1];
+        const uint64_t n_entries = nb + (g.multi ? 1u : 0u);
         if ((g.kind != DPROP_GRID_CYLINDER && g.kind != DPROP_GRID_DISC) ||
-            g.n_bins[0] == 0 || g.n_bins[1] == 0 ||
-            static_cast<uint64_t>(g.bin_offset) + nb > d->n_grid_bins ||
+            g.n_bins[0] == 0 || g.n_bins[1] == 0 || g.multi > 1u ||
+            static_cast<uint64_t>(g.bin_offset) + n_entries > d->n_grid_bins ||
             g.transform >= d->n_transforms ||
             !(g.axis_max[0] > g.axis_min[0]) || !(g.axis_max[1] > g.axis_min[1])) {
             return "grid " + std::to_string(i) + " is inconsistent";
         }
+        if (g.multi) {
+            for (uint64_t b = 0; b < n_entries; ++b) {
+                const uint64_t e = g.bin_offset + b;
+                is_range[e] = true;
+                if (d->grid_bins[e] > d->n_grid_bins ||
+                    (b > 0 && d->grid_bins[e] < d->grid_bins[e - 1])) {
+                    return "grid " + std::to_string(i) +
+                           " has an inconsistent bin range";
+                }
+            }
+        }
     }
     for (uint32_t i = 0; i < d->n_grid_bins; ++i) {
-        if (d->grid_bins[i] != DPROP_INVALID_INDEX &&
+        if (!is_range[i] && d->grid_bins[i] != DPROP_INVALID_INDEX &&
             d->grid_bins[i] >= d->n_surfaces) {
             return "grid bin " + std::to_string(i) + " out of range";
         }
@@ -124,6 +141,8 @@ dev_slab<S> convert_slab(const dprop_slab_desc& s) {
     o.density_x1 = static_cast<S>(s.density_x1);
     o.density_c = static_cast<S>(s.density_c);
     o.has_density_effect = s.has_density_effect ? S(1) : S(0);
+    o.X0 = static_cast<S>(s.X0);
+    o.is_rod = (s.kind == DPROP_MATERIAL_ROD) ? S(1) : S(0);
     return o;
 }
 
@@ -186,6 +205,7 @@ host_tables<S> convert_desc(const dprop_detector_desc* d) {
         o.n1 = g.n_bins[1];
         o.bin_offset = g.bin_offset;
         o.transform = g.transform;
+        o.multi = g.multi;
         o.min0 = static_cast<S>(g.axis_min[0]);
         o.max0 = static_cast<S>(g.axis_max[0]);
         o.min1 = static_cast<S>(g.axis_min[1]);

@@ -5,12 +5,13 @@
 //   ray-plane        navigation/intersection/ray_plane_intersector.hpp:60-93
 //   ray-cylinder     navigation/intersection/ray_cylinder_intersector.hpp:61-122
 //   ray-portal cyl.  navigation/intersection/ray_cylinder_portal_intersector.hpp:67-132
+//   ray-line         navigation/intersection/ray_line_intersector.hpp:58-99
 //   quadratic        utils/quadratic_equation.hpp:30-90
 //   resolve_mask     navigation/intersection/intersector_base.hpp:167-252
 //   mask checks      geometry/shapes/{rectangle2D,trapezoid2D,ring2D,
-//                    cylinder2D,concentric_cylinder2D}.hpp
+//                    cylinder2D,concentric_cylinder2D,line}.hpp
 //   local frames     geometry/coordinates/{cartesian2D,polar2D,
-//                    concentric_cylindrical2D,cylindrical2D}.hpp
+//                    concentric_cylindrical2D,cylindrical2D,line2D}.hpp
 #pragma once
 
 #include "tables.cuh"
@@ -135,6 +136,35 @@ DPROP_HD mask_result<S> check_portal_z(const dev_mask<S>& m, S z, S tol) {
     return {in, in};
 }
 
+// line<square>: a drift cell, |x|, |y| <= half width, |z| <= half_z in the
+// cartesian frame of the wire; line<circular>: a straw tube,
+// radius <= r, |z| <= half_z (line.hpp check_boundaries)
+template <typename S>
+DPROP_HD mask_result<S> check_line(const dev_mask<S>& m, vec3<S> l, S tol,
+                                   S edge_tol) {
+    mask_result<S> r;
+    r.edge = false;
+    if (m.v[2] != S(0)) {
+        const S a0 = fabs(l.x), a1 = fabs(l.y), a2 = fabs(l.z);
+        r.inside = a0 <= (m.v[0] + tol) && a1 <= (m.v[0] + tol) &&
+                   a2 <= (m.v[1] + tol);
+        if (edge_tol > S(0)) {
+            const S ft = tol + edge_tol;
+            r.edge = a0 <= (m.v[0] + ft) && a1 <= (m.v[0] + ft) &&
+                     a2 <= (m.v[1] + ft);
+        }
+        return r;
+    }
+    const S a0 = fabs(perp(l));
+    const S a1 = fabs(l.z);
+    r.inside = a0 <= (m.v[0] + tol) && a1 <= (m.v[1] + tol);
+    if (edge_tol > S(0)) {
+        const S ft = tol + edge_tol;
+        r.edge = a0 <= (m.v[0] + ft) && a1 <= (m.v[1] + ft);
+    }
+    return r;
+}
+
 // Mask check of a global intersection point, resolving the local frame of
 // the shape (mask::resolve, geometry/mask.hpp).
 template <typename S>
@@ -159,6 +189,8 @@ DPROP_HD mask_result<S> check_mask(uint8_t shape, const dev_mask<S>& m,
             const vec3<S> l = trf.point_to_local(ip.glob);
             return check_cylinder_z(m, l.z, tol, edge_tol);
         }
+        case e_line:
+            return check_line(m, trf.point_to_local(ip.glob), tol, edge_tol);
         case e_concentric_cylinder:
         default: {
             // the portal intersector only provides the global z
@@ -325,7 +357,43 @@ DPROP_HD int intersect_cylinder(vec3<S> ro, vec3<S> rd,
     return n;
 }
 
+// Line (wire): the point of closest approach of the ray to the wire,
+// ray_line_intersector.hpp:58-99.  A ray (almost) parallel to the wire has
+// no intersection.
+template <typename S>
+DPROP_HD isect_point<S> intersect_line(vec3<S> ro, vec3<S> rd,
+                                       const dev_transform<S>& trf) {
+    isect_point<S> ip;
+    const vec3<S> z = trf.z();
+    const S zd = dot(z, rd);
+    const S denom = S(1) - zd * zd;
+    if (denom < S(1e-5)) {
+        ip.path = limits<S>::max();
+        ip.glob = {limits<S>::max(), limits<S>::max(), limits<S>::max()};
+        return ip;
+    }
+    const vec3<S> t2l = trf.translation() - ro;
+    const S t2l_on_line = dot(t2l, z);
+    const S t2l_on_track = dot(t2l, rd);
+    ip.path = S(1) / denom * (t2l_on_track - t2l_on_line * zd);
+    ip.glob = ro + ip.path * rd;
+    return ip;
+}
+
 // ----------------------------------------------- local frames (bound loc)
+// line2D (geometry/coordinates/line2D.hpp): loc0 = signed distance from the
+// wire, negative when the wire lies on the side of z x dir; loc1 = position
+// along the wire.
+template <typename S>
+DPROP_HD void line_bound_local(const dev_transform<S>& trf, vec3<S> p,
+                               vec3<S> dir, S& l0, S& l1) {
+    const vec3<S> local3 = trf.point_to_local(p);
+    const vec3<S> r = cross(trf.z(), dir);
+    const S sign = dot(r, trf.translation() - p) > S(0) ? S(-1) : S(1);
+    l0 = sign * perp(local3);
+    l1 = local3.z;
+}
+
 // free_to_bound: the two local coordinates of a global point on the surface
 template <typename S>
 DPROP_HD void global_to_bound_local(uint8_t shape,

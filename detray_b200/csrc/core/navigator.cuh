@@ -244,6 +244,8 @@ DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& d
     if (sf.shape == e_concentric_cylinder) {
         ip = intersect_portal_cylinder(ro, rd, det.masks[m0].v[0],
                                        cfg.overstep_tol);
+    } else if (sf.shape == e_line) {
+        ip = intersect_line(ro, rd, trf);
     } else {
         ip = intersect_plane(ro, rd, trf);
     }
@@ -287,6 +289,8 @@ DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S>& det
         if (sf.shape == e_concentric_cylinder) {
             ip = intersect_portal_cylinder(ro, rd, det.masks[m0].v[0],
                                            cfg.overstep_tol);
+        } else if (sf.shape == e_line) {
+            ip = intersect_line(ro, rd, trf);
         } else {
             ip = intersect_plane(ro, rd, trf);
         }
@@ -396,11 +400,19 @@ DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S>& det,
         const int j0 = (g.kind == 1u) ? wrap_bin(i0, n0) : i0;
         for (int i1 = lo1; i1 < hi1; ++i1) {
             const int j1 = (g.kind == 1u) ? i1 : wrap_bin(i1, n1);
-            const uint32_t sf =
-                det.grid_bins[g.bin_offset + static_cast<uint32_t>(j0) +
-                              static_cast<uint32_t>(j1) * g.n0];
-            if (sf != k_invalid) {
-                candidate_search(nav, det, sf, ro, rd, icfg);
+            const uint32_t b = g.bin_offset + static_cast<uint32_t>(j0) +
+                               static_cast<uint32_t>(j1) * g.n0;
+            if (g.multi) {
+                // dynamic bins: [begin, end) of the bin's surfaces
+                const uint32_t e1 = det.grid_bins[b + 1u];
+                for (uint32_t e = det.grid_bins[b]; e < e1; ++e) {
+                    candidate_search(nav, det, det.grid_bins[e], ro, rd, icfg);
+                }
+            } else {
+                const uint32_t sf = det.grid_bins[b];
+                if (sf != k_invalid) {
+                    candidate_search(nav, det, sf, ro, rd, icfg);
+                }
             }
         }
     }

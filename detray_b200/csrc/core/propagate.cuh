@@ -195,7 +195,7 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
         // parameter_setter
         if (success) {
             const vec3<S> d = bound_dir(b.v[2], b.v[3]);
-            st.pos = bound_to_free_pos(det, dst, b.v[0], b.v[1]);
+            st.pos = bound_to_free_pos(det, dst, b.v[0], b.v[1], d);
             st.time = b.v[5];
             st.dir = d;
             st.qop = b.v[4];

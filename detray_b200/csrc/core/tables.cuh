@@ -91,7 +91,8 @@ struct alignas(16) dev_slab {
     S mean_excitation_energy;
     S density_a, density_m, density_x0, density_x1, density_c;
     S has_density_effect;  // 0 or 1
-    S pad[2];
+    S X0;                  // radiation length
+    S is_rod;              // 0: slab of thickness t; 1: rod of radius t
 };
 
 struct alignas(16) dev_volume {
@@ -107,7 +108,8 @@ struct alignas(16) dev_grid {
     uint32_t n0, n1;
     uint32_t bin_offset;
     uint32_t transform;
-    uint32_t pad[3];
+    uint32_t multi;  // 1: bins hold [begin, end) ranges into grid_bins
+    uint32_t pad[2];
     S min0, max0, min1, max1;
     S radius;
     S pad2[3];

@@ -8,6 +8,10 @@ of the benchmark detectors into compressed .npz files next to this script:
                              7 endcap discs per side, 0.15 mm Si modules
   telescope_10x1m_300um.npz  10 1 m x 1 m Si planes normal to x at
                              x = 0, 50, ..., 450 mm, 0.3 mm thick
+  wire_chamber_10l_cells.npz wire chamber: 10 layers of 10 mm square drift
+                             cells from r = 500 mm, 1 m half length, 50 mrad
+                             stereo angle, 15 um tungsten wires
+  wire_chamber_10l_straws.npz the same with circular straw tubes
 """
 from __future__ import annotations
 
@@ -26,6 +30,8 @@ from detray_b200 import geometry  # noqa: E402
 GEOMETRIES = {
     "toy_4brl_7edc": ["toy", "4", "7", "0.15"],
     "telescope_10x1m_300um": ["telescope", "500", "500", "0.3"],
+    "wire_chamber_10l_cells": ["wire", "10", "1", "0.015"],
+    "wire_chamber_10l_straws": ["wire", "10", "0", "0.015"],
 }
 TELESCOPE_POSITIONS = [str(50.0 * i) for i in range(10)]
 

@@ -19,6 +19,7 @@
 #include "detray_b200/dprop.h"
 
 #include <cstdint>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -153,7 +154,33 @@ dprop_slab_desc to_slab_desc(const slab_t& slab) {
     return d;
 }
 
-/// Material-store visitor: homogeneous slabs only.
+/// A detray material rod (material/material_rod.hpp) around a line surface
+/// as a dprop_slab_desc of kind DPROP_MATERIAL_ROD (thickness = radius).
+template <typename rod_t>
+dprop_slab_desc to_rod_desc(const rod_t& rod) {
+    const auto& mat = rod.get_material();
+    dprop_slab_desc d{};
+    d.kind = DPROP_MATERIAL_ROD;
+    d.thickness = static_cast<double>(rod.radius());
+    d.X0 = static_cast<double>(mat.X0());
+    d.thickness_in_X0 = d.thickness / d.X0;
+    d.molar_electron_density =
+        static_cast<double>(mat.molar_electron_density());
+    d.mean_excitation_energy =
+        static_cast<double>(mat.mean_excitation_energy());
+    d.has_density_effect = mat.has_density_effect_data() ? 1u : 0u;
+    if (mat.has_density_effect_data()) {
+        const auto& de = mat.density_effect_data();
+        d.density_a = static_cast<double>(de.get_A_density());
+        d.density_m = static_cast<double>(de.get_M_density());
+        d.density_x0 = static_cast<double>(de.get_X0_density());
+        d.density_x1 = static_cast<double>(de.get_X1_density());
+        d.density_c = static_cast<double>(de.get_C_density());
+    }
+    return d;
+}
+
+/// Material-store visitor: homogeneous slabs and rods.
 struct slab_copier {
     template <typename mat_group_t, typename index_t>
     void operator()(const mat_group_t& group, const index_t& idx,
@@ -164,6 +191,13 @@ struct slab_copier {
                           s.get_material();
                       }) {
             const dprop_slab_desc d = to_slab_desc(group[idx]);
+            sf.material = static_cast<uint32_t>(out.slabs.size());
+            out.slabs.push_back(d);
+        } else if constexpr (requires(const mat_t& s) {
+                                 s.radius();
+                                 s.get_material();
+                             }) {
+            const dprop_slab_desc d = to_rod_desc(group[idx]);
             sf.material = static_cast<uint32_t>(out.slabs.size());
             out.slabs.push_back(d);
         } else {
@@ -214,18 +248,35 @@ struct accel_copier {
             gd.bin_offset = static_cast<uint32_t>(out.grid_bins.size());
             const std::size_t nb =
                 static_cast<std::size_t>(gd.n_bins[0]) * gd.n_bins[1];
+            // bin contents in the grid's own order
+            std::vector<std::vector<uint32_t>> content(nb);
+            std::size_t max_count = 0u;
             for (std::size_t b = 0; b < nb; ++b) {
-                uint32_t entry = DPROP_INVALID_INDEX;
-                std::size_t count = 0u;
                 for (const auto& sf : g.bin(static_cast<detray::dindex>(b))) {
-                    entry = static_cast<uint32_t>(sf.index());
-                    ++count;
+                    content[b].push_back(static_cast<uint32_t>(sf.index()));
                 }
-                if (count > 1u) {
-                    throw std::runtime_error(
-                        "dprop::flatten: more than one surface per grid bin");
+                max_count = std::max(max_count, content[b].size());
+            }
+            if (max_count <= 1u) {
+                gd.multi = 0u;
+                for (std::size_t b = 0; b < nb; ++b) {
+                    out.grid_bins.push_back(content[b].empty()
+                                                ? DPROP_INVALID_INDEX
+                                                : content[b][0]);
                 }
-                out.grid_bins.push_back(entry);
+            } else {
+                // ranges first (nb + 1 positions), then the entries
+                gd.multi = 1u;
+                std::size_t pos = out.grid_bins.size() + nb + 1u;
+                for (std::size_t b = 0; b < nb; ++b) {
+                    out.grid_bins.push_back(static_cast<uint32_t>(pos));
+                    pos += content[b].size();
+                }
+                out.grid_bins.push_back(static_cast<uint32_t>(pos));
+                for (std::size_t b = 0; b < nb; ++b) {
+                    out.grid_bins.insert(out.grid_bins.end(),
+                                         content[b].begin(), content[b].end());
+                }
             }
             vol.grid = static_cast<uint32_t>(out.grids.size());
             out.grids.push_back(gd);

@@ -80,7 +80,8 @@ typedef enum dprop_shape {
     DPROP_SHAPE_RING = 2,          /* ring2D: v0 inner_r, v1 outer_r                    */
     DPROP_SHAPE_CYLINDER = 3,      /* cylinder2D: v0 r, v1 lower_z, v2 upper_z          */
     DPROP_SHAPE_CONCENTRIC_CYL = 4,/* concentric_cylinder2D: v0 r, v1 lower_z, v2 upper_z */
-    DPROP_SHAPE_LINE = 5,          /* line (straw/wire cell): v0 cell r, v1 half_z, v2 square(1)/radial(0) */
+    DPROP_SHAPE_LINE = 5,          /* line (drift cell / straw tube, line.hpp): v0 cell half width or
+                                      radius, v1 half_z, v2 square cross-section (1) / circular (0) */
     DPROP_SHAPE_COUNT = 6
 } dprop_shape;
 
@@ -134,8 +135,17 @@ typedef struct dprop_slab_desc {
     double mean_excitation_energy;  /* I                                 */
     double density_a, density_m, density_x0, density_x1, density_c;
     uint32_t has_density_effect;
-    uint32_t pad;
+    uint32_t kind;                  /* dprop_material_kind                  */
 } dprop_slab_desc;
+
+/* Surface material kinds (material/material_slab.hpp,
+ * material/material_rod.hpp). */
+typedef enum dprop_material_kind {
+    DPROP_MATERIAL_SLAB = 0,  /* thickness t: path t / |cos(incidence)|       */
+    DPROP_MATERIAL_ROD = 1    /* rod of radius t around a line surface: path
+                                 2 sqrt((t^2 - d^2) / sin^2(incidence)) at
+                                 closest approach d, 0 for |d| > t           */
+} dprop_material_kind;
 
 typedef enum dprop_grid_kind {
     DPROP_GRID_NONE = 0,
@@ -143,15 +153,21 @@ typedef enum dprop_grid_kind {
     DPROP_GRID_DISC = 2      /* axes (r closed, phi circular [-pi,pi])              */
 } dprop_grid_kind;
 
-/* A 2D surface grid, spatial_grid<..., static_array<surface,1>> of
- * navigation/accelerators/spatial_grid.hpp with regular binning. */
+/* A 2D surface grid of navigation/accelerators/spatial_grid.hpp with
+ * regular binning: spatial_grid<..., static_array<surface,1>> (one surface
+ * per bin, multi = 0) or spatial_grid<..., dynamic_array<surface>> (several
+ * surfaces per bin, multi = 1). */
 typedef struct dprop_grid_desc {
     uint32_t kind;          /* dprop_grid_kind                                  */
     uint32_t n_bins[2];
-    uint32_t bin_offset;    /* into grid_bins: n_bins[0]*n_bins[1] entries,
-                               serialised as bin0 + bin1 * n_bins[0]            */
+    uint32_t bin_offset;    /* into grid_bins, bins serialised as
+                               bin0 + bin1 * n_bins[0].  multi = 0: one entry
+                               per bin, a surface index or DPROP_INVALID_INDEX.
+                               multi = 1: n_bins[0]*n_bins[1] + 1 entries;
+                               entries b and b+1 are the [begin, end) positions
+                               in grid_bins of bin b's surface indices          */
     uint32_t transform;     /* grid placement (the volume's transform)          */
-    uint32_t pad;
+    uint32_t multi;
     double axis_min[2];
     double axis_max[2];
     double radius;          /* reference cylinder radius (DPROP_GRID_CYLINDER)  */

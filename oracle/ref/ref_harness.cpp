@@ -38,6 +38,7 @@
 #include "detray/propagator/rk_stepper.hpp"
 #include "detray/test/common/build_telescope_detector.hpp"
 #include "detray/test/common/build_toy_detector.hpp"
+#include "detray/test/common/build_wire_chamber.hpp"
 #include "detray/tracks/ray.hpp"
 
 #include <vecmem/memory/host_memory_resource.hpp>
@@ -69,11 +70,12 @@ thread_local std::string g_error;
 // ---------------------------------------------------------------- detectors
 using toy_det_t = detector<toy_metadata<algebra_t>>;
 using tel_det_t = detector<telescope_metadata<algebra_t, rectangle2D>>;
+using wire_det_t = detector<wire_chamber_metadata<algebra_t>>;
 
 struct det_handle {
     vecmem::host_memory_resource mr;
     std::variant<std::monostate, std::unique_ptr<toy_det_t>,
-                 std::unique_ptr<tel_det_t>>
+                 std::unique_ptr<tel_det_t>, std::unique_ptr<wire_det_t>>
         det;
     dprop::flat_detector flat;
     dprop_detector_desc desc{};
@@ -587,6 +589,47 @@ int ref_build_telescope(const ref_tel_cfg* c, void** out) {
     }
 }
 
+/// Wire chamber parameters (build_wire_chamber.hpp:35-145,
+/// wire_layer_generator.hpp:33-66).
+typedef struct ref_wire_cfg {
+    uint32_t n_layers;
+    uint32_t square_cells;     /* 1: line_square drift cells, 0: straw tubes */
+    double first_layer_inner_radius;
+    double half_z;
+    double cell_size;
+    double stereo_angle;
+    double mat_radius;         /* tungsten wire radius (mm)                  */
+} ref_wire_cfg;
+
+int ref_build_wire_chamber(const ref_wire_cfg* c, void** out) {
+    try {
+        auto h = std::make_unique<det_handle>();
+        auto build = [&](auto shape_tag) {
+            using shape_t = decltype(shape_tag);
+            wire_chamber_config<scalar, shape_t> cfg{};
+            cfg.n_layers(c->n_layers)
+                .first_layer_inner_radius(
+                    static_cast<scalar>(c->first_layer_inner_radius))
+                .half_z(static_cast<scalar>(c->half_z))
+                .cell_size(static_cast<scalar>(c->cell_size))
+                .stereo_angle(static_cast<scalar>(c->stereo_angle))
+                .mat_radius(static_cast<scalar>(c->mat_radius))
+                .do_check(false);
+            auto [det, names] = build_wire_chamber<algebra_t>(h->mr, cfg);
+            return std::make_unique<wire_det_t>(std::move(det));
+        };
+        auto d = c->square_cells ? build(line_square{}) : build(line_circular{});
+        h->flat = dprop::flatten(*d);
+        h->desc = h->flat.desc();
+        h->det = std::move(d);
+        *out = h.release();
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
 int ref_tables(void* handle, dprop_detector_desc* out) {
     auto* h = static_cast<det_handle*>(handle);
     *out = h->desc;
@@ -639,6 +682,10 @@ int ref_propagate_jac(void* handle, const ref_field_desc* fd,
         }
         if (auto* tel = std::get_if<std::unique_ptr<tel_det_t>>(&h->det)) {
             return dispatch(**tel, f, *cfg, tracks, n, out, n_threads, chunk,
+                            with_abort_reasons, rec_jac);
+        }
+        if (auto* wire = std::get_if<std::unique_ptr<wire_det_t>>(&h->det)) {
+            return dispatch(**wire, f, *cfg, tracks, n, out, n_threads, chunk,
                             with_abort_reasons, rec_jac);
         }
         g_error = "ref_propagate_jac: empty detector handle";

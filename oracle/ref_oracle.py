@@ -181,6 +181,34 @@ def build_toy(n_brl_layers=4, n_edc_layers=7, module_mat_thickness=0.15,
     return RefDetector(lib, h)
 
 
+class _RefWireCfg(C.Structure):
+    _fields_ = [
+        ("n_layers", C.c_uint32),
+        ("square_cells", C.c_uint32),
+        ("first_layer_inner_radius", C.c_double),
+        ("half_z", C.c_double),
+        ("cell_size", C.c_double),
+        ("stereo_angle", C.c_double),
+        ("mat_radius", C.c_double),
+    ]
+
+
+def build_wire_chamber(n_layers=10, square_cells=True,
+                       first_layer_inner_radius=500.0, half_z=1000.0,
+                       cell_size=10.0, stereo_angle=0.05, mat_radius=0.015,
+                       precision="f64") -> RefDetector:
+    """The reference's wire chamber (tests/include/detray/test/common/
+    build_wire_chamber.hpp) with drift cells (square) or straw tubes."""
+    lib = load(precision)
+    lib.ref_build_wire_chamber.argtypes = [C.POINTER(_RefWireCfg),
+                                           C.POINTER(C.c_void_p)]
+    cfg = _RefWireCfg(n_layers, int(square_cells), first_layer_inner_radius,
+                      half_z, cell_size, stereo_angle, mat_radius)
+    h = C.c_void_p()
+    _check(lib, lib.ref_build_wire_chamber(C.byref(cfg), C.byref(h)))
+    return RefDetector(lib, h)
+
+
 def build_telescope(positions=tuple(50.0 * i for i in range(10)),
                     half_x=500.0, half_y=500.0, pilot_dir=(1.0, 0.0, 0.0),
                     mat_thickness=0.3, envelope=0.0,

@@ -79,3 +79,43 @@ def test_core_noise_estimation_and_no_material(core_host, oracle):
         s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
                     tol_rel=1e-7, cov_rel=tight_cov)
         assert s["seq_mismatch"] == 0, kw
+
+
+WIRE = {"wire_chamber_10l_cells": True, "wire_chamber_10l_straws": False}
+
+
+@pytest.mark.parametrize("name", ["toy_4brl_7edc", "telescope_10x1m_300um",
+                                  *WIRE])
+def test_committed_geometries_match_reference_builders(oracle, name):
+    """The .npz geometries the product ships are byte-identical to the
+    tables the reference's own builders produce through dprop::flatten."""
+    from detray_b200 import geometry
+    if name.startswith("toy"):
+        det = oracle.build_toy()
+    elif name.startswith("telescope"):
+        det = oracle.build_telescope()
+    else:
+        det = oracle.build_wire_chamber(square_cells=WIRE[name])
+    ref = det.tables()
+    got = geometry.load_geometry(name)
+    for key, _ in geometry.TABLES:
+        assert ref[key].tobytes() == got[key].tobytes(), key
+
+
+@pytest.mark.parametrize("square", [True, False])
+def test_core_f64_matches_reference_wire_chamber(core_host, oracle, square):
+    """Line surfaces (drift cells / straw tubes), material rods on the wires
+    and grids with several surfaces per bin: same surfaces and parameters
+    as the reference in double precision, loopers included."""
+    from detray_b200 import abi, tracks
+    det = oracle.build_wire_chamber(square_cells=square)
+    cfg = abi.make_config(max_records=64, search_window=(3, 3),
+                          estimate_scattering_noise=0)
+    trk = tracks.toy_tracks(1500, seed=5, pt_range=(0.1, 100.0),
+                            eta_range=(-1.0, 1.0), vertex_sigma=(0, 0, 0))
+    ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)}, cfg, trk)
+    assert ref["n_records"].mean() > 8
+    got = run_core(core_host, oracle, det.desc, cfg, trk, 8)
+    s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
+                tol_rel=1e-7, cov_rel=1e-5)
+    assert s["seq_mismatch"] == 0 and s["status_mismatch"] == 0

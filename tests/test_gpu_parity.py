@@ -50,6 +50,12 @@ def _setup(kind):
         tables = geometry.load_geometry("telescope_10x1m_300um")
         cfg = abi.make_config(max_records=16)
         trk = tracks.telescope_tracks(4000, seed=11)
+    elif kind.startswith("wire"):
+        tables = geometry.load_geometry(kind)
+        cfg = abi.make_config(max_records=64, search_window=(3, 3),
+                              estimate_scattering_noise=0)
+        trk = tracks.toy_tracks(20000, seed=13, pt_range=(0.1, 100.0),
+                                eta_range=(-1.0, 1.0), vertex_sigma=(0, 0, 0))
     else:
         tables = geometry.load_geometry("toy_4brl_7edc")
         cfg = abi.make_config(max_records=32, search_window=(3, 3))
@@ -59,11 +65,16 @@ def _setup(kind):
     return det, field, cfg, trk
 
 
-@pytest.mark.parametrize("kind", ["telescope", "toy"])
+@pytest.mark.parametrize("kind", ["telescope", "toy", "wire_chamber_10l_cells",
+                                  "wire_chamber_10l_straws"])
 def test_device_vs_oracle(torch_cuda, oracle, kind):
     det, field, cfg, trk = _setup(kind)
-    ref_det = (oracle.build_telescope() if kind == "telescope"
-               else oracle.build_toy())
+    if kind == "telescope":
+        ref_det = oracle.build_telescope()
+    elif kind.startswith("wire"):
+        ref_det = oracle.build_wire_chamber(square_cells=kind.endswith("cells"))
+    else:
+        ref_det = oracle.build_toy()
     ref = oracle.propagate(ref_det, field.spec, cfg, trk)
     got = _run_device(torch_cuda, det, field, cfg, trk)
     summary = compare(ref, got, max_seq_mismatch_frac=1e-3, tol_abs=TOL_ABS,
