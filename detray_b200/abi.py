@@ -218,7 +218,8 @@ class Launch(C.Structure):
         ("ctas_per_sm", C.c_uint32),
         ("sort_tracks", C.c_uint32),
         ("use_graph", C.c_uint32),
-        ("reserved", C.c_uint32 * 3),
+        ("precision", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 

@@ -31,6 +31,10 @@ dprop_status enqueue_direction_sort(const float* dx, const float* dy,
                                     const float* dz, uint64_t n, void* scratch,
                                     size_t scratch_bytes, cudaStream_t stream,
                                     const uint32_t** order);
+dprop_status enqueue_direction_sort(const double* dx, const double* dy,
+                                    const double* dz, uint64_t n, void* scratch,
+                                    size_t scratch_bytes, cudaStream_t stream,
+                                    const uint32_t** order);
 
 }  // namespace dprop::api
 
@@ -52,7 +56,26 @@ struct dprop_detector {
     uint32_t* bf_surfaces{nullptr};
     dprop::dev_grid<float>* grids{nullptr};
     uint32_t* grid_bins{nullptr};
+    // double-precision copies of the floating-point tables (fp64 launches)
+    dprop::dev_mask<double>* masks_d{nullptr};
+    dprop::dev_transform<double>* transforms_d{nullptr};
+    dprop::dev_slab<double>* slabs_d{nullptr};
+    dprop::dev_grid<double>* grids_d{nullptr};
     uint32_t n_volumes{0}, n_surfaces{0};
+    dprop::detector_view<double> view_d() const {
+        dprop::detector_view<double> v;
+        v.volumes = volumes;
+        v.surfaces = surfaces;
+        v.masks = masks_d;
+        v.transforms = transforms_d;
+        v.slabs = slabs_d;
+        v.bf_surfaces = bf_surfaces;
+        v.grids = grids_d;
+        v.grid_bins = grid_bins;
+        v.n_volumes = n_volumes;
+        v.n_surfaces = n_surfaces;
+        return v;
+    }
     dprop::detector_view<float> view() const {
         dprop::detector_view<float> v;
         v.volumes = volumes;
@@ -73,4 +96,17 @@ struct dprop_field {
     int device{0};
     float4* nodes{nullptr};
     dprop::field_view<float> view{};
+    dprop::field_view<double> view_d{};  // same nodes, double arithmetic
 };
+
+namespace dprop::api {
+
+// fp64 propagation (dprop_launch.precision == 8): double inputs, arithmetic
+// and results; plain one-thread-per-track kernel, optional direction sort.
+dprop_status propagate_fp64(const dprop_config& cfg, const dprop_launch* lc,
+                            const dprop_detector* det, const dprop_field* field,
+                            const dprop_tracks& tracks,
+                            const dprop_results& results, uint64_t n,
+                            cudaStream_t stream);
+
+}  // namespace dprop::api

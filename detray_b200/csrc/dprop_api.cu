@@ -244,6 +244,14 @@ dprop_status enqueue_direction_sort(const float* dx, const float* dy,
                                order);
 }
 
+dprop_status enqueue_direction_sort(const double* dx, const double* dy,
+                                    const double* dz, uint64_t n, void* scratch,
+                                    size_t scratch_bytes, cudaStream_t stream,
+                                    const uint32_t** order) {
+    return enqueue_sort<double>(dx, dy, dz, n, scratch, scratch_bytes, stream,
+                                order);
+}
+
 }  // namespace dprop::api
 
 using dprop::api::occupancy_of;
@@ -883,6 +891,14 @@ dprop_status dprop_detector_create(const dprop_detector_desc* d, int device,
         dprop_detector_destroy(det);
         return st;
     }
+    const host_tables<double> td = convert_desc<double>(d);
+    if ((st = upload(td.masks, &det->masks_d)) != DPROP_OK ||
+        (st = upload(td.transforms, &det->transforms_d)) != DPROP_OK ||
+        (st = upload(td.slabs, &det->slabs_d)) != DPROP_OK ||
+        (st = upload(td.grids, &det->grids_d)) != DPROP_OK) {
+        dprop_detector_destroy(det);
+        return st;
+    }
     *out = det;
     return DPROP_OK;
 }
@@ -899,6 +915,10 @@ dprop_status dprop_detector_destroy(dprop_detector* det) {
     cudaFree(det->bf_surfaces);
     cudaFree(det->grids);
     cudaFree(det->grid_bins);
+    cudaFree(det->masks_d);
+    cudaFree(det->transforms_d);
+    cudaFree(det->slabs_d);
+    cudaFree(det->grids_d);
     delete det;
     return DPROP_OK;
 }
@@ -1019,6 +1039,12 @@ dprop_status dprop_field_create_const(double bx, double by, double bz,
     f->view.b[1] = static_cast<float>(by);
     f->view.b[2] = static_cast<float>(bz);
     f->view.nodes = nullptr;
+    f->view_d.kind = 0u;
+    f->view_d.n_r = f->view_d.n_phi = f->view_d.n_z = 1u;
+    f->view_d.b[0] = bx;
+    f->view_d.b[1] = by;
+    f->view_d.b[2] = bz;
+    f->view_d.nodes = nullptr;
     *out = f;
     return DPROP_OK;
 }
@@ -1059,6 +1085,19 @@ dprop_status dprop_field_create_grid(const double* lo, const double* hi,
     v.z_lo = static_cast<float>(lo[2]);
     v.z_step_inv = n[2] > 1 ? static_cast<float>((n[2] - 1) / (hi[2] - lo[2])) : 0.f;
     v.nodes = f->nodes;
+    field_view<double>& vd = f->view_d;
+    vd.kind = 1u;
+    vd.n_r = n[0];
+    vd.n_phi = n[1];
+    vd.n_z = n[2];
+    vd.b[0] = vd.b[1] = vd.b[2] = 0.;
+    vd.r_lo = lo[0];
+    vd.r_step_inv = n[0] > 1 ? (n[0] - 1) / (hi[0] - lo[0]) : 0.;
+    vd.phi_lo = lo[1];
+    vd.phi_step_inv = n[1] / (2.0 * constant::pi);
+    vd.z_lo = lo[2];
+    vd.z_step_inv = n[2] > 1 ? (n[2] - 1) / (hi[2] - lo[2]) : 0.;
+    vd.nodes = f->nodes;
     *out = f;
     return DPROP_OK;
 }
@@ -1094,6 +1133,14 @@ dprop_status dprop_propagate(const dprop_config* cfg, const dprop_launch* lc,
     }
     if (!tracks->time || !tracks->qop || !results->status) {
         return fail(DPROP_E_INVALID, "propagate: missing track/status array");
+    }
+    if (lc && lc->precision == 8u) {
+        return dprop::api::propagate_fp64(*cfg, lc, det, field, *tracks,
+                                          *results, n,
+                                          static_cast<cudaStream_t>(stream));
+    }
+    if (lc && lc->precision != 0u && lc->precision != 4u) {
+        return fail(DPROP_E_INVALID, "propagate: precision must be 0, 4 or 8");
     }
     const io_ptrs<float> io = make_io<float>(*tracks, *results);
     return launch<float>(*cfg, lc, det, field, io, n,

@@ -1,0 +1,102 @@
+// fp64 propagation: the propagation core instantiated in double precision
+// (the reference's full-fp64 build, DETRAY_CUSTOM_SCALARTYPE=double), for
+// dprop_propagate with dprop_launch.precision = 8.  Track arrays, arithmetic
+// and results are double; the field map nodes stay float4 (the reference's
+// covfie field stores floats) and are interpolated in double.
+//
+// Kernel:
+//   propagate_fp64_kernel<MB>  one thread per track, the whole propagation,
+//                              register budget MB resident CTAs of 128
+//                              threads per SM (8: 64 registers, 12: 40)
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "api_common.cuh"
+#include "core/config.hpp"
+#include "track_io.cuh"
+
+using namespace dprop;
+using dprop::api::fail;
+
+namespace {
+
+constexpr int k_f64_block = 128;
+
+template <int MinBlocks>
+__global__ void __launch_bounds__(k_f64_block, MinBlocks)
+    propagate_fp64_kernel(const detector_view<double> det,
+                          const field_view<double> field,
+                          const prop_cfg<double> cfg,
+                          const api::io_ptrs<double, double> io, uint64_t n,
+                          const uint32_t* __restrict__ order) {
+    const uint64_t i =
+        static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
+    api::run_one(t, n, det, field, cfg, io);
+}
+
+// library-owned grow-only sort scratch of fp64 launches
+struct f64_sort_scratch {
+    void* buf{nullptr};
+    size_t bytes{0};
+    int device{-1};
+};
+f64_sort_scratch g_f64_sort;
+std::mutex g_f64_mutex;
+
+}  // namespace
+
+namespace dprop::api {
+
+dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
+                            const dprop_detector* det, const dprop_field* field,
+                            const dprop_tracks& tracks,
+                            const dprop_results& results, uint64_t n,
+                            cudaStream_t stream) {
+    if (n > 0x7fffffffull * k_f64_block) {
+        return fail(DPROP_E_INVALID, "propagate fp64: too many tracks");
+    }
+    const io_ptrs<double, double> io = make_io<double, double>(tracks, results);
+    std::lock_guard<std::mutex> lock(g_f64_mutex);
+    const uint32_t* order = nullptr;
+    if (lc && lc->sort_tracks) {
+        const size_t need = sort_scratch_bytes(n);
+        int dev = 0;
+        DPROP_CUDA(cudaGetDevice(&dev));
+        if (g_f64_sort.bytes < need || g_f64_sort.device != dev) {
+            if (g_f64_sort.buf) {
+                DPROP_CUDA(cudaStreamSynchronize(stream));
+                cudaFree(g_f64_sort.buf);
+                g_f64_sort.buf = nullptr;
+                g_f64_sort.bytes = 0;
+            }
+            DPROP_CUDA(cudaMalloc(&g_f64_sort.buf, need));
+            g_f64_sort.bytes = need;
+            g_f64_sort.device = dev;
+        }
+        const dprop_status s = enqueue_direction_sort(
+            io.trk[4], io.trk[5], io.trk[6], n, g_f64_sort.buf,
+            g_f64_sort.bytes, stream, &order);
+        if (s != DPROP_OK) {
+            return s;
+        }
+    }
+    const prop_cfg<double> pc = make_prop_cfg<double>(c);
+    const unsigned int grid =
+        static_cast<unsigned int>((n + k_f64_block - 1) / k_f64_block);
+    if (occupancy_of(lc) >= 12) {
+        propagate_fp64_kernel<12><<<grid, k_f64_block, 0, stream>>>(
+            det->view_d(), field->view_d, pc, io, n, order);
+    } else {
+        propagate_fp64_kernel<8><<<grid, k_f64_block, 0, stream>>>(
+            det->view_d(), field->view_d, pc, io, n, order);
+    }
+    DPROP_CUDA(cudaGetLastError());
+    return DPROP_OK;
+}
+
+}  // namespace dprop::api

@@ -6,29 +6,30 @@
 
 namespace dprop::api {
 
-// Device pointers of the inputs/outputs, by value into the kernels
-template <typename In>
+// Device pointers of the inputs/outputs, by value into the kernels: In is
+// the element type of the track inputs, S the arithmetic and result type.
+template <typename In, typename S = float>
 struct io_ptrs {
     const In* trk[8];
     uint8_t* status;
     uint32_t* n_records;
     uint32_t* n_steps;
     uint32_t* n_trials;
-    float* path_length;
-    float* final_free[8];
+    S* path_length;
+    S* final_free[8];
     uint64_t* rec_barcode;
-    float* rec_bound[6];
-    float* rec_cov[21];
-    float* rec_path;
+    S* rec_bound[6];
+    S* rec_cov[21];
+    S* rec_path;
     uint8_t* rec_flags;
     uint32_t* n_isect;
     uint32_t* n_transport;
     uint32_t* n_material;
 };
 
-template <typename In>
-io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
-    io_ptrs<In> io{};
+template <typename In, typename S = float>
+io_ptrs<In, S> make_io(const dprop_tracks& t, const dprop_results& r) {
+    io_ptrs<In, S> io{};
     for (int i = 0; i < 3; ++i) {
         io.trk[i] = static_cast<const In*>(t.pos[i]);
         io.trk[4 + i] = static_cast<const In*>(t.dir[i]);
@@ -39,18 +40,18 @@ io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
     io.n_records = r.n_records;
     io.n_steps = r.n_steps;
     io.n_trials = r.n_trials;
-    io.path_length = static_cast<float*>(r.path_length);
+    io.path_length = static_cast<S*>(r.path_length);
     for (int i = 0; i < 8; ++i) {
-        io.final_free[i] = static_cast<float*>(r.final_free[i]);
+        io.final_free[i] = static_cast<S*>(r.final_free[i]);
     }
     io.rec_barcode = r.rec_barcode;
     for (int i = 0; i < 6; ++i) {
-        io.rec_bound[i] = static_cast<float*>(r.rec_bound[i]);
+        io.rec_bound[i] = static_cast<S*>(r.rec_bound[i]);
     }
     for (int i = 0; i < 21; ++i) {
-        io.rec_cov[i] = static_cast<float*>(r.rec_cov[i]);
+        io.rec_cov[i] = static_cast<S*>(r.rec_cov[i]);
     }
-    io.rec_path = static_cast<float*>(r.rec_path);
+    io.rec_path = static_cast<S*>(r.rec_path);
     io.rec_flags = r.rec_flags;
     io.n_isect = r.n_intersections;
     io.n_transport = r.n_transports;
@@ -58,28 +59,29 @@ io_ptrs<In> make_io(const dprop_tracks& t, const dprop_results& r) {
     return io;
 }
 
-// One track from its inputs to its results.  With Adjoint the propagation
-// also writes the derivative tape of track t (adjoint.cuh).
-template <typename In, bool Adjoint = false>
+// One track from its inputs to its results, in arithmetic type S.  With
+// Adjoint the propagation also writes the derivative tape of track t
+// (adjoint.cuh).
+template <typename In, bool Adjoint = false, typename S = float>
 __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
-                                        const detector_view<float>& det,
-                                        const field_view<float>& field,
-                                        const prop_cfg<float>& cfg,
-                                        const io_ptrs<In>& io,
-                                        const tape_view<float>& tv = {}) {
-    const vec3<float> pos{static_cast<float>(io.trk[0][t]),
-                          static_cast<float>(io.trk[1][t]),
-                          static_cast<float>(io.trk[2][t])};
-    const vec3<float> dir{static_cast<float>(io.trk[4][t]),
-                          static_cast<float>(io.trk[5][t]),
-                          static_cast<float>(io.trk[6][t])};
-    const float time = static_cast<float>(io.trk[3][t]);
-    const float qop = static_cast<float>(io.trk[7][t]);
+                                        const detector_view<S>& det,
+                                        const field_view<S>& field,
+                                        const prop_cfg<S>& cfg,
+                                        const io_ptrs<In, S>& io,
+                                        const tape_view<S>& tv = {}) {
+    const vec3<S> pos{static_cast<S>(io.trk[0][t]),
+                      static_cast<S>(io.trk[1][t]),
+                      static_cast<S>(io.trk[2][t])};
+    const vec3<S> dir{static_cast<S>(io.trk[4][t]),
+                      static_cast<S>(io.trk[5][t]),
+                      static_cast<S>(io.trk[6][t])};
+    const S time = static_cast<S>(io.trk[3][t]);
+    const S qop = static_cast<S>(io.trk[7][t]);
 
-    track_state<float> ts;
+    track_state<S> ts;
     init_track_state(ts, pos, time, dir, qop, cfg);
 
-    record_sink<float> rec;
+    record_sink<S> rec;
     rec.barcode = io.rec_barcode;
     for (int i = 0; i < 6; ++i) {
         rec.bound[i] = io.rec_bound[i];
@@ -96,7 +98,7 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
 
     uint8_t status;
     if constexpr (Adjoint) {
-        adjoint_tape<float> tape;
+        adjoint_tape<S> tape;
         tape.v = tv;
         tape.track = t;
         status = propagate_track(ts, det, field, cfg, rec, tape);
@@ -111,10 +113,10 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     if (io.n_isect) io.n_isect[t] = ts.nav.n_isect;
     if (io.n_transport) io.n_transport[t] = ts.n_transport;
     if (io.n_material) io.n_material[t] = ts.n_material;
-    if (io.path_length) io.path_length[t] = static_cast<float>(ts.step.path_length);
-    const float fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
-                          ts.step.time,  ts.step.dir.x, ts.step.dir.y,
-                          ts.step.dir.z, ts.step.qop};
+    if (io.path_length) io.path_length[t] = static_cast<S>(ts.step.path_length);
+    const S fin[8] = {ts.step.pos.x, ts.step.pos.y, ts.step.pos.z,
+                      ts.step.time,  ts.step.dir.x, ts.step.dir.y,
+                      ts.step.dir.z, ts.step.qop};
     for (int i = 0; i < 8; ++i) {
         if (io.final_free[i]) io.final_free[i][t] = fin[i];
     }

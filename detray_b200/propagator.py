@@ -170,13 +170,16 @@ class Field:
 
 def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
                 ctas_per_sm: int = 0, sort_tracks: int = 0,
-                use_graph: int = 0) -> abi.Launch:
+                use_graph: int = 0, precision: int = 0) -> abi.Launch:
+    """Launch shape; ``precision`` 8 runs the propagation in fp64 end to end
+    (double track tensors and results)."""
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
     lc.ctas_per_sm = ctas_per_sm
     lc.sort_tracks = sort_tracks
     lc.use_graph = use_graph
+    lc.precision = precision
     return lc
 
 
@@ -189,9 +192,12 @@ class DeviceResults:
 
 
 def alloc_device_results(n: int, max_records: int, device="cuda",
-                         with_records=True, with_cov=True) -> DeviceResults:
+                         with_records=True, with_cov=True,
+                         dtype=None) -> DeviceResults:
+    """Result buffers; floating-point fields in ``dtype`` (float32 default,
+    float64 for fp64 launches)."""
     import torch
-    f32 = dict(dtype=torch.float32, device=device)
+    f32 = dict(dtype=dtype or torch.float32, device=device)
     t = {
         "status": torch.empty(n, dtype=torch.uint8, device=device),
         "n_records": torch.empty(n, dtype=torch.int32, device=device),
@@ -257,12 +263,15 @@ def propagate(cfg: abi.Config, det: Detector, field: Field, tracks,
     import torch
     if not (hasattr(tracks, "is_cuda") and tracks.is_cuda):
         raise PropagationError("propagate() needs a CUDA tensor of tracks")
-    if tracks.dtype != torch.float32 or tracks.dim() != 2 or tracks.shape[0] != 8:
-        raise PropagationError("tracks must be a (8, n) float32 tensor")
+    fp64 = launch is not None and launch.precision == 8
+    want = torch.float64 if fp64 else torch.float32
+    if tracks.dtype != want or tracks.dim() != 2 or tracks.shape[0] != 8:
+        raise PropagationError(f"tracks must be a (8, n) {want} tensor")
     tracks = tracks.contiguous()
     n = tracks.shape[1]
     if results is None:
-        results = alloc_device_results(n, cfg.max_records, tracks.device)
+        results = alloc_device_results(n, cfg.max_records, tracks.device,
+                                       dtype=want)
     if stream is None:
         stream = torch.cuda.current_stream(tracks.device)
     ts = tracks_struct(tracks)

@@ -305,7 +305,14 @@ typedef struct dprop_launch {
     uint32_t use_graph;          /* 1: capture the whole propagate call into a
                                     CUDA graph on first use and replay it on
                                     later calls with identical arguments       */
-    uint32_t reserved[3];
+    uint32_t precision;          /* 0 or 4: fp32 arithmetic, float track
+                                    arrays and results (the default);
+                                    8: fp64 end to end - double track arrays,
+                                    double arithmetic and double results (the
+                                    reference's full-fp64 build); plain kernel,
+                                    method and use_graph ignored.  Device API
+                                    (dprop_propagate) only                     */
+    uint32_t reserved[2];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */

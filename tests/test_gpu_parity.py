@@ -253,3 +253,28 @@ def test_graph_replay_and_autotune(torch_cuda):
     assert lc.ctas_per_sm in (8, 12, 16)
     assert lc.method in (abi.METHOD_PLAIN, abi.METHOD_PERSISTENT)
     assert all(t > 0 for t in times)
+
+
+@pytest.mark.parametrize("kind", ["toy", "wire_chamber_10l_cells"])
+def test_fp64_device_vs_oracle(torch_cuda, oracle, kind):
+    """dprop_launch.precision = 8: the propagation core in double on the
+    GPU (the reference's full-fp64 build) against the fp64 oracle.  Only the
+    device math library's last bits differ from the host's: same surfaces
+    except <= 0.01 % of tracks, parameters to ~1e-9."""
+    from detray_b200 import propagator
+    det, field, cfg, trk = _setup(kind)
+    ref_det = (oracle.build_toy() if kind == "toy"
+               else oracle.build_wire_chamber(square_cells=True))
+    ref = oracle.propagate(ref_det, field.spec, cfg, trk)
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float64, device="cuda")
+    lc = propagator.make_launch(sort_tracks=1, precision=8)
+    res = propagator.propagate(cfg, det, field, dev, launch=lc)
+    torch_cuda.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+    got["rec_barcode"] = got["rec_barcode"].view(np.uint64)
+    assert res.tensors["rec_bound"].dtype == torch_cuda.float64
+    tight = {"loc0": 1e-6, "loc1": 1e-6, "phi": 1e-9, "theta": 1e-9,
+             "qop": 1e-12, "time": 1e-9}
+    s = compare(ref, got, max_seq_mismatch_frac=1e-4, tol_abs=tight,
+                tol_rel=1e-8, cov_rel=1e-6)
+    print(kind, s)
