@@ -56,6 +56,9 @@ def parse_args():
                    default="auto")
     p.add_argument("--no-sort", action="store_true",
                    help="propagate in input order instead of direction order")
+    p.add_argument("--ctas", type=int, default=12, choices=(8, 12, 16),
+                   help="register budget (resident CTAs per SM) when "
+                        "--method is not auto")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true",
@@ -375,7 +378,7 @@ def run_ours(args):
                   "persistent": abi.METHOD_PERSISTENT}[args.method]
         lc = propagator.make_launch(method=method,
                                     sort_tracks=int(not args.no_sort),
-                                    ctas_per_sm=12, use_graph=1)
+                                    ctas_per_sm=args.ctas, use_graph=1)
     method = lc.method
 
     def step():

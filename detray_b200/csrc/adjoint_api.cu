@@ -28,12 +28,12 @@ namespace {
 
 constexpr int k_adj_block = 128;
 
-template <int MinBlocks>
+template <int MinBlocks, bool W>
 __global__ void __launch_bounds__(k_adj_block, MinBlocks)
-    propagate_adjoint_kernel(const detector_view<float> det,
-                             const field_view<float> field,
-                             const prop_cfg<float> cfg,
-                             const api::io_ptrs<float> io,
+    propagate_adjoint_kernel(const __grid_constant__ detector_view<float, W> det,
+                             const __grid_constant__ field_view<float> field,
+                             const __grid_constant__ prop_cfg<float> cfg,
+                             const __grid_constant__ api::io_ptrs<float> io,
                              const tape_view<float> tv, uint64_t n,
                              const uint32_t* __restrict__ order) {
     const uint64_t i =
@@ -97,14 +97,19 @@ std::mutex g_adj_mutex;
 
 template <int MB>
 void launch_adjoint_mb(unsigned int grid, cudaStream_t st,
-                       const detector_view<float>& det,
+                       const dprop_detector* det,
                        const field_view<float>& field,
                        const prop_cfg<float>& cfg,
                        const api::io_ptrs<float>& io,
                        const tape_view<float>& tv, uint64_t n,
                        const uint32_t* order) {
-    propagate_adjoint_kernel<MB><<<grid, k_adj_block, 0, st>>>(
-        det, field, cfg, io, tv, n, order);
+    if (det->wires) {
+        propagate_adjoint_kernel<MB, true><<<grid, k_adj_block, 0, st>>>(
+            det->view_as<true>(), field, cfg, io, tv, n, order);
+    } else {
+        propagate_adjoint_kernel<MB, false><<<grid, k_adj_block, 0, st>>>(
+            det->view_as<false>(), field, cfg, io, tv, n, order);
+    }
 }
 
 }  // namespace
@@ -196,13 +201,12 @@ dprop_status dprop_propagate_adjoint(const dprop_config* cfg,
     const unsigned int grid =
         static_cast<unsigned int>((n + k_adj_block - 1) / k_adj_block);
     const int mb = api::occupancy_of(lc);
-    const detector_view<float> dv = det->view();
     if (mb == 8) {
-        launch_adjoint_mb<8>(grid, st, dv, field->view, pc, io, tv, n, order);
+        launch_adjoint_mb<8>(grid, st, det, field->view, pc, io, tv, n, order);
     } else if (mb == 12) {
-        launch_adjoint_mb<12>(grid, st, dv, field->view, pc, io, tv, n, order);
+        launch_adjoint_mb<12>(grid, st, det, field->view, pc, io, tv, n, order);
     } else {
-        launch_adjoint_mb<16>(grid, st, dv, field->view, pc, io, tv, n, order);
+        launch_adjoint_mb<16>(grid, st, det, field->view, pc, io, tv, n, order);
     }
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;

@@ -62,6 +62,9 @@ struct dprop_detector {
     dprop::dev_slab<double>* slabs_d{nullptr};
     dprop::dev_grid<double>* grids_d{nullptr};
     uint32_t n_volumes{0}, n_surfaces{0};
+    // the detector holds line surfaces, material rods or multi-entry grid
+    // bins: launches use the kernels that include the code for them
+    bool wires{false};
     dprop::detector_view<double> view_d() const {
         dprop::detector_view<double> v;
         v.volumes = volumes;
@@ -76,8 +79,10 @@ struct dprop_detector {
         v.n_surfaces = n_surfaces;
         return v;
     }
-    dprop::detector_view<float> view() const {
-        dprop::detector_view<float> v;
+    dprop::detector_view<float> view() const { return view_as<true>(); }
+    template <bool W>
+    dprop::detector_view<float, W> view_as() const {
+        dprop::detector_view<float, W> v;
         v.volumes = volumes;
         v.surfaces = surfaces;
         v.masks = masks;

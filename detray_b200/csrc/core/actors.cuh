@@ -71,14 +71,39 @@ DPROP_HD void line_frame(const dev_transform<S>& trf, vec3<S> dir,
     nz = cross(nx, ny);
 }
 
+// x and y axes of the line frame (the loc0 / loc1 directions)
+template <typename S>
+struct axes2 {
+    vec3<S> x, y;
+};
+
+template <typename S>
+DPROP_HD_LINE axes2<S> line_loc_axes(const dev_transform<S>& trf, vec3<S> dir) {
+    axes2<S> a;
+    vec3<S> nz;
+    line_frame(trf, dir, a.x, a.y, nz);
+    return a;
+}
+
+// line2D::local_to_global
+template <typename S>
+DPROP_HD_LINE vec3<S> line_to_global(const dev_transform<S>& trf, S l0, S l1,
+                                     vec3<S> dir) {
+    const vec3<S> on_wire = trf.point_to_global({S(0), S(0), l1});
+    return on_wire + l0 * normalize(cross(trf.z(), dir));
+}
+
 // bound -> free position for the surface frame (bound_to_free_vector,
 // tracks/detail/transform_track_parameters.hpp:43-74); the line frame needs
 // the track direction (line2D::local_to_global)
-template <typename S>
-DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S, W>& det,
                                    const dev_surface& sf, S l0, S l1,
                                    vec3<S> dir) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
+    if (W && sf.shape == e_line) {
+        return line_to_global(trf, l0, l1, dir);
+    }
     switch (sf.shape) {
         case e_ring:
             return trf.point_to_global({l0 * cos(l1), l0 * sin(l1), S(0)});
@@ -86,22 +111,20 @@ DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S>& det,
             const S r = det.masks[sf.mask_begin].v[0];
             return {r * cos(l0), r * sin(l0), l1};
         }
-        case e_line: {
-            const vec3<S> on_wire = trf.point_to_global({S(0), S(0), l1});
-            return on_wire + l0 * normalize(cross(trf.z(), dir));
-        }
         default:
             return trf.point_to_global({l0, l1, S(0)});
     }
 }
 
 // free -> bound vector on a surface (free_to_bound_vector)
-template <typename S>
-DPROP_HD void free_to_bound(const detector_view<S>& det, const dev_surface& sf,
+template <typename S, bool W>
+DPROP_HD void free_to_bound(const detector_view<S, W>& det, const dev_surface& sf,
                             const step_state<S>& st, S out[6]) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
-    if (sf.shape == e_line) {
-        line_bound_local(trf, st.pos, st.dir, out[0], out[1]);
+    if (W && sf.shape == e_line) {
+        const local2<S> l = line_bound_local(trf, st.pos, st.dir);
+        out[0] = l.l0;
+        out[1] = l.l1;
     } else {
         global_to_bound_local(sf.shape, trf, st.pos, out[0], out[1]);
     }
@@ -112,16 +135,17 @@ DPROP_HD void free_to_bound(const detector_view<S>& det, const dev_surface& sf,
 }
 
 // columns d(pos)/d(loc0), d(pos)/d(loc1) (get_derivative_dpos_dloc)
-template <typename S>
-DPROP_HD void dpos_dloc(const detector_view<S>& det, const dev_surface& sf,
+template <typename S, bool W>
+DPROP_HD void dpos_dloc(const detector_view<S, W>& det, const dev_surface& sf,
                         vec3<S> pos, vec3<S> dir, vec3<S>& c0, vec3<S>& c1) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
+    if (W && sf.shape == e_line) {
+        const axes2<S> a = line_loc_axes(trf, dir);
+        c0 = a.x;
+        c1 = a.y;
+        return;
+    }
     switch (sf.shape) {
-        case e_line: {
-            vec3<S> nz;
-            line_frame(trf, dir, c0, c1, nz);
-            return;
-        }
         case e_ring: {
             const vec3<S> l = trf.point_to_local(pos);
             const S lrad = perp(l);
@@ -149,16 +173,17 @@ DPROP_HD void dpos_dloc(const detector_view<S>& det, const dev_surface& sf,
 }
 
 // rows d(loc0)/d(pos), d(loc1)/d(pos) (get_derivative_dloc_dpos)
-template <typename S>
-DPROP_HD void dloc_dpos(const detector_view<S>& det, const dev_surface& sf,
+template <typename S, bool W>
+DPROP_HD void dloc_dpos(const detector_view<S, W>& det, const dev_surface& sf,
                         vec3<S> pos, vec3<S> dir, vec3<S>& r0, vec3<S>& r1) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
+    if (W && sf.shape == e_line) {
+        const axes2<S> a = line_loc_axes(trf, dir);
+        r0 = a.x;
+        r1 = a.y;
+        return;
+    }
     switch (sf.shape) {
-        case e_line: {
-            vec3<S> nz;
-            line_frame(trf, dir, r0, r1, nz);
-            return;
-        }
         case e_ring: {
             const vec3<S> l = trf.point_to_local(pos);
             const S lrad = perp(l);
@@ -186,8 +211,8 @@ DPROP_HD void dloc_dpos(const detector_view<S>& det, const dev_surface& sf,
 }
 
 // surface normal used by the path derivative and the incidence angle
-template <typename S>
-DPROP_HD vec3<S> surface_normal_at_pos(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD vec3<S> surface_normal_at_pos(const detector_view<S, W>& det,
                                        const dev_surface& sf, vec3<S> pos) {
     if (sf.shape == e_concentric_cylinder) {
         const S ph = phi_of(pos);
@@ -196,8 +221,8 @@ DPROP_HD vec3<S> surface_normal_at_pos(const detector_view<S>& det,
     return det.transforms[sf.transform].z();
 }
 
-template <typename S>
-DPROP_HD vec3<S> surface_normal_at_bound(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD vec3<S> surface_normal_at_bound(const detector_view<S, W>& det,
                                          const dev_surface& sf, S l0) {
     if (sf.shape == e_concentric_cylinder) {
         return {cos(l0), sin(l0), S(0)};
@@ -210,19 +235,27 @@ DPROP_HD vec3<S> surface_normal_at_bound(const detector_view<S>& det,
 // normal; for a line (jacobian_line.hpp path_derivative) the closest
 // approach also moves with the direction and the track's curvature.
 template <typename S>
-DPROP_HD void path_derivative(const detector_view<S>& det,
+DPROP_HD_LINE axes2<S> line_path_derivative(const dev_transform<S>& trf,
+                                            vec3<S> pos, vec3<S> dir,
+                                            vec3<S> dtds) {
+    const vec3<S> pc = pos - trf.translation();
+    const vec3<S> z = trf.z();
+    const S pz = dot(pc, z);
+    const S dz = dot(z, dir);
+    const vec3<S> pc_x = pc - pz * z;
+    const S norm = S(-1) / (S(1) - dz * dz + dot(pc_x, dtds));
+    return {norm * (dir - dz * z), norm * pc_x};
+}
+
+template <typename S, bool W>
+DPROP_HD void path_derivative(const detector_view<S, W>& det,
                               const dev_surface& sf, vec3<S> pos, vec3<S> dir,
                               vec3<S> dtds, vec3<S>& f_pos, vec3<S>& f_dir) {
-    if (sf.shape == e_line) {
-        const dev_transform<S>& trf = det.transforms[sf.transform];
-        const vec3<S> pc = pos - trf.translation();
-        const vec3<S> z = trf.z();
-        const S pz = dot(pc, z);
-        const S dz = dot(z, dir);
-        const vec3<S> pc_x = pc - pz * z;
-        const S norm = S(-1) / (S(1) - dz * dz + dot(pc_x, dtds));
-        f_pos = norm * (dir - dz * z);
-        f_dir = norm * pc_x;
+    if (W && sf.shape == e_line) {
+        const axes2<S> f = line_path_derivative(det.transforms[sf.transform],
+                                                pos, dir, dtds);
+        f_pos = f.x;
+        f_dir = f.y;
         return;
     }
     const vec3<S> n = surface_normal_at_pos(det, sf, pos);
@@ -234,19 +267,17 @@ DPROP_HD void path_derivative(const detector_view<S>& det,
 // d(pos)/d(phi), d(pos)/d(theta) of the line frame at fixed local position
 // (jacobian_line.hpp get_derivative_dpos_dangle); zero for the other frames.
 template <typename S>
-DPROP_HD void line_dpos_dangle(const dev_transform<S>& trf, vec3<S> pos,
-                               vec3<S> dir, vec3<S> dd_phi, vec3<S> dd_th,
-                               vec3<S>& c_phi, vec3<S>& c_th) {
-    S l0, l1;
-    line_bound_local(trf, pos, dir, l0, l1);
+DPROP_HD_LINE axes2<S> line_dpos_dangle(const dev_transform<S>& trf,
+                                        vec3<S> pos, vec3<S> dir,
+                                        vec3<S> dd_phi, vec3<S> dd_th) {
+    const local2<S> l = line_bound_local(trf, pos, dir);
     vec3<S> nx, ny, nz;
     line_frame(trf, dir, nx, ny, nz);
     const S ipdn = S(1) / dot(dir, nz);
-    const S C = ipdn * l0;
+    const S C = ipdn * l.l0;
     const vec3<S> y_phi = cross(ny, dd_phi);
     const vec3<S> y_th = cross(ny, dd_th);
-    c_phi = C * (y_phi - nx * dot(nx, y_phi));
-    c_th = C * (y_th - nx * dot(nx, y_th));
+    return {C * (y_phi - nx * dot(nx, y_phi)), C * (y_th - nx * dot(nx, y_th))};
 }
 
 // ---------------------------------------------------- full Jacobian
@@ -254,8 +285,8 @@ DPROP_HD void line_dpos_dangle(const dev_transform<S>& trf, vec3<S> pos,
 // the current (destination) free state.  Only rows 0..3 x cols 0..4 are
 // non-trivial (the q/p row and the time column are identity, as the
 // covariance-transport generator assumes); they are returned in G[4][5].
-template <typename S>
-DPROP_HD void full_jacobian(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void full_jacobian(const detector_view<S, W>& det,
                             const bound_state<S>& dep, const dev_surface& dep_sf,
                             const dev_surface& dst_sf, const step_state<S>& st,
                             vec3<S> dtds, S G[4][5]) {
@@ -303,11 +334,11 @@ DPROP_HD void full_jacobian(const detector_view<S>& det,
         m1d[r][3] = b3;
         m1d[r][4] = da[r];
     }
-    if (dep_sf.shape == e_line) {
+    if (W && dep_sf.shape == e_line) {
         // the line frame's position also moves with the angles
-        vec3<S> c_phi, c_th;
-        line_dpos_dangle(det.transforms[dep_sf.transform], dep_pos, dep_dir,
-                         dd_phi, dd_th, c_phi, c_th);
+        const axes2<S> cd = line_dpos_dangle(det.transforms[dep_sf.transform],
+                                             dep_pos, dep_dir, dd_phi, dd_th);
+        const vec3<S> c_phi = cd.x, c_th = cd.y;
         const S cpa[3] = {c_phi.x, c_phi.y, c_phi.z};
         const S cta[3] = {c_th.x, c_th.y, c_th.z};
         for (int r = 0; r < 3; ++r) {
@@ -324,7 +355,7 @@ DPROP_HD void full_jacobian(const detector_view<S>& det,
     for (int c = 0; c < 5; ++c) {
         s[c] = f[0] * m1p[0][c] + f[1] * m1p[1][c] + f[2] * m1p[2][c];
     }
-    if (dst_sf.shape == e_line) {
+    if (W && dst_sf.shape == e_line) {
         for (int c = 0; c < 5; ++c) {
             s[c] += f_dir.x * m1d[0][c] + f_dir.y * m1d[1][c] +
                     f_dir.z * m1d[2][c];
@@ -488,7 +519,7 @@ DPROP_HD S scattering_theta0(S x_over_x0, const rel_quantities<S>& rq, S q,
 // Path through a rod of radius r around a line surface at closest approach
 // d (material_rod::path_segment)
 template <typename S>
-DPROP_HD S rod_path(S r, S cos_inc, S d) {
+DPROP_HD_LINE S rod_path(S r, S cos_inc, S d) {
     if (fabs(d) > r) {
         return S(0);
     }
@@ -497,8 +528,8 @@ DPROP_HD S rod_path(S r, S cos_inc, S d) {
 }
 
 // pointwise_material_interactor::update on the bound state
-template <typename S>
-DPROP_HD bool interact(const detector_view<S>& det, const dev_surface& sf,
+template <typename S, bool W>
+DPROP_HD bool interact(const detector_view<S, W>& det, const dev_surface& sf,
                        bound_state<S>& b, const actor_cfg<S>& cfg, S q,
                        S nav_dir) {
     if (sf.material == k_invalid) {
@@ -516,7 +547,7 @@ DPROP_HD bool interact(const detector_view<S>& det, const dev_surface& sf,
         return false;
     }
     S path_segment, x_over_x0;
-    if (mat.is_rod != S(0)) {
+    if (W && mat.is_rod != S(0)) {
         path_segment = rod_path(mat.thickness, cos_inc, b.v[0]);
         x_over_x0 = path_segment / mat.X0;
     } else {

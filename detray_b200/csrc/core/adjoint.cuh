@@ -126,8 +126,8 @@ struct no_tape {
 // with respect to the initial free parameters (x, y, z, tx, ty, tz, q/p),
 // from the transport Jacobian accumulated since the start.  Same product as
 // full_jacobian, with B2F replaced by the identity on the free parameters.
-template <typename S>
-DPROP_HD void initial_jacobian(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void initial_jacobian(const detector_view<S, W>& det,
                                const dev_surface& dst_sf,
                                const step_state<S>& st, vec3<S> dtds,
                                S K[5][7]) {
@@ -221,8 +221,8 @@ DPROP_HD S bethe_bloch_dqop(const dev_slab<S>& mat, const rel_quantities<S>& rq,
 // the particle stops (q/p becomes the invalid maximum).  For a material rod
 // around a wire the dependence of the path on the closest approach (loc0)
 // is not included.
-template <typename S>
-DPROP_HD void kick_derivatives(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void kick_derivatives(const detector_view<S, W>& det,
                                const dev_surface& sf, const S* b, S mass, S q,
                                S nav_dir, S& mq, S& mc) {
     mq = S(1);
@@ -242,7 +242,7 @@ DPROP_HD void kick_derivatives(const detector_view<S>& det,
     // path through the material and its derivative by |d.n| (the closest
     // approach of a rod is held fixed)
     S path, dpath_dcos;
-    if (mat.is_rod != S(0)) {
+    if (W && mat.is_rod != S(0)) {
         path = rod_path(mat.thickness, cos_inc, b[0]);
         dpath_dcos = path * cos_inc / (S(1) - cos_inc * cos_inc);
     } else {
@@ -275,8 +275,8 @@ DPROP_HD void kick_derivatives(const detector_view<S>& det,
 // g: dL/db_k^+, down: a_k - g_k (the part that comes from later records).
 // Returns false for surfaces without an alignment model here (cylinders,
 // lines).
-template <typename S>
-DPROP_HD bool alignment_contribution(const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD bool alignment_contribution(const detector_view<S, W>& det,
                                      const dev_surface& sf, const S* b,
                                      vec3<S> dtds, S qop_in, S mc, const S* g,
                                      const S* down, S out[6]) {
@@ -347,8 +347,8 @@ DPROP_HD bool alignment_contribution(const detector_view<S>& det,
 // the direction part is tangent to the unit sphere at dir0 (the propagation
 // treats the input direction as a unit vector).  Align(sf_index, out[6])
 // receives the alignment contributions.
-template <typename S, typename R, typename Align>
-DPROP_HD void backward_track(const detector_view<S>& det,
+template <typename S, bool W, typename R, typename Align>
+DPROP_HD void backward_track(const detector_view<S, W>& det,
                              const tape_view<S>& tp, uint64_t t,
                              uint32_t n_records, const uint64_t* rec_barcode,
                              const uint8_t* rec_flags,

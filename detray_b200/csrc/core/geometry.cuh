@@ -140,8 +140,8 @@ DPROP_HD mask_result<S> check_portal_z(const dev_mask<S>& m, S z, S tol) {
 // cartesian frame of the wire; line<circular>: a straw tube,
 // radius <= r, |z| <= half_z (line.hpp check_boundaries)
 template <typename S>
-DPROP_HD mask_result<S> check_line(const dev_mask<S>& m, vec3<S> l, S tol,
-                                   S edge_tol) {
+DPROP_HD_LINE mask_result<S> check_line(const dev_mask<S>& m, vec3<S> l, S tol,
+                                        S edge_tol) {
     mask_result<S> r;
     r.edge = false;
     if (m.v[2] != S(0)) {
@@ -167,7 +167,8 @@ DPROP_HD mask_result<S> check_line(const dev_mask<S>& m, vec3<S> l, S tol,
 
 // Mask check of a global intersection point, resolving the local frame of
 // the shape (mask::resolve, geometry/mask.hpp).
-template <typename S>
+// W: the detector may hold line surfaces
+template <bool W, typename S>
 DPROP_HD mask_result<S> check_mask(uint8_t shape, const dev_mask<S>& m,
                                    const dev_transform<S>& trf,
                                    const isect_point<S>& ip, S tol,
@@ -190,7 +191,11 @@ DPROP_HD mask_result<S> check_mask(uint8_t shape, const dev_mask<S>& m,
             return check_cylinder_z(m, l.z, tol, edge_tol);
         }
         case e_line:
-            return check_line(m, trf.point_to_local(ip.glob), tol, edge_tol);
+            if (W) {
+                return check_line(m, trf.point_to_local(ip.glob), tol,
+                                  edge_tol);
+            }
+            return {false, false};
         case e_concentric_cylinder:
         default: {
             // the portal intersector only provides the global z
@@ -200,7 +205,7 @@ DPROP_HD mask_result<S> check_mask(uint8_t shape, const dev_mask<S>& m,
 }
 
 // resolve_mask (intersector_base.hpp:167-252) for one mask of a surface
-template <typename S>
+template <bool W, typename S>
 DPROP_HD void resolve_mask(candidate<S>& is, const isect_point<S>& ip,
                            uint32_t sf_idx, const dev_surface& sf,
                            const dev_mask<S>& m, const dev_transform<S>& trf,
@@ -216,7 +221,8 @@ DPROP_HD void resolve_mask(candidate<S>& is, const isect_point<S>& ip,
         base_tol = max_(cfg.min_mask_tol,
                         min_(cfg.max_mask_tol, cfg.mask_tol_scalor * fabs(ip.path)));
     }
-    const mask_result<S> r = check_mask(sf.shape, m, trf, ip, base_tol, ext_tol);
+    const mask_result<S> r =
+        check_mask<W>(sf.shape, m, trf, ip, base_tol, ext_tol);
     if (r.edge) {
         is.status = e_edge;
     }
@@ -361,8 +367,8 @@ DPROP_HD int intersect_cylinder(vec3<S> ro, vec3<S> rd,
 // ray_line_intersector.hpp:58-99.  A ray (almost) parallel to the wire has
 // no intersection.
 template <typename S>
-DPROP_HD isect_point<S> intersect_line(vec3<S> ro, vec3<S> rd,
-                                       const dev_transform<S>& trf) {
+DPROP_HD_LINE isect_point<S> intersect_line(vec3<S> ro, vec3<S> rd,
+                                            const dev_transform<S>& trf) {
     isect_point<S> ip;
     const vec3<S> z = trf.z();
     const S zd = dot(z, rd);
@@ -385,13 +391,17 @@ DPROP_HD isect_point<S> intersect_line(vec3<S> ro, vec3<S> rd,
 // wire, negative when the wire lies on the side of z x dir; loc1 = position
 // along the wire.
 template <typename S>
-DPROP_HD void line_bound_local(const dev_transform<S>& trf, vec3<S> p,
-                               vec3<S> dir, S& l0, S& l1) {
+struct local2 {
+    S l0, l1;
+};
+
+template <typename S>
+DPROP_HD_LINE local2<S> line_bound_local(const dev_transform<S>& trf,
+                                         vec3<S> p, vec3<S> dir) {
     const vec3<S> local3 = trf.point_to_local(p);
     const vec3<S> r = cross(trf.z(), dir);
     const S sign = dot(r, trf.translation() - p) > S(0) ? S(-1) : S(1);
-    l0 = sign * perp(local3);
-    l1 = local3.z;
+    return {sign * perp(local3), local3.z};
 }
 
 // free_to_bound: the two local coordinates of a global point on the surface

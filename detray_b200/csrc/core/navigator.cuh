@@ -208,8 +208,8 @@ DPROP_HD void nav_insert(nav_state<S>& nav, const candidate<S>& nc) {
 
 // -------------------------------------------- intersection_initialize
 // Intersect one surface with the tangential ray and insert the result(s).
-template <typename S>
-DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S, W>& det,
                                uint32_t sf_idx, vec3<S> ro, vec3<S> rd,
                                const isect_cfg<S>& cfg) {
     const dev_surface sf = det.surfaces[sf_idx];
@@ -227,7 +227,7 @@ DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& d
             candidate<S> is = invalid_candidate<S>();
             int n_found = 0;
             for (int i = 0; i < 2; ++i) {
-                resolve_mask(is, ips[i], sf_idx, sf, det.masks[mi], trf, cfg,
+                resolve_mask<W>(is, ips[i], sf_idx, sf, det.masks[mi], trf, cfg,
                              nav.external_tol);
                 if (is.is_probably_inside()) {
                     nav_insert(nav, is);
@@ -244,7 +244,7 @@ DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& d
     if (sf.shape == e_concentric_cylinder) {
         ip = intersect_portal_cylinder(ro, rd, det.masks[m0].v[0],
                                        cfg.overstep_tol);
-    } else if (sf.shape == e_line) {
+    } else if (W && sf.shape == e_line) {
         ip = intersect_line(ro, rd, trf);
     } else {
         ip = intersect_plane(ro, rd, trf);
@@ -254,7 +254,7 @@ DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& d
     }
     for (uint32_t mi = m0; mi < m1; ++mi) {
         candidate<S> is = invalid_candidate<S>();
-        resolve_mask(is, ip, sf_idx, sf, det.masks[mi], trf, cfg,
+        resolve_mask<W>(is, ip, sf_idx, sf, det.masks[mi], trf, cfg,
                      nav.external_tol);
         if (is.is_probably_inside()) {
             nav_insert(nav, is);
@@ -264,8 +264,8 @@ DPROP_HD_LEAF void candidate_search(nav_state<S>& nav, const detector_view<S>& d
 }
 
 // ------------------------------------------------- intersection_update
-template <typename S>
-DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S, W>& det,
                                vec3<S> ro, vec3<S> rd, const isect_cfg<S>& cfg,
                                S external_tol, uint32_t& n_isect) {
     if (c.sf == k_invalid) {
@@ -289,7 +289,7 @@ DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S>& det
         if (sf.shape == e_concentric_cylinder) {
             ip = intersect_portal_cylinder(ro, rd, det.masks[m0].v[0],
                                            cfg.overstep_tol);
-        } else if (sf.shape == e_line) {
+        } else if (W && sf.shape == e_line) {
             ip = intersect_line(ro, rd, trf);
         } else {
             ip = intersect_plane(ro, rd, trf);
@@ -299,7 +299,7 @@ DPROP_HD_LEAF bool update_candidate(candidate<S>& c, const detector_view<S>& det
         }
     }
     for (uint32_t mi = m0; mi < m1; ++mi) {
-        resolve_mask(c, ip, sf_idx, sf, det.masks[mi], trf, cfg, external_tol);
+        resolve_mask<W>(c, ip, sf_idx, sf, det.masks[mi], trf, cfg, external_tol);
         if (c.is_probably_inside()) {
             return true;
         }
@@ -357,8 +357,8 @@ DPROP_HD int wrap_bin(int b, int bins) {
     return (bins + (b % bins)) % bins;
 }
 
-template <typename S>
-DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S, W>& det,
                           const dev_grid<S>& g, const track_view<S>& trk,
                           vec3<S> ro, vec3<S> rd, const nav_cfg<S>& cfg,
                           const isect_cfg<S>& icfg) {
@@ -402,10 +402,18 @@ DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S>& det,
             const int j1 = (g.kind == 1u) ? i1 : wrap_bin(i1, n1);
             const uint32_t b = g.bin_offset + static_cast<uint32_t>(j0) +
                                static_cast<uint32_t>(j1) * g.n0;
-            if (g.multi) {
-                // dynamic bins: [begin, end) of the bin's surfaces
-                const uint32_t e1 = det.grid_bins[b + 1u];
-                for (uint32_t e = det.grid_bins[b]; e < e1; ++e) {
+            if constexpr (W) {
+                // the bin's surfaces as a range of grid_bins: [begin, end)
+                // of a dynamic bin, or the bin's own entry (empty if
+                // invalid); one call site keeps a single inlined copy of the
+                // candidate search
+                uint32_t e0 = b;
+                uint32_t e1 = (det.grid_bins[b] != k_invalid) ? b + 1u : b;
+                if (g.multi) {
+                    e0 = det.grid_bins[b];
+                    e1 = det.grid_bins[b + 1u];
+                }
+                for (uint32_t e = e0; e < e1; ++e) {
                     candidate_search(nav, det, det.grid_bins[e], ro, rd, icfg);
                 }
             } else {
@@ -419,8 +427,8 @@ DPROP_HD void grid_search(nav_state<S>& nav, const detector_view<S>& det,
 }
 
 // --------------------------------------------------- local_navigation
-template <typename S>
-DPROP_HD_COLD void local_navigation(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD_COLD void local_navigation(nav_state<S>& nav, const detector_view<S, W>& det,
                                const track_view<S>& trk, const nav_cfg<S>& cfg,
                                bool resolve_overstepping) {
     const dev_volume vol = det.volumes[nav.volume];
@@ -451,8 +459,8 @@ DPROP_HD_COLD void local_navigation(nav_state<S>& nav, const detector_view<S>& d
 }
 
 // ------------------------------------------------------- volume_switch
-template <typename S>
-DPROP_HD void volume_switch(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void volume_switch(nav_state<S>& nav, const detector_view<S, W>& det,
                             const track_view<S>& trk, const nav_cfg<S>& cfg) {
     if (nav.current().volume_link == k_invalid_link) {
         nav.status = e_nav_exit;
@@ -466,8 +474,8 @@ DPROP_HD void volume_switch(nav_state<S>& nav, const detector_view<S>& det,
 }
 
 // ------------------------------------------------------- init_loose_cfg
-template <typename S>
-DPROP_HD_COLD void init_loose(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD_COLD void init_loose(nav_state<S>& nav, const detector_view<S, W>& det,
                          const track_view<S>& trk, nav_cfg<S> loose) {
     const S a = S(100) * loose.isect.overstep_tol;
     const S b = S(-10) * loose.isect.max_mask_tol;
@@ -479,8 +487,8 @@ DPROP_HD_COLD void init_loose(nav_state<S>& nav, const detector_view<S>& det,
 }
 
 // ------------------------------------------- navigator init / update
-template <typename S>
-DPROP_HD void navigator_init(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD void navigator_init(nav_state<S>& nav, const detector_view<S, W>& det,
                              const track_view<S>& trk, const nav_cfg<S>& cfg) {
     local_navigation(nav, det, trk, cfg, false);
 }
@@ -488,8 +496,8 @@ DPROP_HD void navigator_init(nav_state<S>& nav, const detector_view<S>& det,
 // caching_navigator::update_impl, high-trust branch: re-intersect only the
 // target.  Returns true if the update is complete (update_impl returned
 // there); false if trust dropped to fair and the cache must be re-evaluated.
-template <typename S>
-DPROP_HD bool high_trust_update(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD bool high_trust_update(nav_state<S>& nav, const detector_view<S, W>& det,
                                 const track_view<S>& trk,
                                 const nav_cfg<S>& cfg) {
     const vec3<S> ro = trk.pos;
@@ -516,9 +524,9 @@ DPROP_HD bool high_trust_update(nav_state<S>& nav, const detector_view<S>& det,
 
 // caching_navigator::update_impl, fair- and no-trust branches.  Returns
 // whether the volume was (re-)initialised.
-template <typename S>
+template <typename S, bool W>
 DPROP_HD_COLD bool fair_or_no_trust_update(nav_state<S>& nav,
-                                           const detector_view<S>& det,
+                                           const detector_view<S, W>& det,
                                            const track_view<S>& trk,
                                            const nav_cfg<S>& cfg) {
     const vec3<S> ro = trk.pos;
@@ -568,8 +576,8 @@ DPROP_HD_COLD bool fair_or_no_trust_update(nav_state<S>& nav,
 
 // Volume switch and loose re-initialisation after the trust-level update
 // (navigator_base::update, navigator_base.hpp:121-140).
-template <typename S>
-DPROP_HD_COLD bool finish_update(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD_COLD bool finish_update(nav_state<S>& nav, const detector_view<S, W>& det,
                                  const track_view<S>& trk,
                                  const nav_cfg<S>& cfg, bool is_init) {
     if (nav.is_on_portal()) {
@@ -587,8 +595,8 @@ DPROP_HD_COLD bool finish_update(nav_state<S>& nav, const detector_view<S>& det,
 }
 
 // navigator_base::update
-template <typename S>
-DPROP_HD bool navigator_update(nav_state<S>& nav, const detector_view<S>& det,
+template <typename S, bool W>
+DPROP_HD bool navigator_update(nav_state<S>& nav, const detector_view<S, W>& det,
                                const track_view<S>& trk,
                                const nav_cfg<S>& cfg) {
     if (nav.trust == e_full_trust) {

@@ -25,11 +25,13 @@ struct prop_cfg {
 };
 
 // Where a track writes its records: slot-major arrays, index k * n + t.
+// bound and cov point at the caller's arrays of 6 and 21 component pointers
+// (in a kernel: the launch parameters, so no per-thread copy is made).
 template <typename S>
 struct record_sink {
     uint64_t* barcode;
-    S* bound[6];
-    S* cov[21];
+    S* const* bound;
+    S* const* cov;
     S* path;
     uint8_t* flags;
     uint64_t n_tracks;
@@ -114,9 +116,9 @@ DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
 // adjoint_tape (adjoint mode) the derivative data of each transported record
 // goes to the tape, and the transport Jacobian restarts at the first
 // transported surface as well.
-template <typename S, typename Tape>
+template <typename S, bool W, typename Tape>
 DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
-                                      const detector_view<S>& det,
+                                      const detector_view<S, W>& det,
                                       const field_view<S>& field,
                                       const prop_cfg<S>& cfg,
                                       record_sink<S>& rec, const Tape& tape) {
@@ -222,8 +224,8 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
 }
 
 // Run the actor chain once (propagator.hpp:308).
-template <typename S, typename Tape>
-DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S>& det,
+template <typename S, bool W, typename Tape>
+DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
                          const field_view<S>& field, const prop_cfg<S>& cfg,
                          record_sink<S>& rec, const Tape& tape) {
     step_state<S>& st = ts.step;
@@ -264,9 +266,9 @@ DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
 }
 
 // Propagate one track to the end; returns a dprop_track_status code.
-template <typename S, typename Tape = no_tape>
+template <typename S, bool W, typename Tape = no_tape>
 DPROP_HD uint8_t propagate_track(track_state<S>& ts,
-                                 const detector_view<S>& det,
+                                 const detector_view<S, W>& det,
                                  const field_view<S>& field,
                                  const prop_cfg<S>& cfg, record_sink<S>& rec,
                                  const Tape& tape = Tape{}) {

@@ -115,8 +115,10 @@ struct alignas(16) dev_grid {
     S pad2[3];
 };
 
-// Read-only view handed to the kernels by value.
-template <typename S>
+// Read-only view handed to the kernels by value.  W = false promises that the
+// detector holds no line surfaces, material rods or multi-entry grid bins:
+// the code for them is then left out of the propagation.
+template <typename S, bool W = true>
 struct detector_view {
     const dev_volume* volumes;
     const dev_surface* surfaces;

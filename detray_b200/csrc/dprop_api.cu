@@ -148,11 +148,12 @@ constexpr int k_plain_block = DPROP_BLOCK;
 // thread (the rest spills to L1).  More resident warps hide more of the
 // navigation's memory and instruction-fetch latency; the best budget depends
 // on the workload (constant field vs field map), so it is a launch choice.
-template <typename In, int MinBlocks = DPROP_MIN_BLOCKS>
+template <typename In, int MinBlocks = DPROP_MIN_BLOCKS, bool W = true>
 __global__ void __launch_bounds__(k_plain_block, MinBlocks)
-    propagate_plain_kernel(const detector_view<float> det,
-                           const field_view<float> field,
-                           const prop_cfg<float> cfg, const io_ptrs<In> io,
+    propagate_plain_kernel(const __grid_constant__ detector_view<float, W> det,
+                           const __grid_constant__ field_view<float> field,
+                           const __grid_constant__ prop_cfg<float> cfg,
+                           const __grid_constant__ io_ptrs<In> io,
                            uint64_t n, const uint32_t* __restrict__ order) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) {
@@ -162,11 +163,13 @@ __global__ void __launch_bounds__(k_plain_block, MinBlocks)
     run_one(t, n, det, field, cfg, io);
 }
 
+// Detectors without line surfaces, rods or multi-entry bins only (W = false).
 template <typename In, int MinBlocks = DPROP_MIN_BLOCKS>
 __global__ void __launch_bounds__(k_plain_block, MinBlocks)
-    propagate_persistent_kernel(const detector_view<float> det,
-                                const field_view<float> field,
-                                const prop_cfg<float> cfg, const io_ptrs<In> io,
+    propagate_persistent_kernel(const __grid_constant__ detector_view<float, false> det,
+                                const __grid_constant__ field_view<float> field,
+                                const __grid_constant__ prop_cfg<float> cfg,
+                                const __grid_constant__ io_ptrs<In> io,
                                 uint64_t n, unsigned int* queue,
                                 const uint32_t* __restrict__ order) {
     // each warp pulls the next 32 unprocessed tracks once all of its lanes
@@ -259,18 +262,25 @@ using dprop::api::sort_scratch_bytes;
 
 namespace {
 
+// The plain kernel for a detector: without the wire-surface code unless the
+// detector needs it.
 template <typename In, int MB>
 void launch_plain_mb(unsigned int grid, cudaStream_t st,
-                     const detector_view<float>& det,
+                     const dprop_detector* det,
                      const field_view<float>& field, const prop_cfg<float>& cfg,
                      const io_ptrs<In>& io, uint64_t n, const uint32_t* order) {
-    propagate_plain_kernel<In, MB><<<grid, k_plain_block, 0, st>>>(
-        det, field, cfg, io, n, order);
+    if (det->wires) {
+        propagate_plain_kernel<In, MB, true><<<grid, k_plain_block, 0, st>>>(
+            det->view_as<true>(), field, cfg, io, n, order);
+    } else {
+        propagate_plain_kernel<In, MB, false><<<grid, k_plain_block, 0, st>>>(
+            det->view_as<false>(), field, cfg, io, n, order);
+    }
 }
 
 template <typename In, int MB>
 void launch_persistent_mb(unsigned int grid, cudaStream_t st,
-                          const detector_view<float>& det,
+                          const detector_view<float, false>& det,
                           const field_view<float>& field,
                           const prop_cfg<float>& cfg, const io_ptrs<In>& io,
                           uint64_t n, unsigned int* queue,
@@ -308,8 +318,10 @@ dprop_status enqueue_propagation(const dprop_config& c,
             return s;
         }
     }
-    const detector_view<float> dv = det->view();
-    if (method == DPROP_METHOD_PERSISTENT) {
+    // detectors with wire surfaces run the plain kernel (the queue kernel is
+    // instantiated for the others only)
+    if (method == DPROP_METHOD_PERSISTENT && !det->wires) {
+        const detector_view<float, false> dv = det->view_as<false>();
         if (n > 0xffffff00ull) {
             return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
         }
@@ -332,11 +344,11 @@ dprop_status enqueue_propagation(const dprop_config& c,
         const unsigned int g =
             static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
         if (mb == 8) {
-            launch_plain_mb<In, 8>(g, stream, dv, field->view, cfg, io, n, order);
+            launch_plain_mb<In, 8>(g, stream, det, field->view, cfg, io, n, order);
         } else if (mb == 12) {
-            launch_plain_mb<In, 12>(g, stream, dv, field->view, cfg, io, n, order);
+            launch_plain_mb<In, 12>(g, stream, det, field->view, cfg, io, n, order);
         } else {
-            launch_plain_mb<In, 16>(g, stream, dv, field->view, cfg, io, n, order);
+            launch_plain_mb<In, 16>(g, stream, det, field->view, cfg, io, n, order);
         }
     }
     DPROP_CUDA(cudaGetLastError());
@@ -762,8 +774,8 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         }
         const unsigned int grid =
             static_cast<unsigned int>((m + k_plain_block - 1) / k_plain_block);
-        propagate_plain_kernel<double><<<grid, k_plain_block, 0, st>>>(
-            det->view(), field->view, pcfg, io, m, order);
+        launch_plain_mb<double, DPROP_MIN_BLOCKS>(grid, st, det, field->view,
+                                                  pcfg, io, m, order);
         DPROP_CUDA(cudaGetLastError());
         // pack the records
         const unsigned int cg = static_cast<unsigned int>((m + 1 + 255) / 256);
@@ -890,6 +902,15 @@ dprop_status dprop_detector_create(const dprop_detector_desc* d, int device,
         (st = upload(t.grid_bins, &det->grid_bins)) != DPROP_OK) {
         dprop_detector_destroy(det);
         return st;
+    }
+    for (uint32_t i = 0; i < d->n_surfaces; ++i) {
+        det->wires = det->wires || d->surfaces[i].shape == DPROP_SHAPE_LINE;
+    }
+    for (uint32_t i = 0; i < d->n_slabs; ++i) {
+        det->wires = det->wires || d->slabs[i].kind == DPROP_MATERIAL_ROD;
+    }
+    for (uint32_t i = 0; i < d->n_grids; ++i) {
+        det->wires = det->wires || d->grids[i].multi != 0u;
     }
     const host_tables<double> td = convert_desc<double>(d);
     if ((st = upload(td.masks, &det->masks_d)) != DPROP_OK ||
@@ -1379,8 +1400,8 @@ extern "C" dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
     const prop_cfg<float> pc = make_prop_cfg<float>(*cfg);
     const unsigned int grid =
         static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
-    propagate_plain_kernel<float><<<grid, k_plain_block, 0, stream>>>(
-        det->view(), field->view, pc, io, n, idx_out);
+    launch_plain_mb<float, DPROP_MIN_BLOCKS>(grid, stream, det, field->view, pc,
+                                             io, n, idx_out);
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;
 }

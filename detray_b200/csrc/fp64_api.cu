@@ -25,10 +25,10 @@ constexpr int k_f64_block = 128;
 
 template <int MinBlocks>
 __global__ void __launch_bounds__(k_f64_block, MinBlocks)
-    propagate_fp64_kernel(const detector_view<double> det,
-                          const field_view<double> field,
-                          const prop_cfg<double> cfg,
-                          const api::io_ptrs<double, double> io, uint64_t n,
+    propagate_fp64_kernel(const __grid_constant__ detector_view<double> det,
+                          const __grid_constant__ field_view<double> field,
+                          const __grid_constant__ prop_cfg<double> cfg,
+                          const __grid_constant__ api::io_ptrs<double, double> io, uint64_t n,
                           const uint32_t* __restrict__ order) {
     const uint64_t i =
         static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;

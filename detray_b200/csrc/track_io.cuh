@@ -62,9 +62,9 @@ io_ptrs<In, S> make_io(const dprop_tracks& t, const dprop_results& r) {
 // One track from its inputs to its results, in arithmetic type S.  With
 // Adjoint the propagation also writes the derivative tape of track t
 // (adjoint.cuh).
-template <typename In, bool Adjoint = false, typename S = float>
+template <typename In, bool Adjoint = false, typename S = float, bool W>
 __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
-                                        const detector_view<S>& det,
+                                        const detector_view<S, W>& det,
                                         const field_view<S>& field,
                                         const prop_cfg<S>& cfg,
                                         const io_ptrs<In, S>& io,
@@ -83,12 +83,8 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
 
     record_sink<S> rec;
     rec.barcode = io.rec_barcode;
-    for (int i = 0; i < 6; ++i) {
-        rec.bound[i] = io.rec_bound[i];
-    }
-    for (int i = 0; i < 21; ++i) {
-        rec.cov[i] = io.rec_cov[i];
-    }
+    rec.bound = io.rec_bound;
+    rec.cov = io.rec_cov;
     rec.path = io.rec_path;
     rec.flags = io.rec_flags;
     rec.n_tracks = n;

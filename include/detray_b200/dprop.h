@@ -287,7 +287,9 @@ typedef struct dprop_results {
 typedef enum dprop_method {
     DPROP_METHOD_PLAIN = 0,      /* one thread per track, whole propagation   */
     DPROP_METHOD_PERSISTENT = 1  /* persistent lanes pulling tracks from a
-                                    device work queue                         */
+                                    device work queue (detectors with line
+                                    surfaces, material rods or multi-entry
+                                    grid bins run the plain form)             */
 } dprop_method;
 
 typedef struct dprop_launch {

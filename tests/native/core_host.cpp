@@ -84,14 +84,18 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         std::vector<uint8_t> fl(cap);
         record_sink<S> rec{};
         rec.barcode = bc.data();
+        S* bptr[6];
+        S* cptr[21];
         for (int i = 0; i < 6; ++i) {
             bnd[i].assign(cap, S(0));
-            rec.bound[i] = bnd[i].data();
+            bptr[i] = bnd[i].data();
         }
         for (int i = 0; i < 21; ++i) {
             cv[i].assign(cap, S(0));
-            rec.cov[i] = cv[i].data();
+            cptr[i] = cv[i].data();
         }
+        rec.bound = bptr;
+        rec.cov = cptr;
         rec.path = pth.data();
         rec.flags = fl.data();
         rec.n_tracks = 1u;
