@@ -191,7 +191,8 @@ dprop_status dprop_propagate_adjoint(const dprop_config* cfg,
         const dprop_status s = api::enqueue_direction_sort(
             static_cast<const float*>(tracks->dir[0]),
             static_cast<const float*>(tracks->dir[1]),
-            static_cast<const float*>(tracks->dir[2]), n, g_adj_sort.buf,
+            static_cast<const float*>(tracks->dir[2]),
+            static_cast<const float*>(tracks->qop), n, g_adj_sort.buf,
             g_adj_sort.bytes, st, &order);
         if (s != DPROP_OK) {
             return s;

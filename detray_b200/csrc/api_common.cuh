@@ -24,15 +24,17 @@ int occupancy_of(const dprop_launch* lc);
 // Device scratch bytes of enqueue_direction_sort for n tracks.
 size_t sort_scratch_bytes(uint64_t n);
 
-// Enqueue the direction sort of n tracks (20-bit theta/phi key, CUB radix
-// sort) on stream; *order receives the device array of sorted track
+// Enqueue the sort of n tracks by direction, charge and pT (20-bit key,
+// CUB radix sort) on stream; *order receives the device array of sorted track
 // indices, which lives in scratch.  No allocation, no synchronisation.
 dprop_status enqueue_direction_sort(const float* dx, const float* dy,
-                                    const float* dz, uint64_t n, void* scratch,
+                                    const float* dz, const float* dq,
+                                    uint64_t n, void* scratch,
                                     size_t scratch_bytes, cudaStream_t stream,
                                     const uint32_t** order);
 dprop_status enqueue_direction_sort(const double* dx, const double* dy,
-                                    const double* dz, uint64_t n, void* scratch,
+                                    const double* dz, const double* dq,
+                                    uint64_t n, void* scratch,
                                     size_t scratch_bytes, cudaStream_t stream,
                                     const uint32_t** order);
 

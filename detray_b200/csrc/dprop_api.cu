@@ -104,11 +104,15 @@ struct sort_scratch {
 };
 sort_scratch g_sort;
 
-// Key of the track direction: 10 bits of theta (major) and 10 bits of phi.
+// Sort key of a track, 20 bits: 7 bits of theta (major), 8 bits of phi, the
+// charge sign and 4 bits of log10(pT / GeV) over [-1, 2].  Tracks that share
+// a key cell start in the same direction with similar curvature, so the
+// lanes of a warp cross the same modules at the same loop iterations.
 template <typename In>
 __global__ void direction_key_kernel(const In* __restrict__ dx,
                                      const In* __restrict__ dy,
-                                     const In* __restrict__ dz, uint64_t n,
+                                     const In* __restrict__ dz,
+                                     const In* __restrict__ dq, uint64_t n,
                                      uint32_t* __restrict__ keys,
                                      uint32_t* __restrict__ idx) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -118,13 +122,22 @@ __global__ void direction_key_kernel(const In* __restrict__ dx,
     const float x = static_cast<float>(dx[i]);
     const float y = static_cast<float>(dy[i]);
     const float z = static_cast<float>(dz[i]);
-    const float theta = atan2f(sqrtf(x * x + y * y), z);
+    const float q = static_cast<float>(dq[i]);
+    const float rho = sqrtf(x * x + y * y);
+    const float theta = atan2f(rho, z);
     const float phi = atan2f(y, x);
-    int tb = static_cast<int>(theta * (1024.f / 3.14159265f));
-    int pb = static_cast<int>((phi + 3.14159265f) * (1024.f / 6.2831853f));
-    tb = tb < 0 ? 0 : (tb > 1023 ? 1023 : tb);
-    pb = pb < 0 ? 0 : (pb > 1023 ? 1023 : pb);
-    keys[i] = (static_cast<uint32_t>(tb) << 10) | static_cast<uint32_t>(pb);
+    int tb = static_cast<int>(theta * (128.f / 3.14159265f));
+    int pb = static_cast<int>((phi + 3.14159265f) * (256.f / 6.2831853f));
+    tb = tb < 0 ? 0 : (tb > 127 ? 127 : tb);
+    pb = pb < 0 ? 0 : (pb > 255 ? 255 : pb);
+    // pT = rho / |q/p| (unit direction); non-finite or zero q/p -> top bin
+    const float lpt = log10f(rho / fabsf(q));
+    int kb = static_cast<int>((lpt + 1.f) * (16.f / 3.f));
+    kb = !(lpt == lpt) ? 15 : (kb < 0 ? 0 : (kb > 15 ? 15 : kb));
+    const uint32_t sign = (q < 0.f) ? 1u : 0u;
+    keys[i] = (static_cast<uint32_t>(tb) << 13) |
+              (static_cast<uint32_t>(pb) << 5) | (sign << 4) |
+              static_cast<uint32_t>(kb);
     idx[i] = static_cast<uint32_t>(i);
 }
 
@@ -216,7 +229,7 @@ size_t sort_scratch_bytes(uint64_t n) {
 
 template <typename In>
 dprop_status enqueue_sort(const In* dx, const In* dy, const In* dz,
-                          uint64_t n, void* scratch, size_t scratch_bytes,
+                          const In* dq, uint64_t n, void* scratch, size_t scratch_bytes,
                           cudaStream_t stream, const uint32_t** order) {
     if (n > 0x7fffffffull) {
         return fail(DPROP_E_INVALID, "sort_tracks: too many tracks");
@@ -229,8 +242,8 @@ dprop_status enqueue_sort(const In* dx, const In* dy, const In* dz,
     uint32_t* idx_out = reinterpret_cast<uint32_t*>(p + 3 * arr);
     size_t temp = scratch_bytes - 4 * arr;
     const unsigned int kg = static_cast<unsigned int>((n + 255) / 256);
-    direction_key_kernel<In><<<kg, 256, 0, stream>>>(dx, dy, dz, n, keys_in,
-                                                     idx_in);
+    direction_key_kernel<In><<<kg, 256, 0, stream>>>(dx, dy, dz, dq, n,
+                                                     keys_in, idx_in);
     DPROP_CUDA(cudaGetLastError());
     DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
         p + 4 * arr, temp, keys_in, keys_out, idx_in, idx_out,
@@ -240,19 +253,21 @@ dprop_status enqueue_sort(const In* dx, const In* dy, const In* dz,
 }
 
 dprop_status enqueue_direction_sort(const float* dx, const float* dy,
-                                    const float* dz, uint64_t n, void* scratch,
+                                    const float* dz, const float* dq,
+                                    uint64_t n, void* scratch,
                                     size_t scratch_bytes, cudaStream_t stream,
                                     const uint32_t** order) {
-    return enqueue_sort<float>(dx, dy, dz, n, scratch, scratch_bytes, stream,
-                               order);
+    return enqueue_sort<float>(dx, dy, dz, dq, n, scratch, scratch_bytes,
+                               stream, order);
 }
 
 dprop_status enqueue_direction_sort(const double* dx, const double* dy,
-                                    const double* dz, uint64_t n, void* scratch,
+                                    const double* dz, const double* dq,
+                                    uint64_t n, void* scratch,
                                     size_t scratch_bytes, cudaStream_t stream,
                                     const uint32_t** order) {
-    return enqueue_sort<double>(dx, dy, dz, n, scratch, scratch_bytes, stream,
-                                order);
+    return enqueue_sort<double>(dx, dy, dz, dq, n, scratch, scratch_bytes,
+                                stream, order);
 }
 
 }  // namespace dprop::api
@@ -312,7 +327,8 @@ dprop_status enqueue_propagation(const dprop_config& c,
     const uint32_t* order = nullptr;
     if (launch_cfg && launch_cfg->sort_tracks) {
         const dprop_status s = dprop::api::enqueue_sort<In>(
-            io.trk[4], io.trk[5], io.trk[6], n, scr.sort, scr.sort_bytes,
+            io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, scr.sort,
+            scr.sort_bytes,
             stream, &order);
         if (s != DPROP_OK) {
             return s;
@@ -765,7 +781,7 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         if (sort) {
             const unsigned int kg = static_cast<unsigned int>((m + 255) / 256);
             direction_key_kernel<double><<<kg, 256, 0, st>>>(
-                d_trk[4], d_trk[5], d_trk[6], m, keys_in, idx_in);
+                d_trk[4], d_trk[5], d_trk[6], d_trk[7], m, keys_in, idx_in);
             size_t tb = sort_temp;
             DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
                 sort_tmp, tb, keys_in, keys_out, idx_in, idx_out,
@@ -1392,7 +1408,7 @@ extern "C" dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
     const io_ptrs<float> io = make_io<float>(*tracks, *results);
     const unsigned int key_grid = static_cast<unsigned int>((n + 255) / 256);
     direction_key_kernel<float><<<key_grid, 256, 0, stream>>>(
-        io.trk[4], io.trk[5], io.trk[6], n, keys_in, idx_in);
+        io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, keys_in, idx_in);
     DPROP_CUDA(cudaGetLastError());
     DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in,
                                                keys_out, idx_in, idx_out, ni,

@@ -79,7 +79,7 @@ dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
             g_f64_sort.device = dev;
         }
         const dprop_status s = enqueue_direction_sort(
-            io.trk[4], io.trk[5], io.trk[6], n, g_f64_sort.buf,
+            io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, g_f64_sort.buf,
             g_f64_sort.bytes, stream, &order);
         if (s != DPROP_OK) {
             return s;
