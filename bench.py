@@ -559,6 +559,7 @@ def run_reference(args):
                              abort_reasons=False)
     dt = (time.perf_counter() - t0) / args.steps
     value = n / dt
+    gpu = reference_gpu_row(args, cfg)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -572,8 +573,39 @@ def run_reference(args):
                          "sample": f"{n} tracks per step of the same workload"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_row(args, cfg):
+    """The reference's own CUDA propagation kernel (its benchmark's
+    propagator_benchmark_kernel with the default actor chain, rebuilt for
+    sm_100a from its headers) timed with CUDA events on the same workload
+    and tracks as our arm, device-resident inputs: the GPU "plain form"."""
+    from oracle import ref_oracle
+    from detray_b200.units import T
+    try:
+        import torch
+        if not (ref_oracle.gpu_available() and torch.cuda.is_available()):
+            return None
+        trk = make_tracks(args.tracks, args.seed)
+        # the reference benchmark's input order: by |pi/2 - theta|
+        # (tests/benchmarks/include/detray/benchmarks/benchmark_utils.hpp)
+        theta = np.arccos(np.clip(trk[6], -1.0, 1.0))
+        trk = trk[:, np.argsort(np.abs(0.5 * np.pi - theta), kind="stable")]
+        r = ref_oracle.gpu_toy_bench(cfg, 2.0 * T, trk,
+                                     warmup=args.warmup, steps=args.steps)
+    except (RuntimeError, OSError) as exc:
+        return {"unavailable": str(exc)}
+    return {"value": args.tracks / (r["ms_per_step"] / 1e3), "unit": UNIT,
+            "ms_per_step": round(r["ms_per_step"], 3),
+            "tracks": args.tracks, "n_exited": r["n_exited"],
+            "kernel": "reference propagator_benchmark_kernel (default "
+                      "actor chain: parameter_updater with material "
+                      "interactor), 256 threads, sm_100a, tracks ordered by "
+                      "|pi/2 - theta| as in the reference benchmark, no "
+                      "records written"}
 
 
 def main():

@@ -3,6 +3,14 @@
 #include <cstddef>
 #include <type_traits>
 
+// Device annotations for the CUDA build of the reference's propagator (the
+// GPU baseline); empty for the host compilers.
+#if defined(__CUDACC__)
+#define VECMEM_HOST_AND_DEVICE __host__ __device__
+#else
+#define VECMEM_HOST_AND_DEVICE
+#endif
+
 namespace vecmem::data {
 template <typename T>
 class vector_view {
@@ -11,15 +19,15 @@ class vector_view {
     using pointer = T*;
     using value_type = T;
     vector_view() = default;
-    vector_view(size_type n, pointer p) : m_size(n), m_capacity(n), m_ptr(p) {}
+    VECMEM_HOST_AND_DEVICE vector_view(size_type n, pointer p) : m_size(n), m_capacity(n), m_ptr(p) {}
     template <typename U,
               std::enable_if_t<std::is_convertible_v<U*, T*>, bool> = true>
-    vector_view(const vector_view<U>& o)
+    VECMEM_HOST_AND_DEVICE vector_view(const vector_view<U>& o)
         : m_size(o.size()), m_capacity(o.capacity()), m_ptr(o.ptr()) {}
-    size_type size() const { return m_size; }
-    size_type capacity() const { return m_capacity; }
-    pointer ptr() const { return m_ptr; }
-    size_type* size_ptr() const { return nullptr; }
+    VECMEM_HOST_AND_DEVICE size_type size() const { return m_size; }
+    VECMEM_HOST_AND_DEVICE size_type capacity() const { return m_capacity; }
+    VECMEM_HOST_AND_DEVICE pointer ptr() const { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE size_type* size_ptr() const { return nullptr; }
 
    private:
     size_type m_size{0};
@@ -34,16 +42,16 @@ class jagged_vector_view {
     using value_type = vector_view<T>;
     using pointer = value_type*;
     jagged_vector_view() = default;
-    jagged_vector_view(size_type n, pointer p) : m_size(n), m_ptr(p) {}
+    VECMEM_HOST_AND_DEVICE jagged_vector_view(size_type n, pointer p) : m_size(n), m_ptr(p) {}
     template <typename U,
               std::enable_if_t<std::is_convertible_v<U*, T*>, bool> = true>
-    jagged_vector_view(const jagged_vector_view<U>& o)
+    VECMEM_HOST_AND_DEVICE jagged_vector_view(const jagged_vector_view<U>& o)
         : m_size(o.size()),
           m_ptr(reinterpret_cast<pointer>(o.ptr())) {}
-    size_type size() const { return m_size; }
-    size_type capacity() const { return m_size; }
-    pointer ptr() const { return m_ptr; }
-    pointer host_ptr() const { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE size_type size() const { return m_size; }
+    VECMEM_HOST_AND_DEVICE size_type capacity() const { return m_size; }
+    VECMEM_HOST_AND_DEVICE pointer ptr() const { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE pointer host_ptr() const { return m_ptr; }
 
    private:
     size_type m_size{0};

@@ -16,34 +16,34 @@ class device_vector {
     using iterator = T*;
     using const_iterator = const T*;
     device_vector() = default;
-    explicit device_vector(const data::vector_view<T>& v)
+    VECMEM_HOST_AND_DEVICE explicit device_vector(const data::vector_view<T>& v)
         : m_ptr(v.ptr()), m_size(v.size()), m_capacity(v.capacity()) {}
-    reference operator[](size_type i) { return m_ptr[i]; }
-    const_reference operator[](size_type i) const { return m_ptr[i]; }
-    reference at(size_type i) { return m_ptr[i]; }
-    const_reference at(size_type i) const { return m_ptr[i]; }
-    size_type size() const { return m_size; }
-    size_type capacity() const { return m_capacity; }
-    bool empty() const { return m_size == 0; }
-    iterator begin() { return m_ptr; }
-    iterator end() { return m_ptr + m_size; }
-    const_iterator begin() const { return m_ptr; }
-    const_iterator end() const { return m_ptr + m_size; }
-    pointer data() { return m_ptr; }
-    const_pointer data() const { return m_ptr; }
-    reference front() { return m_ptr[0]; }
-    reference back() { return m_ptr[m_size - 1]; }
-    void push_back(const T& v) {
+    VECMEM_HOST_AND_DEVICE reference operator[](size_type i) { return m_ptr[i]; }
+    VECMEM_HOST_AND_DEVICE const_reference operator[](size_type i) const { return m_ptr[i]; }
+    VECMEM_HOST_AND_DEVICE reference at(size_type i) { return m_ptr[i]; }
+    VECMEM_HOST_AND_DEVICE const_reference at(size_type i) const { return m_ptr[i]; }
+    VECMEM_HOST_AND_DEVICE size_type size() const { return m_size; }
+    VECMEM_HOST_AND_DEVICE size_type capacity() const { return m_capacity; }
+    VECMEM_HOST_AND_DEVICE bool empty() const { return m_size == 0; }
+    VECMEM_HOST_AND_DEVICE iterator begin() { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE iterator end() { return m_ptr + m_size; }
+    VECMEM_HOST_AND_DEVICE const_iterator begin() const { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE const_iterator end() const { return m_ptr + m_size; }
+    VECMEM_HOST_AND_DEVICE pointer data() { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE const_pointer data() const { return m_ptr; }
+    VECMEM_HOST_AND_DEVICE reference front() { return m_ptr[0]; }
+    VECMEM_HOST_AND_DEVICE reference back() { return m_ptr[m_size - 1]; }
+    VECMEM_HOST_AND_DEVICE void push_back(const T& v) {
         assert(m_size < m_capacity);
         m_ptr[m_size++] = v;
     }
-    size_type push_back_default() { return m_size++; }
-    void clear() { m_size = 0; }
-    void resize(size_type n) { m_size = n; }
+    VECMEM_HOST_AND_DEVICE size_type push_back_default() { return m_size++; }
+    VECMEM_HOST_AND_DEVICE void clear() { m_size = 0; }
+    VECMEM_HOST_AND_DEVICE void resize(size_type n) { m_size = n; }
 
    private:
     pointer m_ptr{nullptr};
-    size_type m_size{0};
-    size_type m_capacity{0};
+    VECMEM_HOST_AND_DEVICE size_type m_size{0};
+    VECMEM_HOST_AND_DEVICE size_type m_capacity{0};
 };
 }  // namespace vecmem

@@ -340,3 +340,31 @@ def bethe(name: str, pdg: int, p: float, precision="f64"):
     dv = C.c_double()
     _check(lib, lib.ref_bethe(name.encode(), pdg, p, C.byref(v), C.byref(dv)))
     return v.value, dv.value
+
+
+def gpu_available() -> bool:
+    """The reference's CUDA propagation kernel, built for sm_100a."""
+    return (REF_DIR / "libdetray_ref_gpu.so").exists()
+
+
+def gpu_toy_bench(cfg: abi.Config, bz: float, tracks: np.ndarray,
+                  warmup: int = 3, steps: int = 10) -> dict:
+    """Time the reference's own CUDA propagation kernel
+    (propagator_benchmark_kernel of its CUDA benchmark, rebuilt for sm_100a;
+    oracle/ref/ref_gpu*.{cu,cpp}) on ``tracks`` through the toy detector in
+    a constant field bz along z.  Returns ms per launch and the number of
+    tracks whose propagate() returned true."""
+    lib = C.CDLL(str(REF_DIR / "libdetray_ref_gpu.so"))
+    lib.refgpu_last_error.restype = C.c_char_p
+    lib.refgpu_toy_bench.argtypes = [
+        C.POINTER(abi.Config), C.c_double, C.POINTER(C.c_void_p), C.c_uint64,
+        C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+    trk = np.ascontiguousarray(tracks, dtype=np.float64)
+    ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    ms = C.c_double()
+    ok = C.c_uint64()
+    rc = lib.refgpu_toy_bench(C.byref(cfg), bz, ptrs, trk.shape[1], warmup,
+                              steps, C.byref(ms), C.byref(ok))
+    if rc != 0:
+        raise RuntimeError(lib.refgpu_last_error().decode())
+    return {"ms_per_step": ms.value, "n_exited": int(ok.value)}
