@@ -45,10 +45,17 @@ SF_PORTAL = 0
 SF_SENSITIVE = 1
 SF_PASSIVE = 2
 
+# dprop_material_kind
+MATERIAL_SLAB = 0
+MATERIAL_ROD = 1
+
 # dprop_grid_kind
 GRID_NONE = 0
 GRID_CYLINDER = 1
 GRID_DISC = 2
+GRID_MATERIAL_CYLINDER = 3
+GRID_MATERIAL_DISC = 4
+GRID_MATERIAL_CARTESIAN = 5
 
 # dprop_method
 METHOD_PLAIN = 0
@@ -70,7 +77,8 @@ class SurfaceDesc(C.Structure):
         ("volume", C.c_uint32),
         ("shape", C.c_uint8),
         ("kind", C.c_uint8),
-        ("pad", C.c_uint8 * 2),
+        ("material_kind", C.c_uint8),
+        ("pad", C.c_uint8),
     ]
 
 

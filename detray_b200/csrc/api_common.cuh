@@ -64,8 +64,9 @@ struct dprop_detector {
     dprop::dev_slab<double>* slabs_d{nullptr};
     dprop::dev_grid<double>* grids_d{nullptr};
     uint32_t n_volumes{0}, n_surfaces{0};
-    // the detector holds line surfaces, material rods or multi-entry grid
-    // bins: launches use the kernels that include the code for them
+    // the detector holds line surfaces, material rods, multi-entry grid bins
+    // or material maps: launches use the kernels that include the code for
+    // them
     bool wires{false};
     dprop::detector_view<double> view_d() const {
         dprop::detector_view<double> v;

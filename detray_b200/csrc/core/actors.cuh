@@ -527,6 +527,38 @@ DPROP_HD_LINE S rod_path(S r, S cos_inc, S d) {
     return S(2) * sqrt((r * r - d * d) / sin_inc_2);
 }
 
+// The material slab a track at bound local (l0, l1) sees on a surface:
+// its homogeneous slab or rod, or the bin of its material map that holds the
+// local position (material_accessor::get, material/detail/
+// material_accessor.hpp; axis binning of utils/grid/detail/axis_binning.hpp
+// and the closed / circular bounds of axis_bounds.hpp)
+template <typename S, bool W>
+DPROP_HD dev_slab<S> surface_material(const detector_view<S, W>& det,
+                                      const dev_surface& sf, S l0, S l1) {
+    if (W && sf.material_map) {
+        const dev_grid<S> g = det.grids[sf.material];
+        const int n0 = static_cast<int>(g.n0);
+        const int n1 = static_cast<int>(g.n1);
+        int b0 = axis_bin(l0, g.min0, g.max0, g.n0);
+        int b1 = axis_bin(l1, g.min1, g.max1, g.n1);
+        // circular axes wrap, closed axes clamp (axis_bounds.hpp)
+        if (g.kind == 3u) {  // (r*phi circular, z closed)
+            b0 = wrap_bin(b0, n0);
+        } else {
+            b0 = b0 <= 0 ? 0 : (b0 >= n0 ? n0 - 1 : b0);
+        }
+        if (g.kind == 4u) {  // (r closed, phi circular)
+            b1 = wrap_bin(b1, n1);
+        } else {
+            b1 = b1 <= 0 ? 0 : (b1 >= n1 ? n1 - 1 : b1);
+        }
+        const uint32_t slab = det.grid_bins[g.bin_offset + static_cast<uint32_t>(b0) +
+                                            static_cast<uint32_t>(b1) * g.n0];
+        return det.slabs[slab];
+    }
+    return det.slabs[sf.material];
+}
+
 // pointwise_material_interactor::update on the bound state
 template <typename S, bool W>
 DPROP_HD bool interact(const detector_view<S, W>& det, const dev_surface& sf,
@@ -535,7 +567,7 @@ DPROP_HD bool interact(const detector_view<S, W>& det, const dev_surface& sf,
     if (sf.material == k_invalid) {
         return false;
     }
-    const dev_slab<S> mat = det.slabs[sf.material];
+    const dev_slab<S> mat = surface_material(det, sf, b.v[0], b.v[1]);
     const vec3<S> dir = bound_dir(b.v[2], b.v[3]);
     const vec3<S> n = surface_normal_at_bound(det, sf, b.v[0]);
     const S cos_inc = fabs(dot(dir, n));

@@ -230,7 +230,7 @@ DPROP_HD void kick_derivatives(const detector_view<S, W>& det,
     if (sf.material == k_invalid) {
         return;
     }
-    const dev_slab<S> mat = det.slabs[sf.material];
+    const dev_slab<S> mat = surface_material(det, sf, b[0], b[1]);
     const S qop = b[4];
     if (mat.thickness <= limits<S>::epsilon() || qop == S(0)) {
         return;

@@ -64,7 +64,13 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
             s.mask_end - s.mask_begin > 0xffffu ||
             s.transform >= d->n_transforms || s.volume >= d->n_volumes ||
             s.shape >= DPROP_SHAPE_COUNT || s.kind > DPROP_SF_PASSIVE ||
-            (s.material != DPROP_INVALID_INDEX && s.material >= d->n_slabs)) {
+            s.material_kind > 1u ||
+            (s.material != DPROP_INVALID_INDEX && s.material_kind == 0u &&
+             s.material >= d->n_slabs) ||
+            (s.material != DPROP_INVALID_INDEX && s.material_kind == 1u &&
+             (s.material >= d->n_grids ||
+              (d->grids[s.material].kind < DPROP_GRID_MATERIAL_CYLINDER ||
+               d->grids[s.material].kind > DPROP_GRID_MATERIAL_CARTESIAN)))) {
             return "surface " + std::to_string(i) + " has an out-of-range index";
         }
     }
@@ -78,7 +84,10 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
         const dprop_volume_desc& v = d->volumes[i];
         if (v.transform >= d->n_transforms || v.bf_begin > v.bf_end ||
             v.bf_end > d->n_bf_surfaces ||
-            (v.grid != DPROP_INVALID_INDEX && v.grid >= d->n_grids)) {
+            (v.grid != DPROP_INVALID_INDEX &&
+             (v.grid >= d->n_grids ||
+              (d->grids[v.grid].kind != DPROP_GRID_CYLINDER &&
+               d->grids[v.grid].kind != DPROP_GRID_DISC)))) {
             return "volume " + std::to_string(i) + " has an out-of-range index";
         }
     }
@@ -92,19 +101,35 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
             return "material " + std::to_string(i) + " has an unknown kind";
         }
     }
-    // grid_bins entries that are bin ranges of multi-entry grids (the rest
-    // are surface indices)
+    // grid_bins entries that are bin ranges of multi-entry grids or slab
+    // indices of material maps (the rest are surface indices)
     std::vector<bool> is_range(d->n_grid_bins, false);
     for (uint32_t i = 0; i < d->n_grids; ++i) {
         const dprop_grid_desc& g = d->grids[i];
         const uint64_t nb = static_cast<uint64_t>(g.n_bins[0]) * g.n_bins[1];
         const uint64_t n_entries = nb + (g.multi ? 1u : 0u);
-        if ((g.kind != DPROP_GRID_CYLINDER && g.kind != DPROP_GRID_DISC) ||
+        const bool material_map = g.kind >= DPROP_GRID_MATERIAL_CYLINDER &&
+                                  g.kind <= DPROP_GRID_MATERIAL_CARTESIAN;
+        if ((g.kind != DPROP_GRID_CYLINDER && g.kind != DPROP_GRID_DISC &&
+             !material_map) ||
             g.n_bins[0] == 0 || g.n_bins[1] == 0 || g.multi > 1u ||
+            (material_map && g.multi != 0u) ||
             static_cast<uint64_t>(g.bin_offset) + n_entries > d->n_grid_bins ||
             g.transform >= d->n_transforms ||
             !(g.axis_max[0] > g.axis_min[0]) || !(g.axis_max[1] > g.axis_min[1])) {
             return "grid " + std::to_string(i) + " is inconsistent";
+        }
+        if (material_map) {
+            // bins hold slab indices
+            for (uint64_t b = 0; b < nb; ++b) {
+                const uint64_t e = g.bin_offset + b;
+                is_range[e] = true;
+                if (d->grid_bins[e] >= d->n_slabs ||
+                    d->slabs[d->grid_bins[e]].kind != DPROP_MATERIAL_SLAB) {
+                    return "material map " + std::to_string(i) +
+                           " has a bin without a slab";
+                }
+            }
         }
         if (g.multi) {
             for (uint64_t b = 0; b < n_entries; ++b) {
@@ -166,6 +191,7 @@ host_tables<S> convert_desc(const dprop_detector_desc* d) {
         o.shape = s.shape;
         o.kind = s.kind;
         o.volume = s.volume;
+        o.material_map = s.material_kind;
         t.surfaces[i] = o;
     }
     t.masks.resize(d->n_masks);

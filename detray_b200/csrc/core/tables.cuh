@@ -37,7 +37,7 @@ struct alignas(16) dev_surface {
     uint8_t shape;
     uint8_t kind;
     uint32_t volume;
-    uint32_t pad;
+    uint32_t material_map;  // 1: material indexes a material-map grid
 };
 
 // 32 bytes (fp32) / 64 bytes (fp64): bounds + next-volume link.
@@ -104,7 +104,8 @@ struct alignas(16) dev_volume {
 
 template <typename S>
 struct alignas(16) dev_grid {
-    uint32_t kind;  // 1 cylinder (phi, z), 2 disc (r, phi)
+    uint32_t kind;  // 1 cylinder (phi, z), 2 disc (r, phi); material maps:
+                    // 3 cylinder (phi, z), 4 disc (r, phi)
     uint32_t n0, n1;
     uint32_t bin_offset;
     uint32_t transform;
@@ -116,8 +117,8 @@ struct alignas(16) dev_grid {
 };
 
 // Read-only view handed to the kernels by value.  W = false promises that the
-// detector holds no line surfaces, material rods or multi-entry grid bins:
-// the code for them is then left out of the propagation.
+// detector holds no line surfaces, material rods, multi-entry grid bins or
+// material maps: the code for them is then left out of the propagation.
 template <typename S, bool W = true>
 struct detector_view {
     const dev_volume* volumes;

@@ -920,7 +920,8 @@ dprop_status dprop_detector_create(const dprop_detector_desc* d, int device,
         return st;
     }
     for (uint32_t i = 0; i < d->n_surfaces; ++i) {
-        det->wires = det->wires || d->surfaces[i].shape == DPROP_SHAPE_LINE;
+        det->wires = det->wires || d->surfaces[i].shape == DPROP_SHAPE_LINE ||
+                     d->surfaces[i].material_kind != 0u;
     }
     for (uint32_t i = 0; i < d->n_slabs; ++i) {
         det->wires = det->wires || d->slabs[i].kind == DPROP_MATERIAL_ROD;

@@ -31,47 +31,6 @@ using namespace detray;
 using algebra_t = detray::array<double>;
 using scalar = double;
 
-namespace {
-
-template <typename T>
-void write_vec(std::FILE* f, const std::vector<T>& v) {
-    if (!v.empty()) {
-        std::fwrite(v.data(), sizeof(T), v.size(), f);
-    }
-}
-
-int write_tables(const dprop::flat_detector& t, const char* path) {
-    std::FILE* f = std::fopen(path, "wb");
-    if (!f) {
-        std::perror(path);
-        return 1;
-    }
-    const uint32_t header[12] = {0x4f454744u,  // "DGEO"
-                                 DPROP_ABI_VERSION,
-                                 static_cast<uint32_t>(t.volumes.size()),
-                                 static_cast<uint32_t>(t.surfaces.size()),
-                                 static_cast<uint32_t>(t.masks.size()),
-                                 static_cast<uint32_t>(t.transforms.size()),
-                                 static_cast<uint32_t>(t.slabs.size()),
-                                 static_cast<uint32_t>(t.bf_surfaces.size()),
-                                 static_cast<uint32_t>(t.grids.size()),
-                                 static_cast<uint32_t>(t.grid_bins.size()),
-                                 0u,
-                                 0u};
-    std::fwrite(header, sizeof(uint32_t), 12, f);
-    write_vec(f, t.volumes);
-    write_vec(f, t.surfaces);
-    write_vec(f, t.masks);
-    write_vec(f, t.transforms);
-    write_vec(f, t.slabs);
-    write_vec(f, t.bf_surfaces);
-    write_vec(f, t.grids);
-    write_vec(f, t.grid_bins);
-    std::fclose(f);
-    return 0;
-}
-
-}  // namespace
 
 int main(int argc, char** argv) {
     if (argc < 2) {
@@ -80,14 +39,16 @@ int main(int argc, char** argv) {
     }
     vecmem::host_memory_resource mr;
     const std::string kind = argv[1];
-    if (kind == "toy" && argc == 6) {
+    if (kind == "toy" && (argc == 6 || argc == 7)) {
+        // a 7th argument "maps": material maps on the portals
+        const bool maps = argc == 7 && std::string(argv[6]) == "maps";
         toy_det_config<scalar> cfg{};
         cfg.n_brl_layers(static_cast<unsigned int>(std::atoi(argv[2])))
             .n_edc_layers(static_cast<unsigned int>(std::atoi(argv[3])))
-            .use_material_maps(false)
+            .use_material_maps(maps)
             .module_mat_thickness(std::atof(argv[4]));
         auto [det, names] = build_toy_detector<algebra_t>(mr, cfg);
-        return write_tables(dprop::flatten(det), argv[5]);
+        return dprop::write_raw_tables(dprop::flatten(det), argv[5]);
     }
     if (kind == "telescope" && argc >= 7) {
         std::vector<scalar> pos;
@@ -99,7 +60,7 @@ int main(int argc, char** argv) {
         detail::ray<algebra_t> pilot{{0., 0., 0.}, 0., {1., 0., 0.}, -1.};
         cfg.positions(pos).pilot_track(pilot).mat_thickness(std::atof(argv[4]));
         auto [det, names] = build_telescope_detector<algebra_t, rectangle2D>(mr, cfg);
-        return write_tables(dprop::flatten(det), argv[5]);
+        return dprop::write_raw_tables(dprop::flatten(det), argv[5]);
     }
     if (kind == "wire" && argc == 6) {
         // 500 mm first layer radius, 1 m half length, 10 mm cells, 50 mrad
@@ -110,7 +71,7 @@ int main(int argc, char** argv) {
                 .mat_radius(std::atof(argv[4]))
                 .do_check(false);
             auto [det, names] = build_wire_chamber<algebra_t>(mr, cfg);
-            return write_tables(dprop::flatten(det), argv[5]);
+            return dprop::write_raw_tables(dprop::flatten(det), argv[5]);
         };
         return std::atoi(argv[3]) ? build(line_square{}) : build(line_circular{});
     }

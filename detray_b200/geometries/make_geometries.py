@@ -6,6 +6,9 @@ of the benchmark detectors into compressed .npz files next to this script:
 
   toy_4brl_7edc.npz          toy barrel + endcap detector, 4 barrel layers,
                              7 endcap discs per side, 0.15 mm Si modules
+  toy_4brl_7edc_maps.npz     the same with the builder's material maps on
+                             the portals (20 x 20 bins on cylinders, 5 x 20
+                             on discs)
   telescope_10x1m_300um.npz  10 1 m x 1 m Si planes normal to x at
                              x = 0, 50, ..., 450 mm, 0.3 mm thick
   wire_chamber_10l_cells.npz wire chamber: 10 layers of 10 mm square drift
@@ -29,6 +32,7 @@ from detray_b200 import geometry  # noqa: E402
 
 GEOMETRIES = {
     "toy_4brl_7edc": ["toy", "4", "7", "0.15"],
+    "toy_4brl_7edc_maps": ["toy", "4", "7", "0.15", "maps"],
     "telescope_10x1m_300um": ["telescope", "500", "500", "0.3"],
     "wire_chamber_10l_cells": ["wire", "10", "1", "0.015"],
     "wire_chamber_10l_straws": ["wire", "10", "0", "0.015"],
@@ -54,7 +58,7 @@ def main() -> None:
         build_exporter(ref, exe)
         for name, args in GEOMETRIES.items():
             raw = Path(tmp) / f"{name}.bin"
-            extra = TELESCOPE_POSITIONS if args[0] == "telescope" else []
+            extra = TELESCOPE_POSITIONS if args[0] == "telescope" else args[4:]
             subprocess.run([str(exe), *args[:4], str(raw), *extra], check=True)
             tables = geometry.read_raw_tables(raw)
             geometry.save_npz(tables, HERE / f"{name}.npz")

@@ -19,6 +19,7 @@
 #include "detray_b200/dprop.h"
 
 #include <cstdint>
+#include <cstdio>
 #include <algorithm>
 #include <stdexcept>
 #include <string>
@@ -180,7 +181,7 @@ dprop_slab_desc to_rod_desc(const rod_t& rod) {
     return d;
 }
 
-/// Material-store visitor: homogeneous slabs and rods.
+/// Material-store visitor: homogeneous slabs, rods and 2D material maps.
 struct slab_copier {
     template <typename mat_group_t, typename index_t>
     void operator()(const mat_group_t& group, const index_t& idx,
@@ -200,10 +201,62 @@ struct slab_copier {
             const dprop_slab_desc d = to_rod_desc(group[idx]);
             sf.material = static_cast<uint32_t>(out.slabs.size());
             out.slabs.push_back(d);
+        } else if constexpr (detray::concepts::material_map<mat_t>) {
+            // 2D material map (material/material_map.hpp): one slab per bin
+            if constexpr (mat_t::dim != 2) {
+                throw std::runtime_error(
+                    "dprop::flatten: volume material maps are not supported "
+                    "on the device path");
+            }
+            const auto g = group[idx];
+            using frame_t = typename mat_t::local_frame_type;
+            using algebra_t = typename frame_t::algebra_type;
+            dprop_grid_desc gd{};
+            if constexpr (std::is_same_v<frame_t,
+                                         detray::concentric_cylindrical2D<
+                                             algebra_t>> ||
+                          std::is_same_v<frame_t,
+                                         detray::cylindrical2D<algebra_t>>) {
+                gd.kind = DPROP_GRID_MATERIAL_CYLINDER;
+            } else if constexpr (std::is_same_v<frame_t,
+                                                detray::polar2D<algebra_t>>) {
+                gd.kind = DPROP_GRID_MATERIAL_DISC;
+            } else if constexpr (std::is_same_v<frame_t,
+                                                detray::cartesian2D<algebra_t>>) {
+                gd.kind = DPROP_GRID_MATERIAL_CARTESIAN;
+            } else {
+                throw std::runtime_error(
+                    "dprop::flatten: unsupported material map frame");
+            }
+            const auto ax0 = g.template get_axis<0>();
+            const auto ax1 = g.template get_axis<1>();
+            gd.n_bins[0] = static_cast<uint32_t>(ax0.nbins());
+            gd.n_bins[1] = static_cast<uint32_t>(ax1.nbins());
+            gd.axis_min[0] = static_cast<double>(ax0.span()[0]);
+            gd.axis_max[0] = static_cast<double>(ax0.span()[1]);
+            gd.axis_min[1] = static_cast<double>(ax1.span()[0]);
+            gd.axis_max[1] = static_cast<double>(ax1.span()[1]);
+            gd.transform = sf.transform;
+            gd.bin_offset = static_cast<uint32_t>(out.grid_bins.size());
+            const std::size_t nb =
+                static_cast<std::size_t>(gd.n_bins[0]) * gd.n_bins[1];
+            for (std::size_t b = 0; b < nb; ++b) {
+                // a bin without an entry holds the empty (zero thickness)
+                // slab, which the interactor skips
+                dprop_slab_desc d{};
+                for (const auto& slab : g.bin(static_cast<detray::dindex>(b))) {
+                    d = to_slab_desc(slab);
+                }
+                out.grid_bins.push_back(static_cast<uint32_t>(out.slabs.size()));
+                out.slabs.push_back(d);
+            }
+            sf.material = static_cast<uint32_t>(out.grids.size());
+            sf.material_kind = 1u;
+            out.grids.push_back(gd);
         } else {
             throw std::runtime_error(
-                "dprop::flatten: only homogeneous material slabs are "
-                "supported on the device path");
+                "dprop::flatten: only homogeneous material slabs, rods and 2D "
+                "material maps are supported on the device path");
         }
     }
 };
@@ -318,6 +371,46 @@ dprop_transform_desc copy_transform(const transform_t& trf) {
 }
 
 }  // namespace adapter_detail
+
+/// Write the flat tables to a raw table file: a 12-word u32 header ("DGEO",
+/// DPROP_ABI_VERSION, the eight table lengths, two zero words) followed by
+/// the tables in declaration order of dprop_detector_desc.  Returns 0 on
+/// success.
+inline int write_raw_tables(const flat_detector& t, const char* path) {
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        return 1;
+    }
+    const uint32_t header[12] = {0x4f454744u,
+                                 DPROP_ABI_VERSION,
+                                 static_cast<uint32_t>(t.volumes.size()),
+                                 static_cast<uint32_t>(t.surfaces.size()),
+                                 static_cast<uint32_t>(t.masks.size()),
+                                 static_cast<uint32_t>(t.transforms.size()),
+                                 static_cast<uint32_t>(t.slabs.size()),
+                                 static_cast<uint32_t>(t.bf_surfaces.size()),
+                                 static_cast<uint32_t>(t.grids.size()),
+                                 static_cast<uint32_t>(t.grid_bins.size()),
+                                 0u,
+                                 0u};
+    bool ok = std::fwrite(header, sizeof(uint32_t), 12, f) == 12u;
+    auto put = [&](const auto& v) {
+        if (!v.empty()) {
+            ok = ok && std::fwrite(v.data(), sizeof(v[0]), v.size(), f) ==
+                           v.size();
+        }
+    };
+    put(t.volumes);
+    put(t.surfaces);
+    put(t.masks);
+    put(t.transforms);
+    put(t.slabs);
+    put(t.bf_surfaces);
+    put(t.grids);
+    put(t.grid_bins);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? 0 : 1;
+}
 
 /// Flatten a host detray detector into the tables of the C ABI.
 template <typename detector_t>

@@ -101,11 +101,14 @@ typedef struct dprop_surface_desc {
     uint32_t mask_begin;    /* [mask_begin, mask_end) into masks                   */
     uint32_t mask_end;
     uint32_t transform;     /* into transforms                                     */
-    uint32_t material;      /* into slabs, or DPROP_INVALID_INDEX                  */
+    uint32_t material;      /* into slabs (material_kind 0) or into grids, a
+                               material map (material_kind 1);
+                               DPROP_INVALID_INDEX: no material              */
     uint32_t volume;        /* owning volume                                       */
     uint8_t shape;          /* dprop_shape of all masks of this surface            */
     uint8_t kind;           /* dprop_surface_kind                                  */
-    uint8_t pad[2];
+    uint8_t material_kind;  /* 0: homogeneous slab / rod, 1: material map          */
+    uint8_t pad;
 } dprop_surface_desc;
 
 typedef struct dprop_mask_desc {
@@ -150,7 +153,14 @@ typedef enum dprop_material_kind {
 typedef enum dprop_grid_kind {
     DPROP_GRID_NONE = 0,
     DPROP_GRID_CYLINDER = 1, /* axes (phi circular [-pi,pi], z closed), ref. radius */
-    DPROP_GRID_DISC = 2      /* axes (r closed, phi circular [-pi,pi])              */
+    DPROP_GRID_DISC = 2,     /* axes (r closed, phi circular [-pi,pi])              */
+    /* Material maps (material/material_map.hpp: a grid of material slabs over
+     * the surface's bound local coordinates, one slab index per bin into
+     * slabs, looked up at the track's bound local position by
+     * material_accessor::get, material/detail/material_accessor.hpp): */
+    DPROP_GRID_MATERIAL_CYLINDER = 3, /* axes (r*phi circular, z closed)         */
+    DPROP_GRID_MATERIAL_DISC = 4,     /* axes (r closed, phi circular)           */
+    DPROP_GRID_MATERIAL_CARTESIAN = 5 /* axes (x closed, y closed)               */
 } dprop_grid_kind;
 
 /* A 2D surface grid of navigation/accelerators/spatial_grid.hpp with
@@ -288,8 +298,9 @@ typedef enum dprop_method {
     DPROP_METHOD_PLAIN = 0,      /* one thread per track, whole propagation   */
     DPROP_METHOD_PERSISTENT = 1  /* persistent lanes pulling tracks from a
                                     device work queue (detectors with line
-                                    surfaces, material rods or multi-entry
-                                    grid bins run the plain form)             */
+                                    surfaces, material rods, multi-entry
+                                    grid bins or material maps run the plain
+                                    form)                                     */
 } dprop_method;
 
 typedef struct dprop_launch {

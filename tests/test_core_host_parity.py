@@ -33,15 +33,18 @@ FP32 = {"loc0": 2e-3, "loc1": 2e-3, "phi": 2e-5, "theta": 2e-5,
         "qop": 1e-7, "time": 1e-6}
 
 
-@pytest.mark.parametrize("kind,n", [("telescope", 1000), ("toy", 3000)])
+@pytest.mark.parametrize("kind,n", [("telescope", 1000), ("toy", 3000),
+                                    ("toy_maps", 3000)])
 def test_core_f64_matches_reference(core_host, oracle, kind, n):
+    """toy_maps: the toy detector with the builder's material maps on its
+    portals (a slab per bin, looked up at the bound local position)."""
     from detray_b200 import abi, tracks
     if kind == "telescope":
         det = oracle.build_telescope()
         cfg = abi.make_config(max_records=16)
         trk = tracks.telescope_tracks(n, seed=3)
     else:
-        det = oracle.build_toy()
+        det = oracle.build_toy(use_material_maps=kind == "toy_maps")
         cfg = abi.make_config(max_records=32, search_window=(3, 3))
         trk = tracks.toy_tracks(n, seed=4)
     ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)}, cfg, trk)
@@ -84,14 +87,14 @@ def test_core_noise_estimation_and_no_material(core_host, oracle):
 WIRE = {"wire_chamber_10l_cells": True, "wire_chamber_10l_straws": False}
 
 
-@pytest.mark.parametrize("name", ["toy_4brl_7edc", "telescope_10x1m_300um",
-                                  *WIRE])
+@pytest.mark.parametrize("name", ["toy_4brl_7edc", "toy_4brl_7edc_maps",
+                                  "telescope_10x1m_300um", *WIRE])
 def test_committed_geometries_match_reference_builders(oracle, name):
     """The .npz geometries the product ships are byte-identical to the
     tables the reference's own builders produce through dprop::flatten."""
     from detray_b200 import geometry
     if name.startswith("toy"):
-        det = oracle.build_toy()
+        det = oracle.build_toy(use_material_maps=name.endswith("maps"))
     elif name.startswith("telescope"):
         det = oracle.build_telescope()
     else:
@@ -119,3 +122,53 @@ def test_core_f64_matches_reference_wire_chamber(core_host, oracle, square):
     s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
                 tol_rel=1e-7, cov_rel=1e-5)
     assert s["seq_mismatch"] == 0 and s["status_mismatch"] == 0
+
+
+def test_material_map_tables_are_validated(core_host):
+    """Material-map tables that point outside the slabs, at a rod, at a
+    navigation grid, or carry an unknown material kind are rejected when the
+    detector is read, before any track runs."""
+    from detray_b200 import abi, geometry, tracks
+    base = geometry.load_geometry("toy_4brl_7edc_maps")
+    cfg = abi.make_config(max_records=8)
+    trk = tracks.toy_tracks(4, seed=1)
+    res, r = _alloc(4, cfg.max_records)
+    mapped = np.nonzero(base["surfaces"]["material_kind"] == 1)[0]
+    first_map = int(base["surfaces"]["material"][mapped[0]])
+    first_bin = int(base["grids"]["bin_offset"][first_map])
+    nav_grid = int(np.nonzero(base["grids"]["kind"] == abi.GRID_CYLINDER)[0][0])
+
+    def run(tables):
+        desc = geometry.Descriptor(tables)
+        ptrs = (C.c_void_p * 8)(*[np.ascontiguousarray(trk[i]).ctypes.data
+                                  for i in range(8)])
+        b = (C.c_double * 3)(0.0, 0.0, 2.0 * T)
+        return core_host.core_host_propagate(8, C.byref(desc.desc), 0, b, None,
+                                             None, None, None, C.byref(cfg),
+                                             ptrs, C.c_uint64(4), C.byref(r))
+
+    assert run(base) == 0
+    bad = []
+    t = {k: v.copy() for k, v in base.items()}
+    t["grid_bins"][first_bin] = len(t["slabs"])
+    bad.append(t)
+    t = {k: v.copy() for k, v in base.items()}
+    t["slabs"]["kind"][t["grid_bins"][first_bin]] = abi.MATERIAL_ROD
+    bad.append(t)
+    t = {k: v.copy() for k, v in base.items()}
+    t["surfaces"]["material"][mapped[0]] = nav_grid
+    bad.append(t)
+    t = {k: v.copy() for k, v in base.items()}
+    t["surfaces"]["material_kind"][mapped[0]] = 2
+    bad.append(t)
+    t = {k: v.copy() for k, v in base.items()}
+    t["grids"]["kind"][first_map] = 6
+    bad.append(t)
+    for i, tables in enumerate(bad):
+        assert run(tables) != 0, i
+        assert core_host.core_host_last_error(), i
+
+
+def _alloc(n, max_records):
+    from oracle import ref_oracle
+    return ref_oracle.alloc_results(n, max_records)

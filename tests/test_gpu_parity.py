@@ -57,7 +57,8 @@ def _setup(kind):
         trk = tracks.toy_tracks(20000, seed=13, pt_range=(0.1, 100.0),
                                 eta_range=(-1.0, 1.0), vertex_sigma=(0, 0, 0))
     else:
-        tables = geometry.load_geometry("toy_4brl_7edc")
+        tables = geometry.load_geometry("toy_4brl_7edc_maps" if kind == "toy_maps"
+                                        else "toy_4brl_7edc")
         cfg = abi.make_config(max_records=32, search_window=(3, 3))
         trk = tracks.toy_tracks(20000, seed=12)
     det = propagator.Detector(tables)
@@ -65,16 +66,20 @@ def _setup(kind):
     return det, field, cfg, trk
 
 
-@pytest.mark.parametrize("kind", ["telescope", "toy", "wire_chamber_10l_cells",
+def _oracle_detector(oracle, kind):
+    if kind == "telescope":
+        return oracle.build_telescope()
+    if kind.startswith("wire"):
+        return oracle.build_wire_chamber(square_cells=kind.endswith("cells"))
+    return oracle.build_toy(use_material_maps=kind == "toy_maps")
+
+
+@pytest.mark.parametrize("kind", ["telescope", "toy", "toy_maps",
+                                  "wire_chamber_10l_cells",
                                   "wire_chamber_10l_straws"])
 def test_device_vs_oracle(torch_cuda, oracle, kind):
     det, field, cfg, trk = _setup(kind)
-    if kind == "telescope":
-        ref_det = oracle.build_telescope()
-    elif kind.startswith("wire"):
-        ref_det = oracle.build_wire_chamber(square_cells=kind.endswith("cells"))
-    else:
-        ref_det = oracle.build_toy()
+    ref_det = _oracle_detector(oracle, kind)
     ref = oracle.propagate(ref_det, field.spec, cfg, trk)
     got = _run_device(torch_cuda, det, field, cfg, trk)
     summary = compare(ref, got, max_seq_mismatch_frac=1e-3, tol_abs=TOL_ABS,
@@ -255,7 +260,7 @@ def test_graph_replay_and_autotune(torch_cuda):
     assert all(t > 0 for t in times)
 
 
-@pytest.mark.parametrize("kind", ["toy", "wire_chamber_10l_cells"])
+@pytest.mark.parametrize("kind", ["toy", "toy_maps", "wire_chamber_10l_cells"])
 def test_fp64_device_vs_oracle(torch_cuda, oracle, kind):
     """dprop_launch.precision = 8: the propagation core in double on the
     GPU (the reference's full-fp64 build) against the fp64 oracle.  Only the
@@ -263,8 +268,7 @@ def test_fp64_device_vs_oracle(torch_cuda, oracle, kind):
     except <= 0.01 % of tracks, parameters to ~1e-9."""
     from detray_b200 import propagator
     det, field, cfg, trk = _setup(kind)
-    ref_det = (oracle.build_toy() if kind == "toy"
-               else oracle.build_wire_chamber(square_cells=True))
+    ref_det = _oracle_detector(oracle, kind)
     ref = oracle.propagate(ref_det, field.spec, cfg, trk)
     dev = torch_cuda.tensor(trk, dtype=torch_cuda.float64, device="cuda")
     lc = propagator.make_launch(sort_tracks=1, precision=8)
