@@ -368,3 +368,34 @@ def gpu_toy_bench(cfg: abi.Config, bz: float, tracks: np.ndarray,
     if rc != 0:
         raise RuntimeError(lib.refgpu_last_error().decode())
     return {"ms_per_step": ms.value, "n_exited": int(ok.value)}
+
+
+def json_available() -> bool:
+    """The reference's JSON detector writer and reader (oracle/ref/
+    ref_json.cpp, built when nlohmann/json is found)."""
+    return (REF_DIR / "ref_json").exists()
+
+
+def write_json(kind: str, directory) -> list:
+    """Build a benchmark detector with the reference's builders and write it
+    with detray::io::write_detector into ``directory``.  kind: toy,
+    toy_maps, telescope, wire_cells, wire_straws.  Returns the written
+    .json files (those with data)."""
+    import subprocess
+    from pathlib import Path
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    subprocess.run([str(REF_DIR / "ref_json"), "write", kind, str(d)],
+                   check=True, capture_output=True)
+    return sorted(str(p) for p in d.glob("*.json"))
+
+
+def read_json_tables(kind: str, files, out_path) -> dict:
+    """Read detray JSON files with the reference's reader
+    (detray::io::read_detector into the detector type of ``kind``) and
+    return dprop::flatten of the result as table arrays."""
+    import subprocess
+    from detray_b200 import geometry
+    subprocess.run([str(REF_DIR / "ref_json"), "read", kind, str(out_path),
+                    *[str(f) for f in files]], check=True, capture_output=True)
+    return geometry.read_raw_tables(out_path)

@@ -6,6 +6,10 @@ are committed so the tests do not need it):
                   tests/unit_tests/cpu/material/bethe_equation.cpp (the
                   instantiations that are commented out there are skipped:
                   the reference does not meet its 5 % bound on them).
+  json_telescope/ the reference's JSON writer output for the 10-plane
+                  telescope (geometry + homogeneous material) and
+                  tables.npz, dprop::flatten of what the reference's JSON
+                  reader builds from those files (needs oracle/_ref/ref_json).
 
 Usage: python tests/golden/make_golden.py [reference checkout]
 """
@@ -50,6 +54,29 @@ def main(argv=None):
     cases = bethe_cases(ref)
     (HERE / "bethe_pdg.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(f"bethe_pdg.json: {len(cases)} cases")
+    json_fixture(HERE / "json_telescope")
+
+
+def json_fixture(out: Path) -> None:
+    import tempfile
+    sys.path.insert(0, str(HERE.parent.parent))
+    from oracle import ref_oracle
+    from detray_b200 import geometry
+    if not ref_oracle.json_available():
+        print("oracle/_ref/ref_json missing: JSON fixture not written")
+        return
+    files = ref_oracle.write_json("telescope", out)
+    # the writer stamps today's date into the headers: keep the fixture
+    # stable by blanking it
+    for f in files:
+        doc = json.loads(Path(f).read_text())
+        doc["header"]["common"]["date"] = ""
+        Path(f).write_text(json.dumps(doc, indent=1) + "\n")
+    with tempfile.TemporaryDirectory() as tmp:
+        tables = ref_oracle.read_json_tables("telescope", files,
+                                             Path(tmp) / "t.bin")
+    geometry.save_npz(tables, out / "tables.npz")
+    print(f"{out.name}: {[Path(f).name for f in files]} + tables.npz")
 
 
 if __name__ == "__main__":
