@@ -199,6 +199,18 @@ class Tracks(C.Structure):
     ]
 
 
+class Sequence(C.Structure):
+    """dprop_sequence: surface sequences for dprop_propagate_direct."""
+    _fields_ = [
+        ("barcodes", C.c_void_p),
+        ("length", C.c_void_p),
+        ("max_length", C.c_uint32),
+        ("direction", C.c_int32),
+        ("start_barcode", C.c_void_p),
+        ("start_bound", C.c_void_p * 6),
+    ]
+
+
 class Results(C.Structure):
     _fields_ = [
         ("status", C.c_void_p),

@@ -265,17 +265,33 @@ DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
     }
 }
 
-// Propagate one track to the end; returns a dprop_track_status code.
-template <typename S, bool W, typename Tape = no_tape>
-DPROP_HD uint8_t propagate_track(track_state<S>& ts,
-                                 const detector_view<S, W>& det,
-                                 const field_view<S>& field,
-                                 const prop_cfg<S>& cfg, record_sink<S>& rec,
-                                 const Tape& tape = Tape{}) {
+// The caching navigator as the loop's navigation policy
+// (navigator_base::init / update, navigation/navigator_base.hpp:56-154).
+struct caching_navigation {
+    template <typename S, bool W>
+    DPROP_HD void init(nav_state<S>& nav, const detector_view<S, W>& det,
+                       const track_view<S>& trk, const nav_cfg<S>& cfg) {
+        navigator_init(nav, det, trk, cfg);
+    }
+    template <typename S, bool W>
+    DPROP_HD bool update(nav_state<S>& nav, const detector_view<S, W>& det,
+                         const track_view<S>& trk, const nav_cfg<S>& cfg) {
+        return navigator_update(nav, det, trk, cfg);
+    }
+};
+
+// Propagate one track to the end with the navigation policy Nav (init and
+// update of the propagator's navigator); returns a dprop_track_status code.
+template <typename S, bool W, typename Tape, typename Nav>
+DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
+                                      const detector_view<S, W>& det,
+                                      const field_view<S>& field,
+                                      const prop_cfg<S>& cfg,
+                                      record_sink<S>& rec, const Tape& tape) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
 
-    navigator_init(nav, det, track_view<S>{st.pos, st.dir}, cfg.nav);
+    navigator.init(nav, det, track_view<S>{st.pos, st.dir}, cfg.nav);
     ts.heartbeat = nav.is_alive();
     bool is_init = true;
     double path_prev = 0.;
@@ -321,7 +337,7 @@ DPROP_HD uint8_t propagate_track(track_state<S>& ts,
                 stall = 0u;
             }
         }
-        is_init = navigator_update(nav, det, track_view<S>{st.pos, st.dir},
+        is_init = navigator.update(nav, det, track_view<S>{st.pos, st.dir},
                                    cfg.nav) ||
                   is_init;
         ts.heartbeat = ts.heartbeat && nav.is_alive();
@@ -343,6 +359,17 @@ DPROP_HD uint8_t propagate_track(track_state<S>& ts,
         default:
             return 3u;
     }
+}
+
+// Propagate one track with the caching navigator.
+template <typename S, bool W, typename Tape = no_tape>
+DPROP_HD uint8_t propagate_track(track_state<S>& ts,
+                                 const detector_view<S, W>& det,
+                                 const field_view<S>& field,
+                                 const prop_cfg<S>& cfg, record_sink<S>& rec,
+                                 const Tape& tape = Tape{}) {
+    caching_navigation navigator;
+    return propagate_track_with(navigator, ts, det, field, cfg, rec, tape);
 }
 
 }  // namespace dprop

@@ -34,7 +34,7 @@ ABI_SYMBOLS = [
     "dprop_field_create_const", "dprop_field_create_grid",
     "dprop_field_destroy", "dprop_propagate", "dprop_propagate_host",
     "dprop_propagate_noalloc", "dprop_autotune", "dprop_propagate_adjoint",
-    "dprop_backward",
+    "dprop_backward", "dprop_propagate_direct",
 ]
 
 
@@ -84,6 +84,10 @@ def load_library() -> C.CDLL:
         C.POINTER(abi.Config), C.c_void_p, C.POINTER(abi.Tracks),
         C.POINTER(abi.Results), C.POINTER(abi.Tape),
         C.POINTER(abi.Gradients), C.c_uint64, C.c_void_p]
+    lib.dprop_propagate_direct.argtypes = [
+        C.POINTER(abi.Config), C.c_void_p, C.c_void_p, C.POINTER(abi.Tracks),
+        C.POINTER(abi.Sequence), C.POINTER(abi.Results), C.c_uint64,
+        C.c_void_p]
     if lib.dprop_abi_version() != abi.DPROP_ABI_VERSION:
         raise PropagationError("detray-b200 library ABI version mismatch")
     _lib = lib
@@ -189,6 +193,7 @@ class DeviceResults:
     them."""
     tensors: dict
     struct: abi.Results
+    inputs: list | None = None  # input tensors a call must keep alive
 
 
 def alloc_device_results(n: int, max_records: int, device="cuda",
@@ -279,6 +284,68 @@ def propagate(cfg: abi.Config, det: Detector, field: Field, tracks,
     _check(load_library().dprop_propagate(
         C.byref(cfg), C.byref(lc), det.handle, field.handle, C.byref(ts),
         C.byref(results.struct), n, C.c_void_p(stream.cuda_stream)))
+    return results
+
+
+def propagate_direct(cfg: abi.Config, det: Detector, field: Field,
+                     sequence, lengths, direction: int = 1, tracks=None,
+                     start_barcode=None, start_bound=None,
+                     results: DeviceResults | None = None,
+                     stream=None) -> DeviceResults:
+    """Propagate along given surface sequences with the direct navigator
+    (dprop_propagate_direct).  ``sequence``: (max_length, n) int64 CUDA
+    tensor of surface barcodes, e.g. ``rec_barcode`` of a propagate() run;
+    ``lengths``: (n,) int32 CUDA tensor (``n_records``).  Start from the
+    (8, n) float32 ``tracks`` or from bound parameters ``start_bound``
+    ((6, n) float32) on the surfaces ``start_barcode`` ((n,) int64)."""
+    import torch
+    n = lengths.shape[0]
+    dev = lengths.device
+    for name, t in (("sequence", sequence), ("lengths", lengths)):
+        if not (hasattr(t, "is_cuda") and t.is_cuda):
+            raise PropagationError(f"{name} must be a CUDA tensor")
+    if sequence.dtype != torch.int64 or sequence.dim() != 2 or \
+            sequence.shape[1] != n:
+        raise PropagationError("sequence must be a (max_length, n) int64 "
+                               "tensor")
+    if lengths.dtype != torch.int32:
+        raise PropagationError("lengths must be an int32 tensor")
+    sequence = sequence.contiguous()
+    lengths = lengths.contiguous()
+    sq = abi.Sequence()
+    sq.barcodes = sequence.data_ptr() if sequence.numel() else None
+    sq.length = lengths.data_ptr()
+    sq.max_length = sequence.shape[0]
+    sq.direction = int(direction)
+    ts = None
+    keep = [sequence, lengths]
+    if start_barcode is not None:
+        if start_bound is None or start_bound.dtype != torch.float32 or \
+                tuple(start_bound.shape) != (6, n):
+            raise PropagationError("start_bound must be a (6, n) float32 "
+                                   "tensor")
+        start_barcode = start_barcode.contiguous()
+        start_bound = start_bound.contiguous()
+        keep += [start_barcode, start_bound]
+        sq.start_barcode = start_barcode.data_ptr()
+        for i in range(6):
+            sq.start_bound[i] = start_bound[i].data_ptr()
+    else:
+        if tracks is None or tracks.dtype != torch.float32 or \
+                tuple(tracks.shape) != (8, n):
+            raise PropagationError("tracks must be a (8, n) float32 tensor")
+        tracks = tracks.contiguous()
+        keep.append(tracks)
+        ts = tracks_struct(tracks)
+    if results is None:
+        results = alloc_device_results(n, cfg.max_records, dev)
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    _check(load_library().dprop_propagate_direct(
+        C.byref(cfg), det.handle, field.handle,
+        C.byref(ts) if ts is not None else None, C.byref(sq),
+        C.byref(results.struct), n, C.c_void_p(stream.cuda_stream)))
+    results.inputs = keep  # alive until the caller drops the results
     return results
 
 

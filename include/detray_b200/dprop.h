@@ -376,6 +376,50 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
                                   const dprop_results* results,
                                   uint64_t n_tracks);
 
+/* ------------------------------------------------------ direct navigation
+ * Propagation along a given sequence of surfaces (the Kalman-filter fit and
+ * smoothing steps either side of the propagation path): replaces the
+ * reference's propagator<rk_stepper, direct_navigator, actor chain>
+ * (core/include/detray/navigation/direct_navigator.hpp:34-304) fed by the
+ * surface_sequencer actor (core/include/detray/propagator/actors/
+ * surface_sequencer.hpp:24-106).
+ *
+ * The sequence of a track is what the sequencer collects: the sensitive and
+ * material surfaces the caching navigator reached, i.e. the records of a
+ * dprop_propagate run with record_all_surfaces = 0 - rec_barcode and
+ * n_records of that run can be passed as they are.  The navigator
+ * intersects only the next surface of the sequence, with every mask
+ * accepting the track, and the actor chain (transport, material
+ * interaction, records) runs on each of them.  direction -1 walks the
+ * sequence from its last entry to its first with the track moving backwards
+ * (energy gained in material).  A track whose next surface cannot be
+ * intersected ends with DPROP_TRK_NO_SURFACE; an empty sequence ends at
+ * once with DPROP_TRK_EXITED and no records. */
+typedef struct dprop_sequence {
+    const uint64_t* barcodes;   /* [max_length * n]: entry k of track t at
+                                   k * n + t (device memory)                   */
+    const uint32_t* length;     /* [n] entries per track; values above
+                                   max_length are read as max_length          */
+    uint32_t max_length;
+    int32_t direction;          /* +1 forward, -1 backward                    */
+    /* Optional start on a surface (bound_track_parameters: the propagator
+     * state converts them to the free vector there, base_stepper.hpp:84-107)
+     * instead of dprop_tracks: NULL start_barcode = start from the tracks. */
+    const uint64_t* start_barcode;  /* [n] surface of the bound start         */
+    const float* start_bound[6];    /* [n] each: loc0, loc1, phi, theta, q/p,
+                                       t                                      */
+} dprop_sequence;
+
+/* Device buffers, float tracks and results as dprop_propagate; `tracks` may
+ * be NULL when the sequence carries a bound start.  Stream ordered. */
+dprop_status dprop_propagate_direct(const dprop_config* cfg,
+                                    const dprop_detector* det,
+                                    const dprop_field* field,
+                                    const dprop_tracks* tracks,
+                                    const dprop_sequence* sequence,
+                                    const dprop_results* results,
+                                    uint64_t n_tracks, void* stream);
+
 /* ------------------------------------------------- allocation-free variant
  * dprop_propagate_noalloc has no counterpart in the reference.
  *

@@ -18,7 +18,10 @@
  *     surface_recorder>>::propagate over a batch of free tracks with OpenMP,
  *     the chain the reference's device tests use
  *     (tests/include/detray/test/device/propagator_test.hpp:84-93,114-168),
- *     writing the same result layout as dprop_propagate_host.
+ *     writing the same result layout as dprop_propagate_host;
+ *   - ref_propagate_direct: the same chain with the direct_navigator
+ *     (core/include/detray/navigation/direct_navigator.hpp) along given
+ *     surface sequences, forward or backward, from free or bound starts.
  *
  * The scalar type is DETRAY_CUSTOM_SCALARTYPE: the recipe builds a double
  * (the correctness oracle) and a float (the CPU timing baseline) library.
@@ -29,6 +32,7 @@
 #include "detray/material/material_slab.hpp"
 #include "detray/material/predefined_materials.hpp"
 #include "detray/navigation/caching_navigator.hpp"
+#include "detray/navigation/direct_navigator.hpp"
 #include "detray/propagator/actor_chain.hpp"
 #include "detray/propagator/actors/aborters.hpp"
 #include "detray/propagator/actors/parameter_updater.hpp"
@@ -265,6 +269,55 @@ struct host_results {
     }
 };
 
+/// Write one track's status, final state and records into the results.
+template <typename state_t>
+void store_results(const dprop_results* out, uint64_t t, uint64_t n,
+                   uint8_t status, const record_buffer& buf,
+                   const state_t& state, uint32_t cap, double* rec_jac) {
+    if (out->status) {
+        out->status[t] = status;
+    }
+    if (out->n_records) {
+        out->n_records[t] = buf.n;
+    }
+    if (out->n_trials) {
+        out->n_trials[t] =
+            static_cast<uint32_t>(state.stepping().n_total_trials());
+    }
+    host_results::put(out->path_length, t, state.stepping().path_length());
+    const auto& fin = state.stepping()();
+    const auto fpos = fin.pos();
+    const auto fdir = fin.dir();
+    const double fvals[8] = {fpos[0], fpos[1], fpos[2], fin.time(),
+                             fdir[0], fdir[1], fdir[2], fin.qop()};
+    for (unsigned int k = 0; k < 8u; ++k) {
+        host_results::put(out->final_free[k], t, fvals[k]);
+    }
+    for (uint32_t k = 0; k < static_cast<uint32_t>(buf.recs.size()); ++k) {
+        const auto& r = buf.recs[k];
+        const uint64_t o = static_cast<uint64_t>(k) * n + t;
+        if (out->rec_barcode) {
+            out->rec_barcode[o] = r.barcode;
+        }
+        if (out->rec_flags) {
+            out->rec_flags[o] = r.flags;
+        }
+        host_results::put(out->rec_path, o, r.path);
+        for (unsigned int i = 0; i < 6u; ++i) {
+            host_results::put(out->rec_bound[i], o, r.bound[i]);
+        }
+        for (unsigned int i = 0; i < 21u; ++i) {
+            host_results::put(out->rec_cov[i], o, r.cov[i]);
+        }
+        if (rec_jac != nullptr) {
+            for (unsigned int i = 0; i < 36u; ++i) {
+                rec_jac[(static_cast<uint64_t>(i) * cap + k) * n + t] =
+                    r.jac[i];
+            }
+        }
+    }
+}
+
 template <typename det_t, bool with_interactor, typename insp_t>
 int propagate_impl(const det_t& det, const oracle_field::field& field,
                    const dprop_config& cfg, const double* const trk[8],
@@ -376,48 +429,129 @@ int propagate_impl(const det_t& det, const oracle_field::field& field,
             }
         }
 
-        if (out->status) {
-            out->status[t] = status;
+        store_results(out, t, n, status, buf, state, cap, rec_jac);
+    }
+    return 0;
+}
+
+// ------------------------------------------------ direct navigation
+// propagator<rk_stepper, direct_navigator, same actor chain> along the given
+// surface sequences (barcodes, slot-major [k * n + t]).
+template <typename det_t, bool with_interactor>
+int propagate_direct_impl(const det_t& det, const oracle_field::field& field,
+                          const dprop_config& cfg, const double* const* trk,
+                          uint64_t n, const uint64_t* seq,
+                          const uint32_t* seq_len, uint32_t max_len,
+                          int direction, const uint64_t* start_bc,
+                          const double* const* start_bound,
+                          const dprop_results* out, int n_threads) {
+    using base = prop_types<det_t, with_interactor, navigation::void_inspector>;
+    using navigator_t = direct_navigator<det_t>;
+    using propagator_t = propagator<typename base::stepper_t, navigator_t,
+                                    typename base::chain_t>;
+    using surface_t = typename det_t::surface_type;
+    const propagation::config pcfg = to_ref_config(cfg);
+    const propagator_t p{pcfg};
+    const field_view fview{&field};
+    const scalar path_limit = cfg.use_path_limit_aborter
+                                  ? static_cast<scalar>(cfg.path_limit)
+                                  : std::numeric_limits<scalar>::max();
+    const uint32_t cap = cfg.max_records;
+    if (n_threads > 0) {
+        omp_set_num_threads(n_threads);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t ti = 0; ti < static_cast<int64_t>(n); ++ti) {
+        const auto t = static_cast<uint64_t>(ti);
+        const uint32_t len = seq_len[t] < max_len ? seq_len[t] : max_len;
+        std::vector<surface_t> sequence;
+        for (uint32_t k = 0; k < len; ++k) {
+            const uint64_t bc = seq[static_cast<uint64_t>(k) * n + t];
+            sequence.push_back(det.surface(
+                static_cast<dindex>((bc >> 27) & 0x1fffffu)));
         }
-        if (out->n_records) {
-            out->n_records[t] = buf.n;
+        if (sequence.empty()) {
+            // the reference asserts a non-empty sequence: an empty one ends
+            // at once, as its update() does when no target is left
+            if (out->status) out->status[t] = DPROP_TRK_EXITED;
+            if (out->n_records) out->n_records[t] = 0u;
+            continue;
         }
-        if (out->n_trials) {
-            out->n_trials[t] =
-                static_cast<uint32_t>(state.stepping().n_total_trials());
-        }
-        host_results::put(out->path_length, t, state.stepping().path_length());
-        const auto& fin = state.stepping()();
-        const auto fpos = fin.pos();
-        const auto fdir = fin.dir();
-        const double fvals[8] = {fpos[0], fpos[1], fpos[2], fin.time(),
-                                 fdir[0], fdir[1], fdir[2], fin.qop()};
-        for (unsigned int k = 0; k < 8u; ++k) {
-            host_results::put(out->final_free[k], t, fvals[k]);
-        }
-        for (uint32_t k = 0; k < static_cast<uint32_t>(buf.recs.size());
-             ++k) {
-            const auto& r = buf.recs[k];
-            const uint64_t o = static_cast<uint64_t>(k) * n + t;
-            if (out->rec_barcode) {
-                out->rec_barcode[o] = r.barcode;
+        auto seq_view = vecmem::get_data(sequence);
+
+        record_buffer buf;
+        buf.capacity = cap;
+        buf.record_all = cfg.record_all_surfaces != 0;
+        buf.recs.reserve(cap);
+        typename actor::pathlimit_aborter<scalar>::state pl{path_limit};
+        actor::parameter_updater_state<algebra_t> us{pcfg};
+        actor::pointwise_material_interactor<algebra_t>::state is{};
+        surface_recorder::state rs{&buf, &us};
+
+        auto run = [&](auto& state) {
+            state.stepping().template set_constraint<
+                step::constraint::e_accuracy>(pcfg.stepping.step_constraint);
+            if (direction < 0) {
+                state.navigation().set_direction(
+                    navigation::direction::e_backward);
             }
-            if (out->rec_flags) {
-                out->rec_flags[o] = r.flags;
+            state.navigation().reset();
+            pdg_particle<scalar> ptc = muon<scalar>();
+            if (cfg.pdg == 211 || cfg.pdg == -211) {
+                ptc = pion_plus<scalar>();
+            } else if (cfg.pdg == 11 || cfg.pdg == -11) {
+                ptc = electron<scalar>();
             }
-            host_results::put(out->rec_path, o, r.path);
-            for (unsigned int i = 0; i < 6u; ++i) {
-                host_results::put(out->rec_bound[i], o, r.bound[i]);
-            }
-            for (unsigned int i = 0; i < 21u; ++i) {
-                host_results::put(out->rec_cov[i], o, r.cov[i]);
-            }
-            if (rec_jac != nullptr) {
-                for (unsigned int i = 0; i < 36u; ++i) {
-                    rec_jac[(static_cast<uint64_t>(i) * cap + k) * n + t] =
-                        r.jac[i];
+            const auto start = state.stepping()();
+            state.set_particle(update_particle_hypothesis(ptc, start));
+            bool ok = false;
+            bool failed = false;
+            try {
+                if constexpr (with_interactor) {
+                    auto refs = detray::tie(pl, us, is, rs);
+                    ok = p.propagate(state, refs);
+                } else {
+                    auto refs = detray::tie(pl, us, rs);
+                    ok = p.propagate(state, refs);
                 }
+            } catch (const std::exception&) {
+                failed = true;
             }
+            const auto& fs = state.stepping()();
+            if (!std::isfinite(static_cast<double>(fs.qop())) ||
+                std::fabs(static_cast<double>(fs.qop())) > 1e30) {
+                failed = true;
+            }
+            uint8_t status = DPROP_TRK_EXITED;
+            if (failed) {
+                status = DPROP_TRK_NONFINITE;
+            } else if (!ok) {
+                status = state.stepping().abs_path_length() >= path_limit
+                             ? DPROP_TRK_PATH_LIMIT
+                             : DPROP_TRK_NO_SURFACE;
+            }
+            store_results(out, t, n, status, buf, state, cap, nullptr);
+        };
+        if (start_bc != nullptr) {
+            bound_track_parameters<algebra_t> bp{};
+            bp.set_surface_link(geometry::identifier{start_bc[t]});
+            for (unsigned int i = 0; i < 6u; ++i) {
+                bp[i] = static_cast<scalar>(start_bound[i][t]);
+            }
+            typename propagator_t::state state(bp, fview, det, seq_view);
+            run(state);
+        } else {
+            free_track_parameters<algebra_t> track{};
+            track.set_pos({static_cast<scalar>(trk[0][t]),
+                           static_cast<scalar>(trk[1][t]),
+                           static_cast<scalar>(trk[2][t])});
+            track.set_time(static_cast<scalar>(trk[3][t]));
+            track.set_dir({static_cast<scalar>(trk[4][t]),
+                           static_cast<scalar>(trk[5][t]),
+                           static_cast<scalar>(trk[6][t])});
+            track.set_qop(static_cast<scalar>(trk[7][t]));
+            typename propagator_t::state state(track, fview, det, seq_view);
+            run(state);
         }
     }
     return 0;
@@ -689,6 +823,54 @@ int ref_propagate_jac(void* handle, const ref_field_desc* fd,
                             with_abort_reasons, rec_jac);
         }
         g_error = "ref_propagate_jac: empty detector handle";
+        return 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/// The reference's direct-navigator propagation along surface sequences
+/// (barcodes [max_len * n], slot-major; lengths [n]); direction +1 / -1;
+/// start from the free tracks, or - with start_bc - from bound parameters
+/// (start_bound: 6 arrays of n) on the surfaces start_bc.  Constant or map
+/// field as ref_propagate.
+int ref_propagate_direct(void* handle, const ref_field_desc* fd,
+                         const dprop_config* cfg, const double* const* tracks,
+                         uint64_t n, const uint64_t* seq,
+                         const uint32_t* seq_len, uint32_t max_len,
+                         int direction, const uint64_t* start_bc,
+                         const double* const* start_bound,
+                         const dprop_results* out, int n_threads) {
+    try {
+        auto* h = static_cast<det_handle*>(handle);
+        oracle_field::field f;
+        if (fd->kind == 0u) {
+            f.set_constant(fd->b[0], fd->b[1], fd->b[2]);
+        } else {
+            f.set_grid(fd->lo, fd->hi, fd->n, fd->values);
+        }
+        auto go = [&](const auto& det) {
+            using det_t = std::decay_t<decltype(det)>;
+            if (cfg->use_material_interactor) {
+                return propagate_direct_impl<det_t, true>(
+                    det, f, *cfg, tracks, n, seq, seq_len, max_len, direction,
+                    start_bc, start_bound, out, n_threads);
+            }
+            return propagate_direct_impl<det_t, false>(
+                det, f, *cfg, tracks, n, seq, seq_len, max_len, direction,
+                start_bc, start_bound, out, n_threads);
+        };
+        if (auto* toy = std::get_if<std::unique_ptr<toy_det_t>>(&h->det)) {
+            return go(**toy);
+        }
+        if (auto* tel = std::get_if<std::unique_ptr<tel_det_t>>(&h->det)) {
+            return go(**tel);
+        }
+        if (auto* wire = std::get_if<std::unique_ptr<wire_det_t>>(&h->det)) {
+            return go(**wire);
+        }
+        g_error = "ref_propagate_direct: empty detector handle";
         return 1;
     } catch (const std::exception& e) {
         g_error = e.what();

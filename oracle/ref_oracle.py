@@ -93,6 +93,10 @@ def load(precision: str = "f64") -> C.CDLL:
         C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
         C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
         C.c_int, C.c_int, C.c_void_p]
+    lib.ref_propagate_direct.argtypes = [
+        C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
+        C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int,
+        C.c_void_p, C.c_void_p, C.POINTER(abi.Results), C.c_int]
     lib.ref_material_slab.argtypes = [C.c_char_p, C.c_double,
                                       C.POINTER(abi.SlabDesc),
                                       C.POINTER(C.c_double)]
@@ -319,6 +323,50 @@ def propagate(det: RefDetector, field: dict, cfg: abi.Config,
         chunk, int(abort_reasons),
         jac.ctypes.data_as(C.c_void_p) if jac is not None else None))
     del keep
+    return res
+
+
+def propagate_direct(det: RefDetector, field: dict, cfg: abi.Config,
+                     sequence: np.ndarray, lengths: np.ndarray,
+                     direction: int = 1, tracks: np.ndarray | None = None,
+                     start_barcode: np.ndarray | None = None,
+                     start_bound: np.ndarray | None = None,
+                     n_threads: int = 0) -> dict:
+    """The reference's propagation with the direct navigator along the
+    surface sequences ``sequence`` (barcodes, shape (max_length, n)) of
+    ``lengths`` entries, forward (+1) or backward (-1); starting from the
+    free ``tracks`` (8, n) or from bound parameters ``start_bound`` (6, n)
+    on the surfaces ``start_barcode`` (n)."""
+    lib = det._lib
+    seq = np.ascontiguousarray(sequence, dtype=np.uint64)
+    lens = np.ascontiguousarray(lengths, dtype=np.uint32)
+    n = lens.shape[0]
+    max_len = seq.shape[0]
+    keep = []
+    trk_ptrs = None
+    if tracks is not None:
+        trk = np.ascontiguousarray(tracks, dtype=np.float64)
+        keep.append(trk)
+        trk_ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    sb_ptrs = None
+    sbc = None
+    if start_barcode is not None:
+        sbc = np.ascontiguousarray(start_barcode, dtype=np.uint64)
+        sb = np.ascontiguousarray(start_bound, dtype=np.float64)
+        keep.append(sb)
+        sb_ptrs = (C.c_void_p * 6)(*[sb[i].ctypes.data for i in range(6)])
+    res, r = alloc_results(n, cfg.max_records)
+    fd, fkeep = field_desc(field)
+    if n_threads <= 0:
+        n_threads = os.cpu_count() or 1
+    _check(lib, lib.ref_propagate_direct(
+        det.handle, C.byref(fd), C.byref(cfg),
+        C.cast(trk_ptrs, C.c_void_p) if trk_ptrs is not None else None, n,
+        seq.ctypes.data if max_len > 0 else None, lens.ctypes.data, max_len,
+        int(direction), sbc.ctypes.data if sbc is not None else None,
+        C.cast(sb_ptrs, C.c_void_p) if sb_ptrs is not None else None,
+        C.byref(r), n_threads))
+    del fkeep, keep
     return res
 
 

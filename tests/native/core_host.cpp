@@ -12,7 +12,7 @@
 
 #include "core/config.hpp"
 #include "core/convert.hpp"
-#include "core/propagate.cuh"
+#include "core/direct.cuh"
 
 using namespace dprop;
 
@@ -26,12 +26,22 @@ struct sink_bufs {
     std::vector<S> path;
 };
 
+// Direct-navigation inputs (dprop_sequence with host double arrays)
+struct direct_args {
+    const uint64_t* barcodes;
+    const uint32_t* length;
+    uint32_t max_length;
+    int32_t direction;
+    const uint64_t* start_barcode;
+    const double* const* start_bound;
+};
+
 template <typename S>
 int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         const double* lo, const double* hi, const uint32_t* nn,
         const float* values, const dprop_config* c, const double* const* trk,
         uint64_t n, const dprop_results* out, double* tape_rec = nullptr,
-        double* tape_init = nullptr) {
+        double* tape_init = nullptr, const direct_args* da = nullptr) {
     const std::string problem = validate_desc(desc);
     if (!problem.empty()) {
         g_err = problem;
@@ -70,13 +80,30 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
     const uint32_t cap = c->max_records;
     for (uint64_t t = 0; t < n; ++t) {
         track_state<S> ts;
-        init_track_state(ts,
-                         vec3<S>{static_cast<S>(trk[0][t]), static_cast<S>(trk[1][t]),
-                                 static_cast<S>(trk[2][t])},
-                         static_cast<S>(trk[3][t]),
-                         vec3<S>{static_cast<S>(trk[4][t]), static_cast<S>(trk[5][t]),
-                                 static_cast<S>(trk[6][t])},
-                         static_cast<S>(trk[7][t]), cfg);
+        bool start_ok = true;
+        if (da != nullptr && da->start_barcode != nullptr) {
+            S bs[6];
+            for (int i = 0; i < 6; ++i) {
+                bs[i] = static_cast<S>(da->start_bound[i][t]);
+            }
+            vec3<S> p{S(0), S(0), S(0)}, d{S(0), S(0), S(1)};
+            S tm = S(0), q = bs[4];
+            const uint32_t sf = barcode_index(da->start_barcode[t]);
+            if (sf < det.n_surfaces) {
+                bound_start(det, sf, bs, p, d, tm, q);
+            } else {
+                start_ok = false;
+            }
+            init_track_state(ts, p, tm, d, q, cfg);
+        } else {
+            init_track_state(ts,
+                             vec3<S>{static_cast<S>(trk[0][t]), static_cast<S>(trk[1][t]),
+                                     static_cast<S>(trk[2][t])},
+                             static_cast<S>(trk[3][t]),
+                             vec3<S>{static_cast<S>(trk[4][t]), static_cast<S>(trk[5][t]),
+                                     static_cast<S>(trk[6][t])},
+                             static_cast<S>(trk[7][t]), cfg);
+        }
         // records into per-track scratch, then widened into the double outputs
         std::vector<uint64_t> bc(cap);
         std::vector<S> bnd[6], cv[21];
@@ -124,6 +151,20 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
                         trec[static_cast<size_t>(comp) * cap + k];
                 }
             }
+        } else if (da != nullptr) {
+            ts.nav.direction = static_cast<S>(da->direction);
+            direct_navigation<S> navigator;
+            navigator.sequence = da->barcodes;
+            navigator.n_tracks = n;
+            navigator.track = t;
+            const uint32_t len = da->length[t];
+            navigator.length = static_cast<int32_t>(
+                len < da->max_length ? len : da->max_length);
+            navigator.next_external = 0;
+            navigator.reset(ts.nav, det);
+            status = start_ok ? propagate_track_with(navigator, ts, det, f,
+                                                     cfg, rec, no_tape{})
+                              : uint8_t(DPROP_TRK_NO_SURFACE);
         } else {
             status = propagate_track(ts, det, f, cfg, rec);
         }
@@ -172,6 +213,29 @@ int core_host_propagate(int precision_bytes, const dprop_detector_desc* desc,
         return run<double>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
     }
     return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
+}
+
+// Direct-navigation propagation (constant field b): as
+// dprop_propagate_direct with host double arrays; trk may be NULL with a
+// bound start.
+int core_host_propagate_direct(int precision_bytes,
+                               const dprop_detector_desc* desc,
+                               const double* b, const dprop_config* cfg,
+                               const double* const* trk, uint64_t n,
+                               const uint64_t* barcodes,
+                               const uint32_t* length, uint32_t max_length,
+                               int32_t direction,
+                               const uint64_t* start_barcode,
+                               const double* const* start_bound,
+                               const dprop_results* out) {
+    const direct_args da{barcodes, length, max_length, direction,
+                         start_barcode, start_bound};
+    if (precision_bytes == 8) {
+        return run<double>(desc, 0u, b, nullptr, nullptr, nullptr, nullptr,
+                           cfg, trk, n, out, nullptr, nullptr, &da);
+    }
+    return run<float>(desc, 0u, b, nullptr, nullptr, nullptr, nullptr, cfg,
+                      trk, n, out, nullptr, nullptr, &da);
 }
 
 // Adjoint-mode propagation: as core_host_propagate, plus the tape

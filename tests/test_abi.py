@@ -64,6 +64,7 @@ STRUCTS = {
     "dprop_volume_desc": abi.VolumeDesc,
     "dprop_tape": abi.Tape,
     "dprop_gradients": abi.Gradients,
+    "dprop_sequence": abi.Sequence,
 }
 
 
@@ -106,3 +107,5 @@ def test_argument_validation_without_device(lib):
     cfg = abi.make_config(use_field_gradient=1)
     assert lib.dprop_propagate(C.byref(cfg), None, None, None, None, None, 0,
                                None) == abi.DPROP_E_UNSUPPORTED
+    assert lib.dprop_propagate_direct(None, None, None, None, None, None, 0,
+                                      None) == abi.DPROP_E_INVALID
