@@ -211,6 +211,34 @@ class Sequence(C.Structure):
     ]
 
 
+# dprop_scan_status
+SCAN_OK = 0
+SCAN_OVERFLOW = 1
+SCAN_EMPTY = 2
+
+
+class ScanResults(C.Structure):
+    """dprop_scan_results: output of dprop_helix_scan."""
+    _fields_ = [
+        ("status", C.c_void_p),
+        ("n_hits", C.c_void_p),
+        ("barcode", C.c_void_p),
+        ("path", C.c_void_p),
+        ("loc", C.c_void_p * 2),
+        ("volume_link", C.c_void_p),
+        ("capacity", C.c_uint32),
+        ("precision", C.c_uint32),
+    ]
+
+
+class Validation(C.Structure):
+    """dprop_validation: output of dprop_validate_navigation."""
+    _fields_ = [
+        ("n_missed", C.c_void_p),
+        ("n_extra", C.c_void_p),
+    ]
+
+
 class Results(C.Structure):
     _fields_ = [
         ("status", C.c_void_p),

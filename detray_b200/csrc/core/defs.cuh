@@ -59,6 +59,7 @@ using std::cos;
 using std::fabs;
 using std::floor;
 using std::fma;
+using std::isfinite;
 using std::log;
 using std::log10;
 using std::pow;

@@ -34,7 +34,8 @@ ABI_SYMBOLS = [
     "dprop_field_create_const", "dprop_field_create_grid",
     "dprop_field_destroy", "dprop_propagate", "dprop_propagate_host",
     "dprop_propagate_noalloc", "dprop_autotune", "dprop_propagate_adjoint",
-    "dprop_backward", "dprop_propagate_direct",
+    "dprop_backward", "dprop_propagate_direct", "dprop_helix_scan",
+    "dprop_validate_navigation",
 ]
 
 
@@ -87,6 +88,13 @@ def load_library() -> C.CDLL:
     lib.dprop_propagate_direct.argtypes = [
         C.POINTER(abi.Config), C.c_void_p, C.c_void_p, C.POINTER(abi.Tracks),
         C.POINTER(abi.Sequence), C.POINTER(abi.Results), C.c_uint64,
+        C.c_void_p]
+    lib.dprop_helix_scan.argtypes = [
+        C.c_void_p, C.POINTER(C.c_double), C.POINTER(abi.Tracks), C.c_uint64,
+        C.c_double, C.POINTER(abi.ScanResults), C.c_void_p]
+    lib.dprop_validate_navigation.argtypes = [
+        C.POINTER(abi.ScanResults), C.POINTER(abi.Results), C.c_uint32,
+        C.c_uint32, C.c_uint64, C.c_double, C.POINTER(abi.Validation),
         C.c_void_p]
     if lib.dprop_abi_version() != abi.DPROP_ABI_VERSION:
         raise PropagationError("detray-b200 library ABI version mismatch")
@@ -347,6 +355,81 @@ def propagate_direct(cfg: abi.Config, det: Detector, field: Field,
         C.byref(results.struct), n, C.c_void_p(stream.cuda_stream)))
     results.inputs = keep  # alive until the caller drops the results
     return results
+
+
+def helix_scan(det: Detector, b, tracks, mask_tolerance: float = 0.0,
+               capacity: int = 256, stream=None) -> dict:
+    """Truth intersections of every track's helix in the constant field
+    ``b`` (3 components, detray units) with all surfaces of ``det``
+    (dprop_helix_scan): per track the hits inside a mask and along the
+    track, sorted by path and cut after the first world exit.  ``tracks``:
+    (8, n) float32 or float64 CUDA tensor; the results have its precision.
+    Returns CUDA tensors: status, n_hits, barcode/path/loc0/loc1/volume_link
+    of shape (capacity, n)."""
+    import torch
+    if not (hasattr(tracks, "is_cuda") and tracks.is_cuda) or \
+            tracks.dim() != 2 or tracks.shape[0] != 8 or \
+            tracks.dtype not in (torch.float32, torch.float64):
+        raise PropagationError("tracks must be a (8, n) float32/float64 "
+                               "CUDA tensor")
+    tracks = tracks.contiguous()
+    n = tracks.shape[1]
+    dev = tracks.device
+    ft = dict(dtype=tracks.dtype, device=dev)
+    out = {
+        "status": torch.empty(n, dtype=torch.uint8, device=dev),
+        "n_hits": torch.empty(n, dtype=torch.int32, device=dev),
+        "barcode": torch.empty((capacity, n), dtype=torch.int64, device=dev),
+        "path": torch.empty((capacity, n), **ft),
+        "loc0": torch.empty((capacity, n), **ft),
+        "loc1": torch.empty((capacity, n), **ft),
+        "volume_link": torch.empty((capacity, n), dtype=torch.int16,
+                                   device=dev),
+    }
+    r = abi.ScanResults()
+    r.status = out["status"].data_ptr()
+    r.n_hits = out["n_hits"].data_ptr()
+    r.barcode = out["barcode"].data_ptr()
+    r.path = out["path"].data_ptr()
+    r.loc[0] = out["loc0"].data_ptr()
+    r.loc[1] = out["loc1"].data_ptr()
+    r.volume_link = out["volume_link"].data_ptr()
+    r.capacity = capacity
+    r.precision = 8 if tracks.dtype == torch.float64 else 4
+    bb = (C.c_double * 3)(*[float(x) for x in b])
+    ts = tracks_struct(tracks)
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    _check(load_library().dprop_helix_scan(
+        det.handle, bb, C.byref(ts), n, float(mask_tolerance), C.byref(r),
+        C.c_void_p(stream.cuda_stream)))
+    out["_inputs"] = tracks
+    out["_struct"] = r
+    return out
+
+
+def validate_navigation(scan: dict, results: DeviceResults, max_records: int,
+                        path_tolerance: float = 0.1, stream=None):
+    """Holes and extra surfaces per track of a propagation (``results`` of
+    propagate() with record_all_surfaces = 1) against the helix_scan() of
+    the same tracks (dprop_validate_navigation).  Returns the CUDA tensors
+    (n_missed, n_extra)."""
+    import torch
+    n = scan["status"].shape[0]
+    dev = scan["status"].device
+    missed = torch.empty(n, dtype=torch.int32, device=dev)
+    extra = torch.empty(n, dtype=torch.int32, device=dev)
+    v = abi.Validation()
+    v.n_missed = missed.data_ptr()
+    v.n_extra = extra.data_ptr()
+    rp = 8 if results.tensors["rec_path"].dtype == torch.float64 else 4
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    _check(load_library().dprop_validate_navigation(
+        C.byref(scan["_struct"]), C.byref(results.struct), rp, max_records,
+        n, float(path_tolerance), C.byref(v),
+        C.c_void_p(stream.cuda_stream)))
+    return missed, extra
 
 
 def alloc_host_results(n: int, max_records: int, pinned: bool = False,

@@ -420,6 +420,72 @@ dprop_status dprop_propagate_direct(const dprop_config* cfg,
                                     const dprop_results* results,
                                     uint64_t n_tracks, void* stream);
 
+/* ------------------------------------------------------------ helix scan
+ * Truth intersections for navigation validation: each track's exact helix
+ * in the constant field b, intersected with every surface of the detector
+ * (Newton-Raphson with bisection safeguard), the intersections inside a mask
+ * and along the track sorted by path length and cut after the first one that
+ * leaves the world.  Replaces the reference's CPU detector scan
+ * detector_scanner::run<helix_scan> (tests/include/detray/test/validation/
+ * detector_scanner.hpp:52-140) with its helix intersectors
+ * (core/include/detray/navigation/intersection/helix_*_intersector.hpp,
+ * core/include/detray/utils/root_finding.hpp); the reference's extra start
+ * record (a marker at the track origin) is not written.
+ *
+ * Mask tolerance: mask_tolerance mm on sensitive and passive surfaces, none
+ * on portals, as the reference scanner.  The scan is brute force: its cost
+ * is n_tracks x n_surfaces root searches. */
+typedef enum dprop_scan_status {
+    DPROP_SCAN_OK = 0,
+    DPROP_SCAN_OVERFLOW = 1,  /* more intersections than capacity: n_hits
+                                 holds the number found, nothing is stored  */
+    DPROP_SCAN_EMPTY = 2      /* no intersection at all                     */
+} dprop_scan_status;
+
+typedef struct dprop_scan_results {
+    uint8_t* status;          /* [n] dprop_scan_status                         */
+    uint32_t* n_hits;         /* [n] intersections stored                      */
+    uint64_t* barcode;        /* [capacity * n]: hit k of track t at k * n + t */
+    void* path;               /* [capacity * n] path length along the helix    */
+    void* loc[2];             /* [capacity * n] each: bound local coordinates
+                                 of the hit; may be NULL                       */
+    uint16_t* volume_link;    /* [capacity * n]: volume behind the hit mask,
+                                 DPROP_INVALID_LINK leaves the world           */
+    uint32_t capacity;
+    uint32_t precision;       /* 4: float tracks and results, 8: double        */
+} dprop_scan_results;
+
+/* Device buffers (tracks in the precision of `results`), stream ordered. */
+dprop_status dprop_helix_scan(const dprop_detector* det, const double b[3],
+                              const dprop_tracks* tracks, uint64_t n_tracks,
+                              double mask_tolerance,
+                              const dprop_scan_results* results,
+                              void* stream);
+
+/* Navigation validation against the scan (the comparison of
+ * tests/include/detray/test/validation/navigation_validation_utils.hpp:
+ * 379-800, per track): `records` are the results of a propagation of the
+ * same tracks with record_all_surfaces = 1 (status, n_records, rec_barcode
+ * and rec_path used; rec_path in float for record_precision 4, double for
+ * 8; max_records its capacity).  A truth surface is missed if no record of
+ * it (for portals: of any portal - two portals coincide at a volume
+ * boundary and the navigator records one) lies within path_tolerance mm of
+ * its path; the truth's final world-exit portal counts as reached when the
+ * track exited.  A record is extra if no truth surface matches it. */
+typedef struct dprop_validation {
+    uint32_t* n_missed;   /* [n] truth surfaces the navigation missed        */
+    uint32_t* n_extra;    /* [n] recorded surfaces not on the helix          */
+} dprop_validation;
+
+dprop_status dprop_validate_navigation(const dprop_scan_results* truth,
+                                       const dprop_results* records,
+                                       uint32_t record_precision,
+                                       uint32_t max_records,
+                                       uint64_t n_tracks,
+                                       double path_tolerance,
+                                       const dprop_validation* out,
+                                       void* stream);
+
 /* ------------------------------------------------- allocation-free variant
  * dprop_propagate_noalloc has no counterpart in the reference.
  *

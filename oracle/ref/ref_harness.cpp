@@ -19,6 +19,11 @@
  *     the chain the reference's device tests use
  *     (tests/include/detray/test/device/propagator_test.hpp:84-93,114-168),
  *     writing the same result layout as dprop_propagate_host;
+ *   - ref_helix_scan: the reference's navigation-validation scan - every
+ *     surface intersected with the track's helix by its helix intersectors
+ *     (detector_scanner::run<helix_scan>, tests/include/detray/test/
+ *     validation/detector_scanner.hpp:52-140, restated here without its CSV
+ *     output dependencies);
  *   - ref_propagate_direct: the same chain with the direct_navigator
  *     (core/include/detray/navigation/direct_navigator.hpp) along given
  *     surface sequences, forward or backward, from free or bound starts.
@@ -32,7 +37,10 @@
 #include "detray/material/material_slab.hpp"
 #include "detray/material/predefined_materials.hpp"
 #include "detray/navigation/caching_navigator.hpp"
+#include "detray/navigation/detail/intersection_kernel.hpp"
 #include "detray/navigation/direct_navigator.hpp"
+#include "detray/navigation/intersector.hpp"
+#include "detray/tracks/helix.hpp"
 #include "detray/propagator/actor_chain.hpp"
 #include "detray/propagator/actors/aborters.hpp"
 #include "detray/propagator/actors/parameter_updater.hpp"
@@ -557,6 +565,101 @@ int propagate_direct_impl(const det_t& det, const oracle_field::field& field,
     return 0;
 }
 
+// ------------------------------------------------------------ helix scan
+template <typename det_t>
+int helix_scan_impl(const det_t& det, const double* bfield,
+                    const double* const* trk, uint64_t n, double mask_tol,
+                    uint32_t cap, uint8_t* status, uint32_t* n_hits,
+                    uint64_t* barcode, double* path, double* loc0,
+                    double* loc1, uint16_t* vlink, int n_threads) {
+    using surface_t = typename det_t::surface_type;
+    using intersection_t =
+        intersection2D<surface_t, algebra_t, intersection::contains_pos>;
+    using kernel_t = detail::intersection_initialize<intersector>;
+    using nav_link_t = typename surface_t::navigation_link;
+    const intersection::config icfg{
+        .min_mask_tolerance = static_cast<float>(mask_tol),
+        .max_mask_tolerance = static_cast<float>(mask_tol),
+        .mask_tolerance_scalor = 0.f,
+        .overstep_tolerance = 0.f};
+    const typename det_t::geometry_context ctx{};
+    const dvector3D<algebra_t> B{static_cast<scalar>(bfield[0]),
+                                 static_cast<scalar>(bfield[1]),
+                                 static_cast<scalar>(bfield[2])};
+    if (n_threads > 0) {
+        omp_set_num_threads(n_threads);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t ti = 0; ti < static_cast<int64_t>(n); ++ti) {
+        const auto t = static_cast<uint64_t>(ti);
+        const detail::helix<algebra_t> h(
+            {static_cast<scalar>(trk[0][t]), static_cast<scalar>(trk[1][t]),
+             static_cast<scalar>(trk[2][t])},
+            static_cast<scalar>(trk[3][t]),
+            {static_cast<scalar>(trk[4][t]), static_cast<scalar>(trk[5][t]),
+             static_cast<scalar>(trk[6][t])},
+            static_cast<scalar>(trk[7][t]), B);
+        std::vector<intersection_t> trace;
+        std::vector<intersection_t> found;
+        for (const auto& sf_desc : det.surfaces()) {
+            const auto sf = geometry::surface{det, sf_desc};
+            try {
+                sf.template visit_mask<kernel_t>(found, h, sf_desc,
+                                                 det.transform_store(), ctx,
+                                                 icfg, scalar{0});
+            } catch (const std::exception&) {
+                // the reference's root finder throws on a bracket it cannot
+                // close; such a surface gives no intersection here
+                found.clear();
+            }
+            for (auto& sfi : found) {
+                if (sfi.is_along()) {
+                    sfi.set_surface(sf_desc);
+                    trace.push_back(sfi);
+                }
+            }
+            found.clear();
+        }
+        if (trace.empty()) {
+            status[t] = DPROP_SCAN_EMPTY;
+            n_hits[t] = 0u;
+            continue;
+        }
+        std::stable_sort(trace.begin(), trace.end(),
+                         [](const intersection_t& a, const intersection_t& b) {
+                             return a < b;
+                         });
+        std::size_t kept = trace.size();
+        for (std::size_t k = 0; k < trace.size(); ++k) {
+            if (trace[k].volume_link() ==
+                detray::detail::invalid_value<nav_link_t>()) {
+                kept = k + 1u;
+                break;
+            }
+        }
+        if (kept > cap) {
+            status[t] = DPROP_SCAN_OVERFLOW;
+            n_hits[t] = static_cast<uint32_t>(kept);
+            continue;
+        }
+        status[t] = DPROP_SCAN_OK;
+        n_hits[t] = static_cast<uint32_t>(kept);
+        for (std::size_t k = 0; k < kept; ++k) {
+            const auto& is = trace[k];
+            const uint64_t o = static_cast<uint64_t>(k) * n + t;
+            barcode[o] = is.surface().identifier().value();
+            path[o] = static_cast<double>(is.path());
+            const auto sf = geometry::surface{det, is.surface()};
+            const auto p = h.pos(is.path());
+            const auto bl = sf.global_to_bound(ctx, p, h.dir(is.path()));
+            loc0[o] = static_cast<double>(bl[0]);
+            loc1[o] = static_cast<double>(bl[1]);
+            vlink[o] = static_cast<uint16_t>(is.volume_link());
+        }
+    }
+    return 0;
+}
+
 template <typename det_t>
 int dispatch(const det_t& det, const oracle_field::field& f,
              const dprop_config& cfg, const double* const trk[8], uint64_t n,
@@ -823,6 +926,40 @@ int ref_propagate_jac(void* handle, const ref_field_desc* fd,
                             with_abort_reasons, rec_jac);
         }
         g_error = "ref_propagate_jac: empty detector handle";
+        return 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+/// The reference's helix scan (navigation-validation truth) of every track
+/// (tracks: 8 arrays of n doubles) in the constant field b: per track the
+/// along-track intersections inside a mask, sorted by |path| and cut after
+/// the first world exit, slot-major [k * n + t] with capacity cap; status
+/// and n_hits as dprop_scan_results.
+int ref_helix_scan(void* handle, const double* b, const double* const* tracks,
+                   uint64_t n, double mask_tol, uint32_t cap, uint8_t* status,
+                   uint32_t* n_hits, uint64_t* barcode, double* path,
+                   double* loc0, double* loc1, uint16_t* vlink,
+                   int n_threads) {
+    try {
+        auto* h = static_cast<det_handle*>(handle);
+        auto go = [&](const auto& det) {
+            return helix_scan_impl(det, b, tracks, n, mask_tol, cap, status,
+                                   n_hits, barcode, path, loc0, loc1, vlink,
+                                   n_threads);
+        };
+        if (auto* toy = std::get_if<std::unique_ptr<toy_det_t>>(&h->det)) {
+            return go(**toy);
+        }
+        if (auto* tel = std::get_if<std::unique_ptr<tel_det_t>>(&h->det)) {
+            return go(**tel);
+        }
+        if (auto* wire = std::get_if<std::unique_ptr<wire_det_t>>(&h->det)) {
+            return go(**wire);
+        }
+        g_error = "ref_helix_scan: empty detector handle";
         return 1;
     } catch (const std::exception& e) {
         g_error = e.what();

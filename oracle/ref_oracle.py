@@ -97,6 +97,10 @@ def load(precision: str = "f64") -> C.CDLL:
         C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
         C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int,
         C.c_void_p, C.c_void_p, C.POINTER(abi.Results), C.c_int]
+    lib.ref_helix_scan.argtypes = [
+        C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_uint64, C.c_double,
+        C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+        C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     lib.ref_material_slab.argtypes = [C.c_char_p, C.c_double,
                                       C.POINTER(abi.SlabDesc),
                                       C.POINTER(C.c_double)]
@@ -367,6 +371,45 @@ def propagate_direct(det: RefDetector, field: dict, cfg: abi.Config,
         C.cast(sb_ptrs, C.c_void_p) if sb_ptrs is not None else None,
         C.byref(r), n_threads))
     del fkeep, keep
+    return res
+
+
+def alloc_scan(n: int, capacity: int) -> dict:
+    """Host arrays for a helix scan (oracle, host core)."""
+    return {
+        "status": np.full(n, 255, dtype=np.uint8),
+        "n_hits": np.zeros(n, dtype=np.uint32),
+        "barcode": np.zeros((capacity, n), dtype=np.uint64),
+        "path": np.zeros((capacity, n), dtype=np.float64),
+        "loc0": np.zeros((capacity, n), dtype=np.float64),
+        "loc1": np.zeros((capacity, n), dtype=np.float64),
+        "volume_link": np.zeros((capacity, n), dtype=np.uint16),
+    }
+
+
+def scan_pointers(res: dict) -> list:
+    return [res[k].ctypes.data for k in ("status", "n_hits", "barcode",
+                                         "path", "loc0", "loc1",
+                                         "volume_link")]
+
+
+def helix_scan(det: RefDetector, b, tracks: np.ndarray, mask_tol: float,
+               capacity: int = 256, n_threads: int = 0) -> dict:
+    """The reference's navigation-validation helix scan of ``tracks``
+    ((8, n) float64) in the constant field ``b``: per track the
+    intersections with all surfaces along the helix, sorted by path and cut
+    after the first world exit (slot-major, ``capacity`` slots)."""
+    lib = det._lib
+    trk = np.ascontiguousarray(tracks, dtype=np.float64)
+    n = trk.shape[1]
+    ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    bb = (C.c_double * 3)(*b)
+    res = alloc_scan(n, capacity)
+    if n_threads <= 0:
+        n_threads = os.cpu_count() or 1
+    _check(lib, lib.ref_helix_scan(det.handle, bb, C.cast(ptrs, C.c_void_p),
+                                   n, mask_tol, capacity,
+                                   *scan_pointers(res), n_threads))
     return res
 
 

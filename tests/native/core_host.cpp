@@ -13,6 +13,9 @@
 #include "core/config.hpp"
 #include "core/convert.hpp"
 #include "core/direct.cuh"
+#include "core/helix.cuh"
+
+#include <algorithm>
 
 using namespace dprop;
 
@@ -236,6 +239,88 @@ int core_host_propagate_direct(int precision_bytes,
     }
     return run<float>(desc, 0u, b, nullptr, nullptr, nullptr, nullptr, cfg,
                       trk, n, out, nullptr, nullptr, &da);
+}
+
+// Helix scan (dprop_helix_scan) with host double arrays, double precision;
+// outputs as ref_helix_scan.
+int core_host_helix_scan(const dprop_detector_desc* desc, const double* b,
+                         const double* const* trk, uint64_t n,
+                         double mask_tol, uint32_t cap, uint8_t* status,
+                         uint32_t* n_hits, uint64_t* barcode, double* path,
+                         double* loc0, double* loc1, uint16_t* vlink) {
+    const std::string problem = validate_desc(desc);
+    if (!problem.empty()) {
+        g_err = problem;
+        return 1;
+    }
+    const host_tables<double> tables = convert_desc<double>(desc);
+    const detector_view<double> det = tables.view();
+    const root_cfg<double> cfg{unit::um, 1000u, 5000.0 * unit::mm};
+    const vec3<double> bf{b[0], b[1], b[2]};
+    for (uint64_t t = 0; t < n; ++t) {
+        helix<double> h;
+        h.init(vec3<double>{trk[0][t], trk[1][t], trk[2][t]},
+               vec3<double>{trk[4][t], trk[5][t], trk[6][t]}, trk[7][t], bf);
+        std::vector<scan_hit<double>> hits;
+        for (uint32_t sf = 0; sf < det.n_surfaces; ++sf) {
+            helix_surface_hits(det, sf, h, mask_tol, cfg,
+                               [&](const scan_hit<double>& x) {
+                                   hits.push_back(x);
+                               });
+        }
+        if (hits.empty()) {
+            status[t] = DPROP_SCAN_EMPTY;
+            n_hits[t] = 0u;
+            continue;
+        }
+        std::stable_sort(hits.begin(), hits.end(),
+                         [](const scan_hit<double>& a,
+                            const scan_hit<double>& c) {
+                             return std::fabs(a.path) < std::fabs(c.path);
+                         });
+        size_t kept = hits.size();
+        for (size_t k = 0; k < hits.size(); ++k) {
+            if (hits[k].volume_link == static_cast<uint16_t>(k_invalid_link)) {
+                kept = k + 1u;
+                break;
+            }
+        }
+        n_hits[t] = static_cast<uint32_t>(kept);
+        if (kept > cap) {
+            status[t] = DPROP_SCAN_OVERFLOW;
+            continue;
+        }
+        status[t] = DPROP_SCAN_OK;
+        for (size_t k = 0; k < kept; ++k) {
+            const uint64_t o = static_cast<uint64_t>(k) * n + t;
+            barcode[o] = det.surfaces[hits[k].sf].barcode;
+            path[o] = hits[k].path;
+            loc0[o] = hits[k].loc0;
+            loc1[o] = hits[k].loc1;
+            vlink[o] = hits[k].volume_link;
+        }
+    }
+    return 0;
+}
+
+// Navigation validation (dprop_validate_navigation) on host arrays: scan
+// outputs as core_host_helix_scan, records as core_host_propagate (double).
+int core_host_validate(uint64_t n, const uint8_t* scan_status,
+                       const uint32_t* n_hits, const uint64_t* truth_bc,
+                       const double* truth_path, const uint16_t* truth_vlink,
+                       const uint8_t* rec_status, const uint32_t* n_records,
+                       const uint64_t* rec_bc, const double* rec_path,
+                       uint32_t max_records, double path_tol,
+                       uint32_t* n_missed, uint32_t* n_extra) {
+    for (uint64_t t = 0; t < n; ++t) {
+        const uint32_t nt = scan_status[t] == DPROP_SCAN_OK ? n_hits[t] : 0u;
+        const uint32_t nr =
+            n_records[t] < max_records ? n_records[t] : max_records;
+        compare_trace(truth_bc, truth_path, truth_vlink, nt, rec_bc, rec_path,
+                      nr, rec_status[t] == DPROP_TRK_EXITED, n, t, path_tol,
+                      n_missed[t], n_extra[t]);
+    }
+    return 0;
 }
 
 // Adjoint-mode propagation: as core_host_propagate, plus the tape

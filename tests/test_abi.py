@@ -65,6 +65,8 @@ STRUCTS = {
     "dprop_tape": abi.Tape,
     "dprop_gradients": abi.Gradients,
     "dprop_sequence": abi.Sequence,
+    "dprop_scan_results": abi.ScanResults,
+    "dprop_validation": abi.Validation,
 }
 
 
@@ -109,3 +111,7 @@ def test_argument_validation_without_device(lib):
                                None) == abi.DPROP_E_UNSUPPORTED
     assert lib.dprop_propagate_direct(None, None, None, None, None, None, 0,
                                       None) == abi.DPROP_E_INVALID
+    assert lib.dprop_helix_scan(None, None, None, 0, 0.0, None,
+                                None) == abi.DPROP_E_INVALID
+    assert lib.dprop_validate_navigation(None, None, 4, 0, 0, 0.1, None,
+                                         None) == abi.DPROP_E_INVALID
