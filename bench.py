@@ -64,6 +64,8 @@ def parse_args():
     p.add_argument("--no-adjoint", action="store_true",
                    help="skip the adjoint/forward cost measurement")
     p.add_argument("--adjoint-tracks", type=int, default=262_144)
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the direct-navigation and helix-scan rows")
     p.add_argument("--seed", type=int, default=20241203)
     return p.parse_args()
 
@@ -350,6 +352,74 @@ def host_threads() -> int:
 
 
 # ------------------------------------------------------------ our impl
+def extra_rows(cfg, det, field, trk, res, stream, dev, steps=5, warmup=2,
+               n_scan=16384):
+    """Throughput of the other propagation-path entry points on the same
+    workload: the direct navigator following the records of the main run
+    (the Kalman-filter fit step), and the helix truth scan with the
+    navigation validation of a propagation trace (n_scan tracks, every
+    surface of the detector per track)."""
+    import torch
+
+    from detray_b200 import abi, propagator
+    from detray_b200.units import T
+    n = trk.shape[1]
+
+    def timed(fn, k):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / k
+
+    seq = res.tensors["rec_barcode"]
+    lens = torch.clamp(res.tensors["n_records"], max=cfg.max_records)
+    out = propagator.alloc_device_results(n, cfg.max_records, dev)
+    ms_direct = timed(lambda: propagator.propagate_direct(
+        cfg, det, field, seq, lens, 1, tracks=trk, results=out,
+        stream=stream), steps)
+    same = bool(torch.equal(out.tensors["n_records"], res.tensors["n_records"]))
+    b = (0.0, 0.0, 2.0 * T)
+    sub64 = trk[:, :n_scan].double().contiguous()
+    sub32 = trk[:, :n_scan].contiguous()
+    ms_scan64 = timed(lambda: propagator.helix_scan(det, b, sub64, 1e-3,
+                                                    stream=stream), 3)
+    ms_scan32 = timed(lambda: propagator.helix_scan(det, b, sub32, 1e-3,
+                                                    stream=stream), 3)
+    vcfg = abi.make_config(max_records=64, search_window=(3, 3),
+                           use_material_interactor=0,
+                           estimate_scattering_noise=0, record_all_surfaces=1)
+    trace = propagator.propagate(vcfg, det, field, sub32, stream=stream)
+    truth = propagator.helix_scan(det, b, sub64, 1e-3, stream=stream)
+    missed, extra = propagator.validate_navigation(truth, trace,
+                                                   vcfg.max_records, 0.1,
+                                                   stream=stream)
+    torch.cuda.synchronize(dev)
+    good = float(((missed == 0) & (extra == 0)).float().mean().item())
+    return {
+        "direct_navigation": {
+            "value": n / (ms_direct / 1e3), "unit": UNIT,
+            "ms_per_step": round(ms_direct, 3),
+            "what": "dprop_propagate_direct forward along the records of the "
+                    "main run (same tracks, same actor chain)",
+            "same_record_counts": same},
+        "helix_scan": {
+            "fp64_tracks_per_s": n_scan / (ms_scan64 / 1e3),
+            "fp32_tracks_per_s": n_scan / (ms_scan32 / 1e3),
+            "ms_fp64": round(ms_scan64, 3), "ms_fp32": round(ms_scan32, 3),
+            "tracks": n_scan, "surfaces_per_track": int(det.n_surfaces),
+            "navigation_validation_clean_fraction": round(good, 5),
+            "what": "dprop_helix_scan (every surface per track) and "
+                    "dprop_validate_navigation of a no-material trace"},
+    }
+
+
 def run_ours(args):
     import torch
 
@@ -482,6 +552,10 @@ def run_ours(args):
     if not args.no_adjoint:
         adj = adjoint_cost(args, dev, stream, world, rank)
 
+    extras = None
+    if not args.no_extras:
+        extras = extra_rows(cfg, det, field, trk, res, stream, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -512,6 +586,7 @@ def run_ours(args):
                              "L2): inputs are re-read from HBM"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "adjoint": adj,
+            "other_entry_points": extras,
             # our kernels per step: the propagation kernel, plus the direction
             # key kernel when sorting (the radix sort itself is CUB's)
             "gpu_launches": args.steps * (1 + int(lc.sort_tracks)),

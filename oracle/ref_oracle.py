@@ -93,14 +93,6 @@ def load(precision: str = "f64") -> C.CDLL:
         C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
         C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(abi.Results), C.c_int,
         C.c_int, C.c_int, C.c_void_p]
-    lib.ref_propagate_direct.argtypes = [
-        C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
-        C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int,
-        C.c_void_p, C.c_void_p, C.POINTER(abi.Results), C.c_int]
-    lib.ref_helix_scan.argtypes = [
-        C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_uint64, C.c_double,
-        C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-        C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     lib.ref_material_slab.argtypes = [C.c_char_p, C.c_double,
                                       C.POINTER(abi.SlabDesc),
                                       C.POINTER(C.c_double)]
@@ -109,8 +101,24 @@ def load(precision: str = "f64") -> C.CDLL:
     lib.ref_field_eval.argtypes = [C.POINTER(RefFieldDesc),
                                    C.POINTER(C.c_double), C.c_uint64,
                                    C.POINTER(C.c_double)]
+    _optional_argtypes(lib)
     _LIBS[precision] = lib
     return lib
+
+
+def _optional_argtypes(lib) -> None:
+    """Entry points that a library built by an older recipe may lack."""
+    if not hasattr(lib, "ref_propagate_direct"):
+        return
+    lib.ref_propagate_direct.argtypes = [
+        C.c_void_p, C.POINTER(RefFieldDesc), C.POINTER(abi.Config),
+        C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int,
+        C.c_void_p, C.c_void_p, C.POINTER(abi.Results), C.c_int]
+    if hasattr(lib, "ref_helix_scan"):
+        lib.ref_helix_scan.argtypes = [
+            C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_uint64,
+            C.c_double, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
 
 
 class RefDetector:
