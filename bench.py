@@ -545,8 +545,9 @@ def run_ours(args):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(ms_e2e, 3), "steps": k_e2e,
                "records_per_step": n_rec,
-               "api": "dprop_propagate_host, jagged records, 2-stream "
-                      "chunked pipeline, pinned host buffers"}
+               "api": "dprop_propagate_host, jagged records, chunked "
+                      "pipeline (4 chunks on prioritized streams, records "
+                      "drained on a copy stream), pinned host buffers"}
 
     adj = None
     if not args.no_adjoint:

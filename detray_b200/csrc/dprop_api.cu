@@ -543,6 +543,15 @@ __global__ void clamp_counts_kernel(const uint32_t* __restrict__ n_rec,
     }
 }
 
+// Host pipeline shape: compute streams (chunks in flight) and the number of
+// chunks a batch is split into.
+#ifndef DPROP_PIPE_SLOTS
+#define DPROP_PIPE_SLOTS 4
+#endif
+#ifndef DPROP_PIPE_SPLIT
+#define DPROP_PIPE_SPLIT 4u
+#endif
+
 struct record_arrays {
     uint64_t* barcode;
     float* bound[6];
@@ -577,20 +586,45 @@ __global__ void pack_records_kernel(record_arrays src, record_arrays dst,
     }
 }
 
+// One pipeline slot: a compute stream (inputs in, sort, propagation, record
+// packing, per-track outputs out) and its device buffers.  The packed
+// records of all slots drain on one copy stream, in chunk order, so that the
+// next chunks' propagation does not queue behind the record copies.  At most
+// k_pipe_slots compute streams plus the copy stream stay within the device's
+// default eight hardware work queues, so that a copy does not wait behind an
+// unrelated kernel sharing its queue.
 struct pipe_slot {
     cudaStream_t stream{nullptr};
-    cudaEvent_t counted{nullptr};
+    cudaEvent_t counted{nullptr};   // packed records and offsets ready
+    cudaEvent_t drained{nullptr};   // packed records copied out
     void* dev{nullptr};
     size_t dev_bytes{0};
     uint32_t* host_offsets{nullptr};  // pinned, chunk + 1 entries
     size_t host_entries{0};
 };
-pipe_slot g_pipe[2];
+constexpr int k_pipe_slots = DPROP_PIPE_SLOTS;
+pipe_slot g_pipe[k_pipe_slots];
+cudaStream_t g_copy_stream = nullptr;
 
-dprop_status ensure_pipe(pipe_slot& ps, size_t dev_bytes, size_t chunk) {
+dprop_status ensure_pipe(pipe_slot& ps, int index, size_t dev_bytes,
+                         size_t chunk) {
     if (!ps.stream) {
-        DPROP_CUDA(cudaStreamCreateWithFlags(&ps.stream, cudaStreamNonBlocking));
+        // earlier chunks of a batch run at higher priority: the block
+        // scheduler finishes them first, so that their records start crossing
+        // PCIe early, while later chunks fill the SMs their tails leave idle
+        int least = 0, greatest = 0;
+        DPROP_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int prio = (greatest + index < least) ? greatest + index : least;
+        DPROP_CUDA(cudaStreamCreateWithPriority(&ps.stream,
+                                                cudaStreamNonBlocking, prio));
+        if (!g_copy_stream) {
+            DPROP_CUDA(cudaStreamCreateWithFlags(&g_copy_stream,
+                                                 cudaStreamNonBlocking));
+        }
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.counted, cudaEventDisableTiming));
+        DPROP_CUDA(cudaEventCreateWithFlags(&ps.drained, cudaEventDisableTiming));
+        // nothing to wait for before the first packing
+        DPROP_CUDA(cudaEventRecord(ps.drained, g_copy_stream));
     }
     if (ps.dev_bytes < dev_bytes) {
         if (ps.dev) {
@@ -613,6 +647,76 @@ dprop_status ensure_pipe(pipe_slot& ps, size_t dev_bytes, size_t chunk) {
     return DPROP_OK;
 }
 
+// device buffers of one slot (the same carving for every chunk)
+struct slot_buffers {
+    const double* trk[8];
+    dprop_results dr;
+    record_arrays slotm, packed;
+    uint32_t *counts, *offsets, *keys_in, *keys_out, *idx_in, *idx_out;
+    void* sort_tmp;
+    void* scan_tmp;
+};
+
+size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+
+slot_buffers carve_slot(void* base, uint64_t chunk, uint64_t rec_slot,
+                        bool with_cov, size_t sort_temp, size_t scan_temp) {
+    slot_buffers b{};
+    char* p = static_cast<char*>(base);
+    auto take = [&](size_t bytes) {
+        char* r = p;
+        p += al256(bytes);
+        return r;
+    };
+    for (int i = 0; i < 8; ++i) {
+        b.trk[i] = reinterpret_cast<double*>(take(chunk * sizeof(double)));
+    }
+    dprop_results& dr = b.dr;
+    dr.status = reinterpret_cast<uint8_t*>(take(chunk));
+    dr.n_records = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    dr.n_steps = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    dr.n_trials = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    dr.path_length = take(chunk * 4);
+    dr.n_intersections = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    dr.n_transports = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    dr.n_material = reinterpret_cast<uint32_t*>(take(chunk * 4));
+    for (int i = 0; i < 8; ++i) {
+        dr.final_free[i] = take(chunk * 4);
+    }
+    b.slotm.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
+    b.packed.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
+    for (int i = 0; i < 6; ++i) {
+        b.slotm.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+        b.packed.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
+    }
+    for (int i = 0; i < 21; ++i) {
+        float* a = reinterpret_cast<float*>(take(rec_slot * 4));
+        float* c = reinterpret_cast<float*>(take(rec_slot * 4));
+        if (with_cov) {
+            b.slotm.cov[i] = a;
+            b.packed.cov[i] = c;
+        }
+    }
+    b.slotm.path = reinterpret_cast<float*>(take(rec_slot * 4));
+    b.packed.path = reinterpret_cast<float*>(take(rec_slot * 4));
+    b.slotm.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
+    b.packed.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
+    dr.rec_barcode = b.slotm.barcode;
+    for (int i = 0; i < 6; ++i) dr.rec_bound[i] = b.slotm.bound[i];
+    for (int i = 0; i < 21; ++i) dr.rec_cov[i] = b.slotm.cov[i];
+    dr.rec_path = b.slotm.path;
+    dr.rec_flags = b.slotm.flags;
+    b.counts = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.offsets = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.keys_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.keys_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.idx_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.idx_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
+    b.sort_tmp = take(sort_temp);
+    b.scan_tmp = take(scan_temp);
+    return b;
+}
+
 dprop_status propagate_host_jagged(const dprop_config& c,
                                    const dprop_launch* lc,
                                    const dprop_detector* det,
@@ -620,7 +724,14 @@ dprop_status propagate_host_jagged(const dprop_config& c,
                                    const dprop_tracks& tracks,
                                    const dprop_results& out, uint64_t n) {
     const uint64_t cap = c.max_records;
-    const uint64_t chunk = n < 262144u ? n : 262144u;
+    // about k_pipe_slots chunks per batch, 32 Ki - 256 Ki tracks each
+    uint64_t chunk = ((n / DPROP_PIPE_SPLIT + 1023u) / 1024u) * 1024u;
+    chunk = chunk < 32768u ? 32768u : (chunk > 262144u ? 262144u : chunk);
+    chunk = n < chunk ? n : chunk;
+    const uint64_t n_chunks = (n + chunk - 1u) / chunk;
+    const int n_slots = n_chunks < static_cast<uint64_t>(k_pipe_slots)
+                            ? static_cast<int>(n_chunks)
+                            : k_pipe_slots;
     const prop_cfg<float> pcfg = make_prop_cfg<float>(c);
     const bool sort = (lc == nullptr) || lc->sort_tracks != 0u;
     const void* h_trk[8] = {tracks.pos[0], tracks.pos[1], tracks.pos[2],
@@ -630,6 +741,10 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         if (!h_trk[i]) {
             return fail(DPROP_E_INVALID, "propagate_host: missing track array");
         }
+    }
+    bool with_cov = false;
+    for (int i = 0; i < 21; ++i) {
+        with_cov = with_cov || out.rec_cov[i] != nullptr;
     }
 
     // device scratch layout of one pipeline slot
@@ -641,26 +756,29 @@ dprop_status propagate_host_jagged(const dprop_config& c,
     DPROP_CUDA(cub::DeviceScan::ExclusiveSum(
         nullptr, scan_temp, static_cast<const uint32_t*>(nullptr),
         static_cast<uint32_t*>(nullptr), static_cast<int>(chunk + 1)));
-    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t rec_slot = cap * chunk;
     size_t need = 0;
-    need += 8 * al(chunk * sizeof(double));                        // inputs
-    need += al(chunk) + 7 * al(chunk * 4) + 8 * al(chunk * 4);     // per-track
-    need += 2 * (al(rec_slot * 8) + 28 * al(rec_slot * 4) + al(rec_slot));
-    need += 6 * al((chunk + 1) * 4) + al(sort_temp) + al(scan_temp);
-    for (auto& ps : g_pipe) {
-        const dprop_status s = ensure_pipe(ps, need, chunk);
+    need += 8 * al256(chunk * sizeof(double));                        // inputs
+    need += al256(chunk) + 7 * al256(chunk * 4) + 8 * al256(chunk * 4);  // per-track
+    need += 2 * (al256(rec_slot * 8) + 28 * al256(rec_slot * 4) + al256(rec_slot));
+    need += 6 * al256((chunk + 1) * 4) + al256(sort_temp) + al256(scan_temp);
+    for (int k = 0; k < n_slots; ++k) {
+        const dprop_status s = ensure_pipe(g_pipe[k], k, need, chunk);
         if (s != DPROP_OK) {
             return s;
         }
     }
+    auto carve = [&](int sl) {
+        return carve_slot(g_pipe[sl].dev, chunk, rec_slot, with_cov, sort_temp,
+                          scan_temp);
+    };
     cudaEvent_t inputs_ready = nullptr;
     DPROP_CUDA(cudaEventCreateWithFlags(&inputs_ready, cudaEventDisableTiming));
     // make the pipeline streams wait for work already queued on the legacy
     // stream (e.g. the caller's uploads)
     DPROP_CUDA(cudaEventRecord(inputs_ready, 0));
-    for (auto& ps : g_pipe) {
-        DPROP_CUDA(cudaStreamWaitEvent(ps.stream, inputs_ready, 0));
+    for (int k = 0; k < n_slots; ++k) {
+        DPROP_CUDA(cudaStreamWaitEvent(g_pipe[k].stream, inputs_ready, 0));
     }
 
     struct chunk_info {
@@ -668,14 +786,12 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         uint64_t count;
         record_arrays packed;
     };
-    chunk_info prev{};
-    bool have_prev = false;
-    int prev_slot = 0;
     uint64_t rec_base = 0;
 
-    // copy a finished chunk's packed records into the caller's arrays
-    auto drain = [&](const chunk_info& ci, int slot) -> dprop_status {
-        pipe_slot& ps = g_pipe[slot];
+    // copy a finished chunk's packed records into the caller's arrays (on
+    // the copy stream; the host has seen the chunk's record count)
+    auto drain = [&](const chunk_info& ci, int sl) -> dprop_status {
+        pipe_slot& ps = g_pipe[sl];
         DPROP_CUDA(cudaEventSynchronize(ps.counted));
         const uint32_t total = ps.host_offsets[ci.count];
         for (uint64_t t = 0; t < ci.count; ++t) {
@@ -685,7 +801,8 @@ dprop_status propagate_host_jagged(const dprop_config& c,
             if (h && d && total) {
                 DPROP_CUDA(cudaMemcpyAsync(static_cast<char*>(h) + rec_base * elem,
                                            d, total * elem,
-                                           cudaMemcpyDeviceToHost, ps.stream));
+                                           cudaMemcpyDeviceToHost,
+                                           g_copy_stream));
             }
             return DPROP_OK;
         };
@@ -699,110 +816,65 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         }
         if ((s = d2h(out.rec_path, ci.packed.path, 4)) != DPROP_OK) return s;
         if ((s = d2h(out.rec_flags, ci.packed.flags, 1)) != DPROP_OK) return s;
+        DPROP_CUDA(cudaEventRecord(ps.drained, g_copy_stream));
         rec_base += total;
         return DPROP_OK;
     };
 
-    int slot = 0;
-    for (uint64_t begin = 0; begin < n; begin += chunk, slot ^= 1) {
-        const uint64_t m = (n - begin) < chunk ? (n - begin) : chunk;
-        pipe_slot& ps = g_pipe[slot];
-        cudaStream_t st = ps.stream;
-        char* p = static_cast<char*>(ps.dev);
-        auto take = [&](size_t b) {
-            char* r = p;
-            p += al(b);
-            return r;
-        };
-        // inputs
-        const double* d_trk[8];
+    // inputs in and direction sort of one chunk
+    auto stage_in = [&](uint64_t begin, uint64_t m, int sl) -> dprop_status {
+        const cudaStream_t st = g_pipe[sl].stream;
+        const slot_buffers b = carve(sl);
         for (int i = 0; i < 8; ++i) {
-            double* d = reinterpret_cast<double*>(take(chunk * sizeof(double)));
-            DPROP_CUDA(cudaMemcpyAsync(d, static_cast<const double*>(h_trk[i]) + begin,
+            DPROP_CUDA(cudaMemcpyAsync(const_cast<double*>(b.trk[i]),
+                                       static_cast<const double*>(h_trk[i]) + begin,
                                        m * sizeof(double), cudaMemcpyHostToDevice, st));
-            d_trk[i] = d;
         }
-        // per-track outputs and slot-major records (row stride m)
-        dprop_results dr{};
-        dr.status = reinterpret_cast<uint8_t*>(take(chunk));
-        dr.n_records = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        dr.n_steps = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        dr.n_trials = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        dr.path_length = take(chunk * 4);
-        dr.n_intersections = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        dr.n_transports = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        dr.n_material = reinterpret_cast<uint32_t*>(take(chunk * 4));
-        for (int i = 0; i < 8; ++i) {
-            dr.final_free[i] = take(chunk * 4);
-        }
-        record_arrays slotm{}, packed{};
-        slotm.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
-        packed.barcode = reinterpret_cast<uint64_t*>(take(rec_slot * 8));
-        for (int i = 0; i < 6; ++i) {
-            slotm.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
-            packed.bound[i] = reinterpret_cast<float*>(take(rec_slot * 4));
-        }
-        for (int i = 0; i < 21; ++i) {
-            if (out.rec_cov[i]) {
-                slotm.cov[i] = reinterpret_cast<float*>(take(rec_slot * 4));
-                packed.cov[i] = reinterpret_cast<float*>(take(rec_slot * 4));
-            } else {
-                take(rec_slot * 4);
-                take(rec_slot * 4);
-            }
-        }
-        slotm.path = reinterpret_cast<float*>(take(rec_slot * 4));
-        packed.path = reinterpret_cast<float*>(take(rec_slot * 4));
-        slotm.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
-        packed.flags = reinterpret_cast<uint8_t*>(take(rec_slot));
-        dr.rec_barcode = slotm.barcode;
-        for (int i = 0; i < 6; ++i) dr.rec_bound[i] = slotm.bound[i];
-        for (int i = 0; i < 21; ++i) dr.rec_cov[i] = slotm.cov[i];
-        dr.rec_path = slotm.path;
-        dr.rec_flags = slotm.flags;
-        uint32_t* counts = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        uint32_t* offsets = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        uint32_t* keys_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        uint32_t* keys_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        uint32_t* idx_in = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        uint32_t* idx_out = reinterpret_cast<uint32_t*>(take((chunk + 1) * 4));
-        void* sort_tmp = take(sort_temp);
-        void* scan_tmp = take(scan_temp);
-
-        dprop_tracks dt{};
-        for (int i = 0; i < 3; ++i) {
-            dt.pos[i] = d_trk[i];
-            dt.dir[i] = d_trk[4 + i];
-        }
-        dt.time = d_trk[3];
-        dt.qop = d_trk[7];
-        const io_ptrs<double> io = make_io<double>(dt, dr);
-        const uint32_t* order = nullptr;
         if (sort) {
             const unsigned int kg = static_cast<unsigned int>((m + 255) / 256);
             direction_key_kernel<double><<<kg, 256, 0, st>>>(
-                d_trk[4], d_trk[5], d_trk[6], d_trk[7], m, keys_in, idx_in);
+                b.trk[4], b.trk[5], b.trk[6], b.trk[7], m, b.keys_in, b.idx_in);
             size_t tb = sort_temp;
             DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
-                sort_tmp, tb, keys_in, keys_out, idx_in, idx_out,
+                b.sort_tmp, tb, b.keys_in, b.keys_out, b.idx_in, b.idx_out,
                 static_cast<int>(m), 0, 20, st));
-            order = idx_out;
         }
+        return DPROP_OK;
+    };
+
+    // propagation, record packing and per-track outputs of one chunk
+    auto stage_run = [&](uint64_t begin, uint64_t m, int sl) -> dprop_status {
+        pipe_slot& ps = g_pipe[sl];
+        const cudaStream_t st = ps.stream;
+        const slot_buffers b = carve(sl);
+        dprop_tracks dt{};
+        for (int i = 0; i < 3; ++i) {
+            dt.pos[i] = b.trk[i];
+            dt.dir[i] = b.trk[4 + i];
+        }
+        dt.time = b.trk[3];
+        dt.qop = b.trk[7];
+        const io_ptrs<double> io = make_io<double>(dt, b.dr);
         const unsigned int grid =
             static_cast<unsigned int>((m + k_plain_block - 1) / k_plain_block);
         launch_plain_mb<double, DPROP_MIN_BLOCKS>(grid, st, det, field->view,
-                                                  pcfg, io, m, order);
+                                                  pcfg, io, m,
+                                                  sort ? b.idx_out : nullptr);
         DPROP_CUDA(cudaGetLastError());
         // pack the records
         const unsigned int cg = static_cast<unsigned int>((m + 1 + 255) / 256);
-        clamp_counts_kernel<<<cg, 256, 0, st>>>(dr.n_records,
+        clamp_counts_kernel<<<cg, 256, 0, st>>>(b.dr.n_records,
                                                 static_cast<uint32_t>(cap),
-                                                static_cast<uint32_t>(m), counts);
+                                                static_cast<uint32_t>(m), b.counts);
         size_t sb = scan_temp;
-        DPROP_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, sb, counts, offsets,
+        DPROP_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, sb, b.counts,
+                                                 b.offsets,
                                                  static_cast<int>(m + 1), st));
+        // the packed buffers are free once the slot's last drain finished
+        DPROP_CUDA(cudaStreamWaitEvent(st, ps.drained, 0));
         const unsigned int pg = static_cast<unsigned int>((m + 127) / 128);
-        pack_records_kernel<<<pg, 128, 0, st>>>(slotm, packed, counts, offsets,
+        pack_records_kernel<<<pg, 128, 0, st>>>(b.slotm, b.packed, b.counts,
+                                                b.offsets,
                                                 static_cast<uint32_t>(m));
         DPROP_CUDA(cudaGetLastError());
         // per-track outputs and the offsets back to the host
@@ -813,6 +885,7 @@ dprop_status propagate_host_jagged(const dprop_config& c,
             }
             return DPROP_OK;
         };
+        const dprop_results& dr = b.dr;
         dprop_status s = DPROP_OK;
         if ((s = d2h(out.status, dr.status, 1)) != DPROP_OK) return s;
         if ((s = d2h(out.n_records, dr.n_records, 4)) != DPROP_OK) return s;
@@ -825,25 +898,60 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         for (int i = 0; i < 8; ++i) {
             if ((s = d2h(out.final_free[i], dr.final_free[i], 4)) != DPROP_OK) return s;
         }
-        DPROP_CUDA(cudaMemcpyAsync(ps.host_offsets, offsets, (m + 1) * 4,
+        DPROP_CUDA(cudaMemcpyAsync(ps.host_offsets, b.offsets, (m + 1) * 4,
                                    cudaMemcpyDeviceToHost, st));
         DPROP_CUDA(cudaEventRecord(ps.counted, st));
-        // drain the previous chunk while this one runs
-        if (have_prev) {
-            if ((s = drain(prev, prev_slot)) != DPROP_OK) return s;
+        return DPROP_OK;
+    };
+
+    // the chunk each slot still has to drain (drained in chunk order: the
+    // slots are used round robin)
+    chunk_info pending[k_pipe_slots] = {};
+    bool has_pending[k_pipe_slots] = {};
+    int slot = 0;
+    // waves of n_slots chunks: first every chunk's inputs and sort, then the
+    // propagation kernels, so that no sort waits behind a propagation kernel
+    // that holds the SMs' registers
+    const uint64_t wave = chunk * static_cast<uint64_t>(n_slots);
+    for (uint64_t w0 = 0; w0 < n; w0 += wave) {
+        const uint64_t w1 = (n - w0) < wave ? n : w0 + wave;
+        int sl = slot;
+        for (uint64_t begin = w0; begin < w1;
+             begin += chunk, sl = (sl + 1) % n_slots) {
+            const uint64_t m = (w1 - begin) < chunk ? (w1 - begin) : chunk;
+            if (has_pending[sl]) {
+                const dprop_status s = drain(pending[sl], sl);
+                if (s != DPROP_OK) return s;
+                has_pending[sl] = false;
+            }
+            const dprop_status s = stage_in(begin, m, sl);
+            if (s != DPROP_OK) return s;
         }
-        prev = chunk_info{begin, m, packed};
-        prev_slot = slot;
-        have_prev = true;
+        sl = slot;
+        for (uint64_t begin = w0; begin < w1;
+             begin += chunk, sl = (sl + 1) % n_slots) {
+            const uint64_t m = (w1 - begin) < chunk ? (w1 - begin) : chunk;
+            const dprop_status s = stage_run(begin, m, sl);
+            if (s != DPROP_OK) return s;
+            pending[sl] = chunk_info{begin, m, carve(sl).packed};
+            has_pending[sl] = true;
+        }
+        slot = sl;
     }
-    if (have_prev) {
-        const dprop_status s = drain(prev, prev_slot);
-        if (s != DPROP_OK) return s;
+    // drain what is left, oldest chunk first
+    for (int k = 0; k < n_slots; ++k) {
+        const int sl = (slot + k) % n_slots;
+        if (has_pending[sl]) {
+            const dprop_status s = drain(pending[sl], sl);
+            if (s != DPROP_OK) return s;
+            has_pending[sl] = false;
+        }
     }
     out.rec_offsets[n] = rec_base;
-    for (auto& ps : g_pipe) {
-        DPROP_CUDA(cudaStreamSynchronize(ps.stream));
+    for (int k = 0; k < n_slots; ++k) {
+        DPROP_CUDA(cudaStreamSynchronize(g_pipe[k].stream));
     }
+    DPROP_CUDA(cudaStreamSynchronize(g_copy_stream));
     cudaEventDestroy(inputs_ready);
     return DPROP_OK;
 }
