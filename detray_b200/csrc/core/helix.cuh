@@ -77,6 +77,28 @@ struct helix {
         d = d + (alpha * sin(ks)) * n0;
         return normalize(d);
     }
+    // position and direction at s from one sine/cosine pair (the same
+    // values as pos(s) and dir(s))
+    DPROP_HD void eval(S s, vec3<S>& p, vec3<S>& d) const {
+        if (straight) {
+            p = pos0 + s * h0;
+            d = t0;
+            return;
+        }
+        const S ks = K * s;
+        const S sn = sin(ks);
+        const S cs = cos(ks);
+        vec3<S> r = pos0;
+        r = r + (delta / K * (ks - sn)) * h0;
+        r = r + (sn / K) * t0;
+        r = r + (alpha / K * (S(1) - cs)) * n0;
+        p = r;
+        vec3<S> v{S(0), S(0), S(0)};
+        v = v + (delta * (S(1) - cs)) * h0;
+        v = v + cs * t0;
+        v = v + (alpha * sn) * n0;
+        d = normalize(v);
+    }
     DPROP_HD vec3<S> b_field() const { return B * h0; }
 };
 
@@ -246,8 +268,10 @@ DPROP_HD root_result<S> helix_plane(const helix<S>& h,
     const S denom = dot(sn, h.dir(S(0.5) * norm(dist)));
     const S s_ini = (denom == S(0)) ? norm(dist) : dot(sn, dist) / denom;
     auto fdf = [&h, &sn, &st](S x, S& f, S& df) {
-        f = dot(sn, h.pos(x) - st);
-        df = dot(sn, h.dir(x));
+        vec3<S> p, d;
+        h.eval(x, p, d);
+        f = dot(sn, p - st);
+        df = dot(sn, d);
     };
     return newton_safe(fdf, s_ini, cfg);
 }
@@ -277,9 +301,11 @@ DPROP_HD void helix_cylinder(const helix<S>& h, const dev_transform<S>& trf,
         guess[1] = -r;
     }
     auto fdf = [&h, &sz, &sc, r](S x, S& f, S& df) {
-        const vec3<S> crp = cross(h.pos(x) - sc, sz);
+        vec3<S> p, d;
+        h.eval(x, p, d);
+        const vec3<S> crp = cross(p - sc, sz);
         f = dot(crp, crp) - r * r;
-        df = S(2) * dot(crp, cross(h.dir(x), sz));
+        df = S(2) * dot(crp, cross(d, sz));
     };
     const S inv = limits<S>::max();
     out[0] = {inv, inv};
@@ -310,8 +336,8 @@ DPROP_HD root_result<S> helix_line(const helix<S>& h,
     const S s_ini = S(1) / denom * (Q - P * lt0);
     const vec3<S> bf = h.b_field();
     auto fdf = [&h, &c, &l, &bf](S x, S& f, S& df) {
-        const vec3<S> t = h.dir(x);
-        const vec3<S> p = h.pos(x);
+        vec3<S> t, p;
+        h.eval(x, p, t);
         const S A = dot(p - c, l);
         const vec3<S> w = p - (c + A * l);
         f = dot(t, w);
