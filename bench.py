@@ -66,6 +66,11 @@ def parse_args():
     p.add_argument("--adjoint-tracks", type=int, default=262_144)
     p.add_argument("--no-extras", action="store_true",
                    help="skip the direct-navigation and helix-scan rows")
+    p.add_argument("--sweep", action="store_true",
+                   help="measure the other benchmark configurations "
+                        "(telescope; toy in the solenoid map; toy + wire "
+                        "chamber in fp32 and fp64) instead of the headline "
+                        "line")
     p.add_argument("--seed", type=int, default=20241203)
     return p.parse_args()
 
@@ -691,8 +696,208 @@ def reference_gpu_row(args, cfg):
                       "records written"}
 
 
+# ------------------------------------------------ other configurations
+def _time_device(fn, dev, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / steps
+
+
+def _errors_vs_oracle(ref, got):
+    """Per-surface errors of a device run against the fp64 oracle over the
+    tracks whose surface sequences agree: max and 99th percentile of the
+    absolute differences of the bound parameters, and the covariance
+    difference relative to sqrt(C_ii C_jj)."""
+    import numpy as np
+    n = ref["status"].shape[0]
+    cap = ref["rec_barcode"].shape[0]
+    nr = np.minimum(ref["n_records"], cap)
+    ng = np.minimum(got["n_records"], cap)
+    same = nr == ng
+    k = np.arange(cap)[:, None]
+    valid = (k < nr[None, :]) & same[None, :]
+    valid &= ref["rec_barcode"] == got["rec_barcode"].astype(np.uint64)
+    seq_ok = np.all(valid | (k >= nr[None, :]), axis=0) & same
+    m = valid & seq_ok[None, :] & ((ref["rec_flags"] & 1) != 0)
+    out = {"tracks": int(n), "same_sequence": float(seq_ok.mean())}
+    names = ["loc0", "loc1", "phi", "theta", "qop", "time"]
+    for i, nm in enumerate(names):
+        d = np.abs(ref["rec_bound"][i][m] - got["rec_bound"][i][m])
+        out[nm] = {"max": float(d.max()) if d.size else 0.0,
+                   "p99": float(np.percentile(d, 99)) if d.size else 0.0}
+    diag = [0, 6, 11, 15, 18, 20]
+    worst = 0.0
+    c = 0
+    for i in range(6):
+        for j in range(i, 6):
+            ci = np.abs(ref["rec_cov"][diag[i]][m])
+            cj = np.abs(ref["rec_cov"][diag[j]][m])
+            den = np.sqrt(ci * cj)
+            ok = den > 0
+            d = np.abs(ref["rec_cov"][c][m] - got["rec_cov"][c][m])[ok] / den[ok]
+            if d.size:
+                worst = max(worst, float(d.max()))
+            c += 1
+    out["cov_rel_max"] = worst
+    return out
+
+
+def run_sweep(args):
+    """The other benchmark configurations, one JSON object per
+    configuration (the headline line is the default run):
+    1. telescope, 10 000 muons at pT 10 GeV within 10 deg of +x, 2 T, fp32:
+       GPU against the reference CPU propagator on the same tracks;
+    3. toy detector in the solenoid field map, 4 M muons pT 0.1-100 GeV:
+       plain and persistent kernels and the autotuned launch under a graph;
+    5. toy detector and wire chamber in the solenoid map, 16 M muons
+       (eta in [-4, 4], pT 0.1-100 GeV) in batches: fp32 and fp64 builds,
+       tracks/s and the per-surface errors against the fp64 oracle on a
+       sample."""
+    import numpy as np
+    import torch
+
+    from detray_b200 import abi, fields, flops, geometry, propagator, tracks
+    from detray_b200.units import T
+    from oracle import ref_oracle
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak32 = flops.nominal_fp32_tflops(sm, 1965.0)
+    rows = []
+    clocks = ClockSampler(0)
+    clocks.start()
+
+    def host(res):
+        out = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+        out["rec_barcode"] = out["rec_barcode"].view(np.uint64)
+        return out
+
+    # ---- config 1: telescope
+    det = propagator.Detector(geometry.load_geometry("telescope_10x1m_300um"))
+    field = propagator.Field.constant((0.0, 0.0, 2.0 * T))
+    cfg = abi.make_config(max_records=16)
+    trk = tracks.telescope_tracks(10_000, seed=args.seed)
+    dt = torch.tensor(trk, dtype=torch.float32, device=dev)
+    res = propagator.alloc_device_results(dt.shape[1], cfg.max_records, dev)
+    lc = propagator.make_launch(sort_tracks=1, use_graph=1)
+    ms = _time_device(lambda: propagator.propagate(
+        cfg, det, field, dt, results=res, launch=lc), dev, 50, 5)
+    cpu = None
+    if ref_oracle.available("f32"):
+        rdet = ref_oracle.build_telescope(precision="f32")
+        ref_oracle.propagate(rdet, field.spec, cfg, trk[:, :1000],
+                             n_threads=host_threads(), abort_reasons=False)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            ref_oracle.propagate(rdet, field.spec, cfg, trk,
+                                 n_threads=host_threads(),
+                                 abort_reasons=False)
+        cpu = trk.shape[1] * 5 / (time.perf_counter() - t0)
+    rows.append({"config": 1, "workload": "telescope_10x1m_300um_const2T_"
+                 "10k_muons_pt10_cone10", "gpu_tracks_per_s":
+                 trk.shape[1] / (ms / 1e3), "gpu_ms": round(ms, 4),
+                 "cpu_reference_tracks_per_s": cpu,
+                 "cpu_threads": host_threads(), "dtype": "f32"})
+
+    # ---- config 3: toy in the solenoid map, plain vs persistent vs tuned
+    fmap = fields.solenoid_map()
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
+    field = propagator.Field.grid(fmap, 0)
+    cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                          estimate_scattering_noise=0)
+    n3 = 4_000_000
+    trk = tracks.toy_tracks(n3, seed=args.seed + 3, pt_range=(0.1, 100.0))
+    dt = torch.tensor(trk, dtype=torch.float32, device=dev)
+    res = propagator.alloc_device_results(n3, cfg.max_records, dev)
+    forms = {}
+    for name, lc in (("plain_unsorted", propagator.make_launch(
+                         method=abi.METHOD_PLAIN, sort_tracks=0)),
+                     ("persistent_sorted", propagator.make_launch(
+                         method=abi.METHOD_PERSISTENT, sort_tracks=1))):
+        forms[name] = _time_device(lambda lc=lc: propagator.propagate(
+            cfg, det, field, dt, results=res, launch=lc), dev, 3, 1)
+    lc, _ = propagator.autotune(cfg, det, field, dt, use_graph=1)
+    forms["autotuned_graph"] = _time_device(lambda: propagator.propagate(
+        cfg, det, field, dt, results=res, launch=lc), dev, 3, 1)
+    rows.append({"config": 3, "workload": "toy_4brl_7edc_solenoid_map_4M_"
+                 "muons_pt0.1-100", "ms": {k: round(v, 3)
+                                            for k, v in forms.items()},
+                 "tracks_per_s": {k: n3 / (v / 1e3)
+                                  for k, v in forms.items()},
+                 "autotuned": {"method": int(lc.method),
+                               "ctas_per_sm": int(lc.ctas_per_sm),
+                               "sort_tracks": int(lc.sort_tracks)},
+                 "dtype": "f32"})
+    del res, dt
+
+    # ---- config 5: toy + wire chamber, fp32 and fp64, 16 M tracks
+    cfg = abi.make_config(max_records=48, search_window=(3, 3),
+                          estimate_scattering_noise=0)
+    per_det = {"toy_4brl_7edc": lambda: ref_oracle.build_toy(),
+               "wire_chamber_10l_cells":
+                   lambda: ref_oracle.build_wire_chamber(square_cells=True)}
+    n5 = 8_000_000
+    batch = 2_000_000
+    sweep = {}
+    for name, build_ref in per_det.items():
+        det = propagator.Detector(geometry.load_geometry(name))
+        for prec, dtype in ((4, torch.float32), (8, torch.float64)):
+            lc = propagator.make_launch(sort_tracks=1, precision=prec)
+            res = propagator.alloc_device_results(batch, cfg.max_records, dev,
+                                                  dtype=dtype)
+            total_ms = 0.0
+            fl = 0.0
+            for b0 in range(0, n5, batch):
+                trk = tracks.toy_tracks(batch, seed=args.seed + 50 + b0,
+                                        pt_range=(0.1, 100.0))
+                dt = torch.tensor(trk, dtype=dtype, device=dev)
+                total_ms += _time_device(lambda: propagator.propagate(
+                    cfg, det, field, dt, results=res, launch=lc), dev, 1,
+                    1 if b0 == 0 else 0)
+                t = res.tensors
+                fl += flops.algorithmic_flops(
+                    t["n_trials"].cpu().numpy(), t["n_steps"].cpu().numpy(),
+                    t["n_intersections"].cpu().numpy(),
+                    t["n_transports"].cpu().numpy(),
+                    t["n_material"].cpu().numpy())
+            peak = peak32 if prec == 4 else peak32 / 2.0
+            key = f"{name}_fp{8 * prec}"
+            sweep[key] = {"tracks": n5, "ms": round(total_ms, 2),
+                          "tracks_per_s": n5 / (total_ms / 1e3),
+                          "achieved_tflops": fl / (total_ms / 1e3) / 1e12,
+                          "roofline_frac": fl / (total_ms / 1e3) / 1e12 / peak,
+                          "peak_source": "nominal FP32" if prec == 4 else
+                                         "nominal FP64 = FP32 / 2"}
+            # per-surface errors against the fp64 oracle on a sample
+            sample = tracks.toy_tracks(3000, seed=args.seed + 99,
+                                       pt_range=(0.1, 100.0))
+            ref = ref_oracle.propagate(build_ref(), field.spec, cfg, sample)
+            got = host(propagator.propagate(
+                cfg, det, field,
+                torch.tensor(sample, dtype=dtype, device=dev), launch=lc))
+            sweep[key]["errors_vs_fp64_oracle"] = _errors_vs_oracle(ref, got)
+            del res
+    rows.append({"config": 5, "workload": "toy_4brl_7edc + "
+                 "wire_chamber_10l_cells, solenoid map, 2 x 8M muons "
+                 "eta -4..4 pT 0.1-100", "results": sweep})
+    clk = clocks.stop()
+    print(json.dumps({"sweep": rows, "clocks": clk}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.sweep:
+        run_sweep(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
