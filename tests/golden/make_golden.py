@@ -6,6 +6,8 @@ are committed so the tests do not need it):
                   tests/unit_tests/cpu/material/bethe_equation.cpp (the
                   instantiations that are commented out there are skipped:
                   the reference does not meet its 5 % bound on them).
+  telescope_smoke.npz  the surface sequence of the smoke test's telescope
+                  sample from the reference propagator.
   json_telescope/ the reference's JSON writer output for the 10-plane
                   telescope (geometry + homogeneous material) and
                   tables.npz, dprop::flatten of what the reference's JSON
@@ -55,6 +57,28 @@ def main(argv=None):
     (HERE / "bethe_pdg.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(f"bethe_pdg.json: {len(cases)} cases")
     json_fixture(HERE / "json_telescope")
+    smoke_fixture(HERE / "telescope_smoke.npz")
+
+
+def smoke_fixture(out: Path) -> None:
+    """Surface sequence of the smoke test's telescope sample (256 muons,
+    seed 7, 2 T) from the reference propagator: __graft_entry__.smoke()
+    checks against it where the oracle library is not built."""
+    import numpy as np
+    sys.path.insert(0, str(HERE.parent.parent))
+    from oracle import ref_oracle
+    from detray_b200 import abi, tracks
+    from detray_b200.units import T
+    if not ref_oracle.available("f64"):
+        print("oracle not built: smoke fixture not written")
+        return
+    cfg = abi.make_config(max_records=16)
+    trk = tracks.telescope_tracks(256, seed=7)
+    ref = ref_oracle.propagate(ref_oracle.build_telescope(),
+                               {"kind": "const", "b": (0.0, 0.0, 2.0 * T)},
+                               cfg, trk)
+    np.savez_compressed(out, rec_barcode=ref["rec_barcode"][:10])
+    print(f"{out.name}: {ref['rec_barcode'][:10].shape}")
 
 
 def json_fixture(out: Path) -> None:

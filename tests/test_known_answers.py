@@ -90,3 +90,21 @@ def test_stopping_power_derivative_sign():
         if len(pts) >= 2 and pts[0][0] < 0.2 and pts[1][0] < 2.0:
             assert pts[0][1] > pts[1][1], mat
     assert np.isfinite([c["dedx_mev_cm2_per_g"] for c in _cases()]).all()
+
+
+def test_smoke_fixture_matches_oracle(oracle):
+    """The committed surface sequence the smoke check falls back on is the
+    reference propagator's for the smoke sample."""
+    from pathlib import Path
+
+    import numpy as np
+
+    from detray_b200 import abi, tracks
+    from detray_b200.units import T
+    gold = np.load(Path(__file__).resolve().parent / "golden" /
+                   "telescope_smoke.npz")["rec_barcode"]
+    ref = oracle.propagate(oracle.build_telescope(),
+                           {"kind": "const", "b": (0.0, 0.0, 2.0 * T)},
+                           abi.make_config(max_records=16),
+                           tracks.telescope_tracks(256, seed=7))
+    assert np.array_equal(ref["rec_barcode"][:10], gold)
