@@ -856,6 +856,7 @@ def run_sweep(args):
                                                   dtype=dtype)
             total_ms = 0.0
             fl = 0.0
+            status = np.zeros(8, dtype=np.int64)
             for b0 in range(0, n5, batch):
                 trk = tracks.toy_tracks(batch, seed=args.seed + 50 + b0,
                                         pt_range=(0.1, 100.0))
@@ -869,6 +870,8 @@ def run_sweep(args):
                     t["n_intersections"].cpu().numpy(),
                     t["n_transports"].cpu().numpy(),
                     t["n_material"].cpu().numpy())
+                status += np.bincount(t["status"].cpu().numpy(),
+                                      minlength=8)[:8]
             peak = peak32 if prec == 4 else peak32 / 2.0
             key = f"{name}_fp{8 * prec}"
             sweep[key] = {"tracks": n5, "ms": round(total_ms, 2),
@@ -876,7 +879,14 @@ def run_sweep(args):
                           "achieved_tflops": fl / (total_ms / 1e3) / 1e12,
                           "roofline_frac": fl / (total_ms / 1e3) / 1e12 / peak,
                           "peak_source": "nominal FP32" if prec == 4 else
-                                         "nominal FP64 = FP32 / 2"}
+                                         "nominal FP64 = FP32 / 2",
+                          "status_counts": {
+                              nm: int(status[c]) for nm, c in (
+                                  ("exited", abi.TRK_EXITED),
+                                  ("path_limit", abi.TRK_PATH_LIMIT),
+                                  ("stalled", abi.TRK_STALLED),
+                                  ("no_surface", abi.TRK_NO_SURFACE),
+                                  ("max_iterations", abi.TRK_MAX_ITER))}}
             # per-surface errors against the fp64 oracle on a sample
             sample = tracks.toy_tracks(3000, seed=args.seed + 99,
                                        pt_range=(0.1, 100.0))

@@ -22,6 +22,7 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "_lib" / "libdetray_b200.so"
 CORE_HOST = REPO / "tests" / "native" / "libcore_host.so"
+CORE_HOST_STEPPED = REPO / "tests" / "native" / "libcore_host_stepped.so"
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
               "--expt-relaxed-constexpr"]
@@ -84,16 +85,22 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
-def build_core_host(force: bool = False) -> Path:
+def build_core_host(force: bool = False, stepped: bool = False) -> Path:
+    """Host build of the core for the tests.  stepped: built with
+    DPROP_NO_CYCLE_SKIP, so that exact cycles are stepped out to the path
+    limit as the reference does instead of being skipped."""
     src = REPO / "tests" / "native" / "core_host.cpp"
-    if not force and _newer(CORE_HOST, [src] + _sources()):
-        return CORE_HOST
+    out = CORE_HOST_STEPPED if stepped else CORE_HOST
+    if not force and _newer(out, [src] + _sources()):
+        return out
     cuda_inc = Path(nvcc()).resolve().parent.parent / "include"
     cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared",
            f"-I{REPO / 'include'}", f"-I{CSRC}", f"-I{cuda_inc}", str(src),
-           "-o", str(CORE_HOST)]
+           "-o", str(out)]
+    if stepped:
+        cmd.insert(1, "-DDPROP_NO_CYCLE_SKIP")
     subprocess.run(cmd, check=True)
-    return CORE_HOST
+    return out
 
 
 def build_oracle(ref: Path | None = None) -> bool:

@@ -9,6 +9,8 @@
 // stepper_rk_policy (navigation/policies.hpp:98-139).
 #pragma once
 
+#include <cstring>
+
 #include "adjoint.cuh"
 
 namespace dprop {
@@ -265,6 +267,119 @@ DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
     }
 }
 
+// 32-bit key of the exact bit pattern of the free state (position,
+// direction, q/p): equal states give equal keys; different ones almost
+// never do.
+DPROP_HD uint32_t scalar_bits(float v) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(v);
+#else
+    uint32_t u;
+    memcpy(&u, &v, sizeof(u));
+    return u;
+#endif
+}
+DPROP_HD uint32_t scalar_bits(double v) {
+#if defined(__CUDA_ARCH__)
+    const uint64_t u = static_cast<uint64_t>(__double_as_longlong(v));
+#else
+    uint64_t u;
+    memcpy(&u, &v, sizeof(u));
+#endif
+    return static_cast<uint32_t>(u) ^ static_cast<uint32_t>(u >> 32);
+}
+template <typename S>
+DPROP_HD uint32_t state_key(const step_state<S>& st) {
+    uint32_t h = scalar_bits(st.pos.x);
+    h = h * 0x9e3779b1u ^ scalar_bits(st.pos.y);
+    h = h * 0x9e3779b1u ^ scalar_bits(st.pos.z);
+    h = h * 0x85ebca6bu ^ scalar_bits(st.dir.x);
+    h = h * 0x85ebca6bu ^ scalar_bits(st.dir.y);
+    h = h * 0x85ebca6bu ^ scalar_bits(st.dir.z);
+    return h * 0xc2b2ae35u ^ scalar_bits(st.qop);
+}
+
+// Exact cycles of the stepping (not in the reference).  A looper whose
+// turning point lies a fraction of a um inside a portal cylinder, or which
+// grazes a wire cell, can see its target a um or two ahead, step past the
+// apex, see it behind and step back, every step longer than the on-surface
+// tolerance.  In single precision the state then repeats bit for bit with a
+// period of a few steps; the progress check passes on every forward step and
+// the reference keeps stepping the cycle until the path-limit aborter ends
+// it (millions of steps for the last metre).  The search finds such a cycle
+// with Brent's algorithm over state keys, confirms it by meeting the same
+// point three times at the same period, and then advances the absolute path,
+// the signed path and the time by the whole cycles that still fit below the
+// path limit, less one.  The track then runs its last cycles normally and the
+// path-limit aborter ends it as in the reference: same status, position,
+// direction and momentum, accumulated paths and time up to rounding.  Only
+// n_steps / n_trials stay short of the reference's counts.
+template <typename S>
+struct cycle_search {
+    static constexpr uint32_t k_done = 0xffffffffu;
+    uint32_t key = 0u;     // state_key of the saved point
+    uint32_t lam = 0u;     // steps since the point was saved or last met
+    uint32_t power = 1u;   // Brent's window: the saved point moves after it
+    uint32_t period = 0u;  // steps between the last two meetings
+    uint32_t hits = 0u;    // meetings in a row at that period, or k_done
+    double abs0 = 0.;      // accumulators at the last visit of the point
+    double path0 = 0.;
+    S time0 = S(0);
+
+    DPROP_HD void save(const step_state<S>& st) {
+        abs0 = st.abs_path_length;
+        path0 = st.path_length;
+        time0 = st.time;
+        lam = 0u;
+    }
+};
+
+// Called after every step.  Built with DPROP_NO_CYCLE_SKIP it does nothing
+// and every cycle is stepped out as the reference does (the test build that
+// checks the two agree).
+template <typename S>
+DPROP_HD void skip_cycles(cycle_search<S>& c, step_state<S>& st,
+                          S path_limit) {
+#if defined(DPROP_NO_CYCLE_SKIP)
+    return;
+#endif
+    // Only the states after steps shorter than 1 mm take part: the states
+    // of a cycle that has such a step repeat with it, so it is still found,
+    // and a cycle of longer steps reaches the path limit within a few
+    // thousand steps anyway.  Ordinary steps pay one comparison.
+    if (!(fabs(st.step_size) < S(1)) || c.hits == cycle_search<S>::k_done) {
+        return;
+    }
+    const uint32_t key = state_key(st);
+    ++c.lam;
+    if (key == c.key) {
+        c.hits = (c.lam == c.period) ? c.hits + 1u : 1u;
+        c.period = c.lam;
+        if (c.hits < 3u) {
+            c.save(st);
+            return;
+        }
+        const double d_abs = st.abs_path_length - c.abs0;
+        const double rest =
+            static_cast<double>(path_limit) - st.abs_path_length;
+        const double k = floor(rest / d_abs) - 1.0;
+        if (d_abs > 0. && k >= 1.0) {
+            st.abs_path_length += k * d_abs;
+            st.path_length += k * (st.path_length - c.path0);
+            st.time += static_cast<S>(k) * (st.time - c.time0);
+        }
+        c.hits = cycle_search<S>::k_done;
+        return;
+    }
+    if (c.lam == c.power) {
+        c.key = key;
+        c.power = c.power < 0x40000000u ? 2u * c.power : c.power;
+        c.period = 0u;
+        c.hits = 0u;
+        c.save(st);
+    }
+}
+
 // The caching navigator as the loop's navigation policy
 // (navigator_base::init / update, navigation/navigator_base.hpp:56-154).
 struct caching_navigation {
@@ -296,6 +411,7 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
     bool is_init = true;
     double path_prev = 0.;
     uint32_t stall = 0u;
+    cycle_search<S> cyc;
     uint32_t i = 0u;
     bool out_of_budget = false;
     for (; (i % 2u == 0u) || ts.heartbeat; ++i) {
@@ -336,6 +452,7 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
             } else {
                 stall = 0u;
             }
+            skip_cycles(cyc, st, cfg.act.path_limit);
         }
         is_init = navigator.update(nav, det, track_view<S>{st.pos, st.dir},
                                    cfg.nav) ||

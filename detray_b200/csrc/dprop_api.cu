@@ -463,11 +463,16 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     graph_entry e;
     e.key = key;
     const size_t sort_bytes = sort ? sort_scratch_bytes(n) : 0;
-    DPROP_CUDA(cudaMalloc(&e.scratch, sort_bytes + 256));
+    // The radix sort's temporary size carries the sort's alignment padding
+    // and is usually odd: the work-queue counter after it goes to the next
+    // 256-byte boundary (an atomic on an unaligned word is a device fault).
+    const size_t queue_offset = (sort_bytes + 255) & ~size_t(255);
+    DPROP_CUDA(cudaMalloc(&e.scratch, queue_offset + 256));
     launch_scratch scr{};
     scr.sort = e.scratch;
     scr.sort_bytes = sort_bytes;
-    scr.queue = reinterpret_cast<unsigned int*>(static_cast<char*>(e.scratch) + sort_bytes);
+    scr.queue = reinterpret_cast<unsigned int*>(static_cast<char*>(e.scratch) +
+                                                queue_offset);
     cudaStream_t cap = nullptr;
     DPROP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;

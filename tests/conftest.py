@@ -32,3 +32,15 @@ def core_host():
     lib = C.CDLL(str(lib_path))
     lib.core_host_last_error.restype = C.c_char_p
     return lib
+
+
+@pytest.fixture(scope="session")
+def core_host_stepped():
+    """The same host build with DPROP_NO_CYCLE_SKIP: exact stepping cycles
+    run to the path limit step by step, as in the reference."""
+    import ctypes as C
+    from detray_b200 import build
+    lib_path = build.build_core_host(stepped=True)
+    lib = C.CDLL(str(lib_path))
+    lib.core_host_last_error.restype = C.c_char_p
+    return lib
