@@ -452,7 +452,14 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
             } else {
                 stall = 0u;
             }
-            skip_cycles(cyc, st, cfg.act.path_limit);
+            // Built into the kernels for detectors with wire surfaces, whose
+            // low-pT loopers meet such cycles (about 1 track in 4 000 in the
+            // wire chamber, in the solenoid map).  None occurred in 8 M
+            // tracks of the toy detector, where the search costs 3-4 % of
+            // the propagation time.
+            if constexpr (W) {
+                skip_cycles(cyc, st, cfg.act.path_limit);
+            }
         }
         is_init = navigator.update(nav, det, track_view<S>{st.pos, st.dir},
                                    cfg.nav) ||
