@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-DPROP_ABI_VERSION = 1
+DPROP_ABI_VERSION = 2
 DPROP_INVALID_INDEX = 0xFFFFFFFF
 DPROP_INVALID_LINK = 0xFFFF
 
@@ -267,6 +267,10 @@ class Launch(C.Structure):
         ("sort_tracks", C.c_uint32),
         ("use_graph", C.c_uint32),
         ("precision", C.c_uint32),
+        ("steps_per_round", C.c_uint32),
+        ("rounds", C.c_uint32),
+        ("yield_lanes", C.c_uint32),
+        ("surface_phase", C.c_uint32),
         ("reserved", C.c_uint32 * 2),
     ]
 

@@ -36,8 +36,8 @@ def _newer(target: Path, sources) -> bool:
 
 
 # translation units of the library, compiled in parallel
-UNITS = ["dprop_api.cu", "adjoint_api.cu", "fp64_api.cu", "direct_api.cu",
-         "scan_api.cu"]
+UNITS = ["dprop_api.cu", "rounds_api.cu", "adjoint_api.cu", "fp64_api.cu",
+         "direct_api.cu", "scan_api.cu"]
 
 
 def _headers():

@@ -23,8 +23,10 @@ struct host_tables {
     std::vector<dev_grid<S>> grids;
     std::vector<uint32_t> grid_bins;
 
-    detector_view<S> view() const {
-        detector_view<S> v;
+    detector_view<S> view() const { return view_as<true>(); }
+    template <bool W>
+    detector_view<S, W> view_as() const {
+        detector_view<S, W> v;
         v.volumes = volumes.data();
         v.surfaces = surfaces.data();
         v.masks = masks.data();

@@ -225,15 +225,11 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
     }
 }
 
-// Run the actor chain once (propagator.hpp:308).
-template <typename S, bool W, typename Tape>
-DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
-                         const field_view<S>& field, const prop_cfg<S>& cfg,
-                         record_sink<S>& rec, const Tape& tape) {
+// pathlimit_aborter (aborters.hpp:23-76): the first actor of the chain.
+template <typename S>
+DPROP_HD void path_limit_aborter(track_state<S>& ts, const prop_cfg<S>& cfg) {
     step_state<S>& st = ts.step;
     nav_state<S>& nav = ts.nav;
-
-    // pathlimit_aborter
     if (!nav.finished()) {
         const S step_limit =
             cfg.act.path_limit - static_cast<S>(fabs(st.abs_path_length));
@@ -243,8 +239,16 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
         }
         st.constraint = min_(st.constraint, fabs(step_limit));
     }
+}
+
+// Run the actor chain once (propagator.hpp:308).
+template <typename S, bool W, typename Tape>
+DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
+                         const field_view<S>& field, const prop_cfg<S>& cfg,
+                         record_sink<S>& rec, const Tape& tape) {
+    path_limit_aborter(ts, cfg);
     // parameter_transporter and observers only act on surfaces
-    if (nav.is_on_surface()) {
+    if (ts.nav.is_on_surface()) {
         run_surface_actors(ts, det, field, cfg, rec, tape);
     }
 }
@@ -395,6 +399,30 @@ struct caching_navigation {
     }
 };
 
+// dprop_track_status code of a track whose propagation loop has ended
+// (propagator.hpp:389-399 and the abort reasons).
+template <typename S>
+DPROP_HD uint8_t track_status(const track_state<S>& ts, bool out_of_budget) {
+    const nav_state<S>& nav = ts.nav;
+    if (out_of_budget) {
+        return 4u;  // DPROP_TRK_MAX_ITER
+    }
+    const bool paused = !ts.heartbeat && nav.is_alive();
+    if (nav.finished() || paused) {
+        return 0u;  // DPROP_TRK_EXITED
+    }
+    switch (nav.reason) {
+        case e_reason_path_limit:
+            return 1u;
+        case e_reason_stalled:
+            return 2u;
+        case e_reason_nonfinite:
+            return 6u;  // DPROP_TRK_NONFINITE
+        default:
+            return 3u;
+    }
+}
+
 // Propagate one track to the end with the navigation policy Nav (init and
 // update of the propagator's navigator); returns a dprop_track_status code.
 template <typename S, bool W, typename Tape, typename Nav>
@@ -466,23 +494,7 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
                   is_init;
         ts.heartbeat = ts.heartbeat && nav.is_alive();
     }
-    if (out_of_budget) {
-        return 4u;  // DPROP_TRK_MAX_ITER
-    }
-    const bool paused = !ts.heartbeat && nav.is_alive();
-    if (nav.finished() || paused) {
-        return 0u;  // DPROP_TRK_EXITED
-    }
-    switch (nav.reason) {
-        case e_reason_path_limit:
-            return 1u;
-        case e_reason_stalled:
-            return 2u;
-        case e_reason_nonfinite:
-            return 6u;  // DPROP_TRK_NONFINITE
-        default:
-            return 3u;
-    }
+    return track_status(ts, out_of_budget);
 }
 
 // Propagate one track with the caching navigator.

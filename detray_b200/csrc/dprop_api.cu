@@ -7,10 +7,7 @@
 //                                propagator_benchmark_kernel
 //                                (tests/benchmarks/include/detray/benchmarks/
 //                                device/cuda/propagation_benchmark.cu:13-68)
-//   propagate_persistent_kernel  a grid sized to the SMs whose threads pull
-//                                track indices from a device work queue until
-//                                it is empty, so lanes freed by short tracks
-//                                are refilled while loopers run on.
+// The persistent method's round-based phase kernels are in rounds_api.cu.
 // Both write the slot-major records of dprop_results.
 #include <cuda_runtime.h>
 
@@ -95,14 +92,14 @@ dprop_status ensure_scratch(size_t bytes) {
     return DPROP_OK;
 }
 
-unsigned int* g_queue_counter = nullptr;
-
-// Library-owned device scratch of the direction sort (grow-only).
+// Library-owned device scratch of the direction sort and of the persistent
+// method (grow-only).
 struct sort_scratch {
     void* buf{nullptr};
     size_t bytes{0};
 };
 sort_scratch g_sort;
+sort_scratch g_rounds;
 
 // Sort key of a track, 20 bits: 7 bits of theta (major), 8 bits of phi, the
 // charge sign and 4 bits of log10(pT / GeV) over [-1, 2].  Tracks that share
@@ -174,36 +171,6 @@ __global__ void __launch_bounds__(k_plain_block, MinBlocks)
     }
     const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
     run_one(t, n, det, field, cfg, io);
-}
-
-// Detectors without line surfaces, rods or multi-entry bins only (W = false).
-template <typename In, int MinBlocks = DPROP_MIN_BLOCKS>
-__global__ void __launch_bounds__(k_plain_block, MinBlocks)
-    propagate_persistent_kernel(const __grid_constant__ detector_view<float, false> det,
-                                const __grid_constant__ field_view<float> field,
-                                const __grid_constant__ prop_cfg<float> cfg,
-                                const __grid_constant__ io_ptrs<In> io,
-                                uint64_t n, unsigned int* queue,
-                                const uint32_t* __restrict__ order) {
-    // each warp pulls the next 32 unprocessed tracks once all of its lanes
-    // are done, so that the lanes of a warp start their tracks together
-    const unsigned int lane = threadIdx.x & 31u;
-    while (true) {
-        unsigned int base = 0u;
-        if (lane == 0u) {
-            base = atomicAdd(queue, 32u);
-        }
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) {
-            break;
-        }
-        const uint64_t i = static_cast<uint64_t>(base) + lane;
-        if (i < n) {
-            const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
-            run_one(t, n, det, field, cfg, io);
-        }
-        __syncwarp();
-    }
 }
 
 }  // namespace
@@ -293,22 +260,12 @@ void launch_plain_mb(unsigned int grid, cudaStream_t st,
     }
 }
 
-template <typename In, int MB>
-void launch_persistent_mb(unsigned int grid, cudaStream_t st,
-                          const detector_view<float, false>& det,
-                          const field_view<float>& field,
-                          const prop_cfg<float>& cfg, const io_ptrs<In>& io,
-                          uint64_t n, unsigned int* queue,
-                          const uint32_t* order) {
-    propagate_persistent_kernel<In, MB><<<grid, k_plain_block, 0, st>>>(
-        det, field, cfg, io, n, queue, order);
-}
-
 // Scratch one propagation launch needs besides inputs and outputs.
 struct launch_scratch {
     void* sort{nullptr};        // sort keys/indices + radix-sort temp storage
     size_t sort_bytes{0};
-    unsigned int* queue{nullptr};  // persistent work-queue counter
+    void* rounds{nullptr};      // persistent method: track slots and queues
+    size_t rounds_bytes{0};
 };
 
 // Enqueue one propagation on a stream using the given scratch; contains no
@@ -334,28 +291,10 @@ dprop_status enqueue_propagation(const dprop_config& c,
             return s;
         }
     }
-    // detectors with wire surfaces run the plain kernel (the queue kernel is
-    // instantiated for the others only)
-    if (method == DPROP_METHOD_PERSISTENT && !det->wires) {
-        const detector_view<float, false> dv = det->view_as<false>();
-        if (n > 0xffffff00ull) {
-            return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
-        }
-        DPROP_CUDA(cudaMemsetAsync(scr.queue, 0, sizeof(unsigned int), stream));
-        int dev = 0, sms = 0;
-        DPROP_CUDA(cudaGetDevice(&dev));
-        DPROP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        uint64_t grid = static_cast<uint64_t>(sms) * static_cast<uint64_t>(mb);
-        const uint64_t need = (n + k_plain_block - 1) / k_plain_block;
-        grid = grid < need ? grid : need;
-        const unsigned int g = static_cast<unsigned int>(grid);
-        if (mb == 8) {
-            launch_persistent_mb<In, 8>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
-        } else if (mb == 12) {
-            launch_persistent_mb<In, 12>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
-        } else {
-            launch_persistent_mb<In, 16>(g, stream, dv, field->view, cfg, io, n, scr.queue, order);
-        }
+    if (method == DPROP_METHOD_PERSISTENT) {
+        return dprop::api::enqueue_rounds<In>(launch_cfg, det, field, cfg, io,
+                                              n, order, scr.rounds,
+                                              scr.rounds_bytes, stream);
     } else {
         const unsigned int g =
             static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
@@ -425,10 +364,19 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
             scr.sort_bytes = need;
         }
         if (persistent) {
-            if (!g_queue_counter) {
-                DPROP_CUDA(cudaMalloc(&g_queue_counter, sizeof(unsigned int)));
+            const size_t need = dprop::api::rounds_scratch_bytes(n, det->wires);
+            if (g_rounds.bytes < need) {
+                if (g_rounds.buf) {
+                    DPROP_CUDA(cudaStreamSynchronize(stream));
+                    cudaFree(g_rounds.buf);
+                    g_rounds.buf = nullptr;
+                    g_rounds.bytes = 0;
+                }
+                DPROP_CUDA(cudaMalloc(&g_rounds.buf, need));
+                g_rounds.bytes = need;
             }
-            scr.queue = g_queue_counter;
+            scr.rounds = g_rounds.buf;
+            scr.rounds_bytes = g_rounds.bytes;
         }
         return enqueue_propagation<In>(c, launch_cfg, det, field, io, n, stream,
                                        scr);
@@ -463,16 +411,19 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     graph_entry e;
     e.key = key;
     const size_t sort_bytes = sort ? sort_scratch_bytes(n) : 0;
+    const size_t rounds_bytes =
+        persistent ? dprop::api::rounds_scratch_bytes(n, det->wires) : 0;
     // The radix sort's temporary size carries the sort's alignment padding
-    // and is usually odd: the work-queue counter after it goes to the next
-    // 256-byte boundary (an atomic on an unaligned word is a device fault).
-    const size_t queue_offset = (sort_bytes + 255) & ~size_t(255);
-    DPROP_CUDA(cudaMalloc(&e.scratch, queue_offset + 256));
+    // and is usually odd: the persistent method's arrays after it start at
+    // the next 256-byte boundary (an atomic on an unaligned word is a device
+    // fault).
+    const size_t rounds_offset = (sort_bytes + 255) & ~size_t(255);
+    DPROP_CUDA(cudaMalloc(&e.scratch, rounds_offset + rounds_bytes + 256));
     launch_scratch scr{};
     scr.sort = e.scratch;
     scr.sort_bytes = sort_bytes;
-    scr.queue = reinterpret_cast<unsigned int*>(static_cast<char*>(e.scratch) +
-                                                queue_offset);
+    scr.rounds = static_cast<char*>(e.scratch) + rounds_offset;
+    scr.rounds_bytes = rounds_bytes;
     cudaStream_t cap = nullptr;
     DPROP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;

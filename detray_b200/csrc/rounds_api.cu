@@ -1,0 +1,564 @@
+// Round-based propagation (dprop_launch.method = DPROP_METHOD_PERSISTENT).
+//
+// The plain form runs the whole propagation loop of a track in one thread:
+// the lanes of a warp diverge at every surface, every navigation
+// re-initialisation and every track end, and the full state of the loop
+// (about 500 bytes a track) has to live in registers and the thread's stack
+// across all of it.  Here the loop is cut into the segments of
+// core/machine.cuh and each track's state lives in device memory between
+// them (core/slots.cuh, one array per field, indexed by the track's slot in
+// the direction-sorted batch).  Every round:
+//
+//   queue_count_kernel / queue_scatter_kernel
+//       read the one-byte next-segment array of all slots and write the
+//       slots of each phase, in slot (= direction) order, into the work
+//       queues of the step, surface and navigation phases;
+//   rounds_fast_kernel
+//       the step phase: RK steps with the high-trust navigation update,
+//       the path-limit aborter and (by default) the surface actors, until a
+//       track needs the volume-level navigation update or ends.  A warp
+//       stops its round once fewer than yield_lanes of its lanes can still
+//       step (a warp vote after every step), so that warps do not run on
+//       with a few lanes;
+//   rounds_surf_kernel (surface_phase = 1)
+//       the surface actors;
+//   rounds_nav_kernel
+//       the navigation update's cache re-evaluation, volume switch and local
+//       navigation (grid and portal search), with all lanes of a warp doing
+//       it at once.
+//
+// Each phase kernel is persistent: a grid of the SMs' resident CTAs whose
+// warps pull 32 queue entries at a time from a device counter until the
+// queue is empty.  After `rounds` rounds, rounds_tail_kernel runs the tracks
+// still alive to their end with every segment inline.  Each kernel loads
+// and stores only the state its segments use, and a track driven through
+// the phases ends bit-identical to the plain kernel's result.
+#include <cuda_runtime.h>
+
+#include <cub/block/block_scan.cuh>
+
+#include "api_common.cuh"
+#include "core/phases.cuh"
+#include "track_io.cuh"
+
+using namespace dprop;
+
+namespace {
+
+constexpr int k_build_threads = 256;  // 16 slots each: one tile per CTA
+static_assert(k_build_threads * 16 == static_cast<int>(k_queue_tile),
+              "queue tile = 16 slots per thread");
+constexpr int k_phase_block = 128;
+
+// Queue of a segment: 0 step phase, 1 surface actors, 2 navigation, -1
+// ended.  merged: every live slot in queue 0 (the tail).
+__device__ __forceinline__ int queue_of(uint32_t pc, bool merged) {
+    if (pc == pc_done) {
+        return -1;
+    }
+    if (merged) {
+        return 0;
+    }
+    if (pc == pc_surf) {
+        return 1;
+    }
+    if (pc == pc_nav) {
+        return 2;
+    }
+    return 0;
+}
+
+// Work-queue state of one propagation: three queues of slot indices, their
+// lengths, the per-tile counts of the builder and the pull counters of the
+// phase kernels.
+struct queue_set {
+    uint32_t* q[3];
+    uint32_t* count;   // [3]
+    uint32_t* pull;    // [3]
+    uint32_t* tiles;   // [3 * n_tiles]
+};
+
+__device__ __forceinline__ void unpack16(uint4 v, uint32_t* b) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    for (int i = 0; i < 4; ++i) {
+        for (int j = 0; j < 4; ++j) {
+            b[4 * i + j] = (w[i] >> (8 * j)) & 0xffu;
+        }
+    }
+}
+
+// Per-tile counts of the slots of each queue.
+__global__ void __launch_bounds__(k_build_threads)
+    queue_count_kernel(const uint8_t* __restrict__ pc, queue_set qs,
+                       int merged) {
+    if (blockIdx.x == 0 && threadIdx.x < 3) {
+        qs.pull[threadIdx.x] = 0u;
+    }
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * k_queue_tile +
+                          static_cast<uint64_t>(threadIdx.x) * 16u;
+    uint32_t b[16];
+    unpack16(*reinterpret_cast<const uint4*>(pc + base), b);
+    uint32_t c[3] = {0u, 0u, 0u};
+    for (int i = 0; i < 16; ++i) {
+        const int q = queue_of(b[i], merged != 0);
+        if (q >= 0) {
+            ++c[q];
+        }
+    }
+    __shared__ uint32_t part[k_build_threads / 32][3];
+    for (int k = 0; k < 3; ++k) {
+        uint32_t v = c[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+        if ((threadIdx.x & 31u) == 0u) {
+            part[threadIdx.x >> 5][k] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        uint32_t v = 0u;
+        for (int w = 0; w < k_build_threads / 32; ++w) {
+            v += part[w][threadIdx.x];
+        }
+        qs.tiles[3u * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+// Slots of each queue in slot order: the tile's offset is the sum of the
+// counts of the tiles before it, positions inside the tile come from a block
+// scan of the per-thread counts (three 21-bit fields of one 64-bit value).
+__global__ void __launch_bounds__(k_build_threads)
+    queue_scatter_kernel(const uint8_t* __restrict__ pc, queue_set qs,
+                         uint32_t n_tiles, int merged) {
+    const uint32_t tile = blockIdx.x;
+    uint32_t before[3] = {0u, 0u, 0u};
+    for (uint32_t j = threadIdx.x; j < tile; j += k_build_threads) {
+        for (int k = 0; k < 3; ++k) {
+            before[k] += qs.tiles[3u * j + k];
+        }
+    }
+    __shared__ uint32_t part[k_build_threads / 32][3];
+    __shared__ uint32_t offset[3];
+    for (int k = 0; k < 3; ++k) {
+        uint32_t v = before[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+        if ((threadIdx.x & 31u) == 0u) {
+            part[threadIdx.x >> 5][k] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        uint32_t v = 0u;
+        for (int w = 0; w < k_build_threads / 32; ++w) {
+            v += part[w][threadIdx.x];
+        }
+        offset[threadIdx.x] = v;
+    }
+    const uint64_t base = static_cast<uint64_t>(tile) * k_queue_tile +
+                          static_cast<uint64_t>(threadIdx.x) * 16u;
+    uint32_t b[16];
+    unpack16(*reinterpret_cast<const uint4*>(pc + base), b);
+    uint64_t mine = 0u;
+    for (int i = 0; i < 16; ++i) {
+        const int q = queue_of(b[i], merged != 0);
+        if (q >= 0) {
+            mine += uint64_t(1) << (21 * q);
+        }
+    }
+    using scan_t = cub::BlockScan<uint64_t, k_build_threads>;
+    __shared__ typename scan_t::TempStorage scan_tmp;
+    uint64_t excl = 0u, total = 0u;
+    scan_t(scan_tmp).ExclusiveSum(mine, excl, total);
+    __syncthreads();  // offset[] visible
+    uint32_t pos[3];
+    for (int k = 0; k < 3; ++k) {
+        pos[k] = offset[k] + static_cast<uint32_t>((excl >> (21 * k)) & 0x1fffffu);
+    }
+    for (int i = 0; i < 16; ++i) {
+        const int q = queue_of(b[i], merged != 0);
+        if (q >= 0) {
+            qs.q[q][pos[q]++] = static_cast<uint32_t>(base + i);
+        }
+    }
+    if (tile == n_tiles - 1u && threadIdx.x < 3) {
+        qs.count[threadIdx.x] =
+            offset[threadIdx.x] +
+            static_cast<uint32_t>((total >> (21 * threadIdx.x)) & 0x1fffffu);
+    }
+}
+
+template <typename In>
+__device__ __forceinline__ record_sink<float> make_sink(
+    const api::io_ptrs<In>& io, uint64_t n, const prop_cfg<float>& cfg) {
+    record_sink<float> rec;
+    rec.barcode = io.rec_barcode;
+    rec.bound = io.rec_bound;
+    rec.cov = io.rec_cov;
+    rec.path = io.rec_path;
+    rec.flags = io.rec_flags;
+    rec.n_tracks = n;
+    rec.track = 0u;
+    rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
+    rec.count = 0u;
+    return rec;
+}
+
+template <typename In>
+__device__ __forceinline__ void write_outputs(const api::io_ptrs<In>& io,
+                                              uint64_t t,
+                                              const track_outputs<float>& o) {
+    if (io.status) io.status[t] = o.status;
+    if (io.n_records) io.n_records[t] = o.n_records;
+    if (io.n_steps) io.n_steps[t] = o.n_steps;
+    if (io.n_trials) io.n_trials[t] = o.n_trials;
+    if (io.n_isect) io.n_isect[t] = o.n_isect;
+    if (io.n_transport) io.n_transport[t] = o.n_transport;
+    if (io.n_material) io.n_material[t] = o.n_material;
+    if (io.path_length) io.path_length[t] = o.path_length;
+    for (int i = 0; i < 8; ++i) {
+        if (io.final_free[i]) io.final_free[i][t] = o.fin[i];
+    }
+}
+
+// Next 32 queue entries for the calling warp (all lanes call it together).
+__device__ __forceinline__ uint32_t pull32(uint32_t* pull) {
+    uint32_t base = 0u;
+    if ((threadIdx.x & 31u) == 0u) {
+        base = atomicAdd(pull, 32u);
+    }
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// Propagation start of every slot; pads the next-segment array to whole
+// tiles with ended slots.
+template <typename In, bool W>
+__global__ void __launch_bounds__(k_phase_block)
+    rounds_init_kernel(const __grid_constant__ detector_view<float, W> det,
+                       const __grid_constant__ prop_cfg<float> cfg,
+                       const __grid_constant__ api::io_ptrs<In> io,
+                       const __grid_constant__ slot_soa<float> s, uint64_t n,
+                       uint64_t n_pad, const uint32_t* __restrict__ order) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t slot = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         slot < n_pad; slot += stride) {
+        if (slot >= n) {
+            s.pc[slot] = pc_done;
+            continue;
+        }
+        const uint64_t t = order ? static_cast<uint64_t>(order[slot]) : slot;
+        const vec3<float> pos{static_cast<float>(io.trk[0][t]),
+                              static_cast<float>(io.trk[1][t]),
+                              static_cast<float>(io.trk[2][t])};
+        const vec3<float> dir{static_cast<float>(io.trk[4][t]),
+                              static_cast<float>(io.trk[5][t]),
+                              static_cast<float>(io.trk[6][t])};
+        phase_init<float, W>(s, slot, static_cast<uint32_t>(t), pos,
+                             static_cast<float>(io.trk[3][t]), dir,
+                             static_cast<float>(io.trk[7][t]), det, cfg);
+    }
+}
+
+#ifndef DPROP_FAST_MIN_BLOCKS
+#define DPROP_FAST_MIN_BLOCKS 4
+#endif
+
+// The step phase.
+template <typename In, bool W, bool InlineSurf>
+__global__ void __launch_bounds__(k_phase_block, DPROP_FAST_MIN_BLOCKS)
+    rounds_fast_kernel(const __grid_constant__ detector_view<float, W> det,
+                       const __grid_constant__ field_view<float> field,
+                       const __grid_constant__ prop_cfg<float> cfg,
+                       const __grid_constant__ api::io_ptrs<In> io,
+                       const __grid_constant__ slot_soa<float> s,
+                       const uint32_t* __restrict__ queue,
+                       const uint32_t* __restrict__ count, uint32_t* pull,
+                       uint64_t n, uint32_t step_budget, uint32_t yield_lanes) {
+    const uint32_t cnt = *count;
+    const unsigned lane = threadIdx.x & 31u;
+    record_sink<float> rec = make_sink(io, n, cfg);
+    while (true) {
+        const uint32_t base = pull32(pull);
+        if (base >= cnt) {
+            break;
+        }
+        const uint32_t idx = base + lane;
+        const bool valid = idx < cnt;
+        const uint64_t slot = valid ? queue[idx] : 0u;
+        track_state<float> ts;
+        loop_state<float> ls;
+        cand_window win;
+        if (valid) {
+            fast_load<float, W>(s, slot, ts, ls, win);
+        }
+        const int n_valid = __popc(__ballot_sync(0xffffffffu, valid));
+        bool active = valid;
+        for (uint32_t it = 0;; ++it) {
+            if (active) {
+                const uint8_t pc = fast_advance<float, W, InlineSurf>(
+                    ts, ls, win, s, slot, det, field, cfg, rec);
+                active = machine_is_fast(pc);
+            }
+            const int m = __popc(__ballot_sync(0xffffffffu, active));
+            if (m == 0 || it + 1u >= step_budget ||
+                (m < static_cast<int>(yield_lanes) && m < n_valid)) {
+                break;
+            }
+        }
+        if (valid) {
+            fast_store<float, W>(s, slot, ts, ls, win);
+            if (ls.pc == pc_done) {
+                write_outputs(io, s.track[slot],
+                              fast_outputs(s, slot, ts, ls));
+            }
+        }
+    }
+}
+
+// The surface actors.
+template <typename In, bool W>
+__global__ void __launch_bounds__(k_phase_block, 4)
+    rounds_surf_kernel(const __grid_constant__ detector_view<float, W> det,
+                       const __grid_constant__ field_view<float> field,
+                       const __grid_constant__ prop_cfg<float> cfg,
+                       const __grid_constant__ api::io_ptrs<In> io,
+                       const __grid_constant__ slot_soa<float> s,
+                       const uint32_t* __restrict__ queue,
+                       const uint32_t* __restrict__ count, uint32_t* pull,
+                       uint64_t n) {
+    const uint32_t cnt = *count;
+    record_sink<float> rec = make_sink(io, n, cfg);
+    while (true) {
+        const uint32_t base = pull32(pull);
+        if (base >= cnt) {
+            break;
+        }
+        const uint32_t idx = base + (threadIdx.x & 31u);
+        if (idx < cnt) {
+            phase_surf<float, W>(s, queue[idx], det, field, cfg, rec);
+        }
+        __syncwarp();
+    }
+}
+
+// The navigation update's volume-level part.
+template <bool W>
+__global__ void __launch_bounds__(k_phase_block, 4)
+    rounds_nav_kernel(const __grid_constant__ detector_view<float, W> det,
+                      const __grid_constant__ prop_cfg<float> cfg,
+                      const __grid_constant__ slot_soa<float> s,
+                      const uint32_t* __restrict__ queue,
+                      const uint32_t* __restrict__ count, uint32_t* pull) {
+    const uint32_t cnt = *count;
+    while (true) {
+        const uint32_t base = pull32(pull);
+        if (base >= cnt) {
+            break;
+        }
+        const uint32_t idx = base + (threadIdx.x & 31u);
+        if (idx < cnt) {
+            phase_nav<float, W>(s, queue[idx], det, cfg);
+        }
+        __syncwarp();
+    }
+}
+
+// The tracks still alive after the last round, every segment inline.
+template <typename In, bool W>
+__global__ void __launch_bounds__(k_phase_block, 8)
+    rounds_tail_kernel(const __grid_constant__ detector_view<float, W> det,
+                       const __grid_constant__ field_view<float> field,
+                       const __grid_constant__ prop_cfg<float> cfg,
+                       const __grid_constant__ api::io_ptrs<In> io,
+                       const __grid_constant__ slot_soa<float> s,
+                       const uint32_t* __restrict__ queue,
+                       const uint32_t* __restrict__ count, uint32_t* pull,
+                       uint64_t n) {
+    const uint32_t cnt = *count;
+    record_sink<float> rec = make_sink(io, n, cfg);
+    while (true) {
+        const uint32_t base = pull32(pull);
+        if (base >= cnt) {
+            break;
+        }
+        const uint32_t idx = base + (threadIdx.x & 31u);
+        if (idx < cnt) {
+            const uint64_t slot = queue[idx];
+            const track_outputs<float> o =
+                phase_tail<float, W>(s, slot, det, field, cfg, rec);
+            write_outputs(io, s.track[slot], o);
+        }
+        __syncwarp();
+    }
+}
+
+// Resident CTAs of a kernel on the current device (the persistent grid).
+template <typename K>
+dprop_status resident_grid(K kernel, unsigned int* grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    DPROP_CUDA(cudaGetDevice(&dev));
+    DPROP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DPROP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, kernel, k_phase_block, 0));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    *grid = static_cast<unsigned int>(sms * per_sm);
+    return DPROP_OK;
+}
+
+struct rounds_layout {
+    slot_soa<float> slots;
+    queue_set qs;
+    uint64_t n_tiles;
+};
+
+size_t al256(size_t b) { return (b + 255u) & ~size_t(255u); }
+
+// Scratch layout: slot arrays, three queues, counters and tile counts.
+size_t rounds_layout_bytes(uint64_t n, bool wires, rounds_layout* out,
+                           void* base) {
+    const uint64_t n_tiles = queue_tiles(n);
+    slot_soa<float> s{};
+    const size_t slot_bytes = carve_slots<float>(base, n, wires, &s);
+    size_t off = al256(slot_bytes);
+    char* p = static_cast<char*>(base);
+    queue_set qs{};
+    for (int k = 0; k < 3; ++k) {
+        qs.q[k] = reinterpret_cast<uint32_t*>(p + off);
+        off += al256(n * 4u);
+    }
+    qs.count = reinterpret_cast<uint32_t*>(p + off);
+    qs.pull = qs.count + 4;
+    off += 256;
+    qs.tiles = reinterpret_cast<uint32_t*>(p + off);
+    off += al256(3u * n_tiles * 4u);
+    if (out) {
+        out->slots = s;
+        out->qs = qs;
+        out->n_tiles = n_tiles;
+    }
+    return off;
+}
+
+template <typename In, bool W, bool InlineSurf>
+dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
+                              const field_view<float>& field,
+                              const prop_cfg<float>& cfg,
+                              const api::io_ptrs<In>& io, uint64_t n,
+                              const uint32_t* order, const rounds_layout& L,
+                              uint32_t rounds, uint32_t step_budget,
+                              uint32_t yield_lanes, cudaStream_t st) {
+    const uint64_t n_pad = L.n_tiles * k_queue_tile;
+    const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
+    unsigned int g_init = 0, g_fast = 0, g_surf = 0, g_nav = 0, g_tail = 0;
+    dprop_status s = DPROP_OK;
+    if ((s = resident_grid(rounds_init_kernel<In, W>, &g_init)) != DPROP_OK ||
+        (s = resident_grid(rounds_fast_kernel<In, W, InlineSurf>, &g_fast)) != DPROP_OK ||
+        (s = resident_grid(rounds_surf_kernel<In, W>, &g_surf)) != DPROP_OK ||
+        (s = resident_grid(rounds_nav_kernel<W>, &g_nav)) != DPROP_OK ||
+        (s = resident_grid(rounds_tail_kernel<In, W>, &g_tail)) != DPROP_OK) {
+        return s;
+    }
+    rounds_init_kernel<In, W><<<g_init, k_phase_block, 0, st>>>(
+        det, cfg, io, L.slots, n, n_pad, order);
+    DPROP_CUDA(cudaGetLastError());
+    for (uint32_t r = 0; r <= rounds; ++r) {
+        const int merged = (r == rounds) ? 1 : 0;
+        queue_count_kernel<<<tiles, k_build_threads, 0, st>>>(L.slots.pc, L.qs,
+                                                              merged);
+        queue_scatter_kernel<<<tiles, k_build_threads, 0, st>>>(
+            L.slots.pc, L.qs, tiles, merged);
+        DPROP_CUDA(cudaGetLastError());
+        if (merged) {
+            rounds_tail_kernel<In, W><<<g_tail, k_phase_block, 0, st>>>(
+                det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count,
+                L.qs.pull, n);
+            DPROP_CUDA(cudaGetLastError());
+            break;
+        }
+        rounds_fast_kernel<In, W, InlineSurf><<<g_fast, k_phase_block, 0, st>>>(
+            det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count, L.qs.pull, n,
+            step_budget, yield_lanes);
+        if (!InlineSurf) {
+            rounds_surf_kernel<In, W><<<g_surf, k_phase_block, 0, st>>>(
+                det, field, cfg, io, L.slots, L.qs.q[1], L.qs.count + 1,
+                L.qs.pull + 1, n);
+        }
+        rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
+            det, cfg, L.slots, L.qs.q[2], L.qs.count + 2, L.qs.pull + 2);
+        DPROP_CUDA(cudaGetLastError());
+    }
+    return DPROP_OK;
+}
+
+}  // namespace
+
+namespace dprop::api {
+
+constexpr uint32_t k_default_steps_per_round = 16u;
+constexpr uint32_t k_default_rounds = 96u;
+constexpr uint32_t k_default_yield_lanes = 8u;
+
+size_t rounds_scratch_bytes(uint64_t n, bool wires) {
+    return rounds_layout_bytes(n, wires, nullptr, nullptr) + 256u;
+}
+
+template <typename In>
+dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
+                            const dprop_field* field,
+                            const prop_cfg<float>& cfg, const io_ptrs<In>& io,
+                            uint64_t n, const uint32_t* order, void* scratch,
+                            size_t scratch_bytes, cudaStream_t stream) {
+    if (n > 0xffffff00ull) {
+        return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
+    }
+    if (scratch_bytes < rounds_scratch_bytes(n, det->wires)) {
+        return fail(DPROP_E_INVALID, "persistent method: scratch too small");
+    }
+    void* base = reinterpret_cast<void*>(
+        (reinterpret_cast<uintptr_t>(scratch) + 255u) & ~uintptr_t(255u));
+    rounds_layout L{};
+    rounds_layout_bytes(n, det->wires, &L, base);
+    const uint32_t rounds = (lc && lc->rounds) ? lc->rounds : k_default_rounds;
+    const uint32_t budget = (lc && lc->steps_per_round) ? lc->steps_per_round
+                                                        : k_default_steps_per_round;
+    const uint32_t yield = (lc && lc->yield_lanes) ? lc->yield_lanes
+                                                   : k_default_yield_lanes;
+    if (rounds > 100000u || yield > 32u) {
+        return fail(DPROP_E_INVALID,
+                    "persistent method: rounds > 100000 or yield_lanes > 32");
+    }
+    const bool inline_surf = !(lc && lc->surface_phase);
+    if (det->wires) {
+        const detector_view<float, true> dv = det->view_as<true>();
+        return inline_surf
+                   ? enqueue_rounds_w<In, true, true>(dv, field->view, cfg, io, n, order, L,
+                                                      rounds, budget, yield, stream)
+                   : enqueue_rounds_w<In, true, false>(dv, field->view, cfg, io, n, order, L,
+                                                       rounds, budget, yield, stream);
+    }
+    const detector_view<float, false> dv = det->view_as<false>();
+    return inline_surf
+               ? enqueue_rounds_w<In, false, true>(dv, field->view, cfg, io, n, order, L,
+                                                   rounds, budget, yield, stream)
+               : enqueue_rounds_w<In, false, false>(dv, field->view, cfg, io, n, order, L,
+                                                    rounds, budget, yield, stream);
+}
+
+template dprop_status enqueue_rounds<float>(const dprop_launch*,
+                                            const dprop_detector*,
+                                            const dprop_field*,
+                                            const prop_cfg<float>&,
+                                            const io_ptrs<float>&, uint64_t,
+                                            const uint32_t*, void*, size_t,
+                                            cudaStream_t);
+template dprop_status enqueue_rounds<double>(const dprop_launch*,
+                                             const dprop_detector*,
+                                             const dprop_field*,
+                                             const prop_cfg<float>&,
+                                             const io_ptrs<double>&, uint64_t,
+                                             const uint32_t*, void*, size_t,
+                                             cudaStream_t);
+
+}  // namespace dprop::api

@@ -118,4 +118,17 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     }
 }
 
+// Round-based propagation (rounds_api.cu): device scratch bytes for n
+// tracks, and the enqueue of the whole propagation on a stream (no
+// allocation, no synchronisation; order is the direction-sorted track order
+// or NULL).
+size_t rounds_scratch_bytes(uint64_t n, bool wires);
+
+template <typename In>
+dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
+                            const dprop_field* field,
+                            const prop_cfg<float>& cfg, const io_ptrs<In>& io,
+                            uint64_t n, const uint32_t* order, void* scratch,
+                            size_t scratch_bytes, cudaStream_t stream);
+
 }  // namespace dprop::api

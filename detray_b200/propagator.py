@@ -182,9 +182,13 @@ class Field:
 
 def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
                 ctas_per_sm: int = 0, sort_tracks: int = 0,
-                use_graph: int = 0, precision: int = 0) -> abi.Launch:
+                use_graph: int = 0, precision: int = 0,
+                steps_per_round: int = 0, rounds: int = 0,
+                yield_lanes: int = 0, surface_phase: int = 0) -> abi.Launch:
     """Launch shape; ``precision`` 8 runs the propagation in fp64 end to end
-    (double track tensors and results)."""
+    (double track tensors and results).  steps_per_round, rounds,
+    yield_lanes and surface_phase shape the persistent (round-based) method;
+    0 picks the library default."""
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
@@ -192,6 +196,10 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
     lc.sort_tracks = sort_tracks
     lc.use_graph = use_graph
     lc.precision = precision
+    lc.steps_per_round = steps_per_round
+    lc.rounds = rounds
+    lc.yield_lanes = yield_lanes
+    lc.surface_phase = surface_phase
     return lc
 
 

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define DPROP_ABI_VERSION 1u
+#define DPROP_ABI_VERSION 2u
 
 /* ------------------------------------------------------------------ status */
 typedef enum dprop_status {
@@ -296,11 +296,22 @@ typedef struct dprop_results {
 /* Launch shape; zero fields pick the library defaults / autotuned values. */
 typedef enum dprop_method {
     DPROP_METHOD_PLAIN = 0,      /* one thread per track, whole propagation   */
-    DPROP_METHOD_PERSISTENT = 1  /* persistent lanes pulling tracks from a
-                                    device work queue (detectors with line
-                                    surfaces, material rods, multi-entry
-                                    grid bins or material maps run the plain
-                                    form)                                     */
+    DPROP_METHOD_PERSISTENT = 1  /* round-based phase kernels: each track's
+                                    state lives in device memory between
+                                    rounds; every round a queue builder
+                                    sorts the live tracks into the work
+                                    queues of the step phase (RK steps,
+                                    high-trust navigation, path-limit
+                                    aborter and - unless surface_phase - the
+                                    surface actors), the surface phase and
+                                    the navigation phase (cache
+                                    re-evaluation, volume switch), in
+                                    direction order, and persistent
+                                    grid-stride kernels pull their tracks
+                                    from those queues; after `rounds` rounds
+                                    the tracks still alive finish in one
+                                    kernel.  Identical results to the plain
+                                    form                                      */
 } dprop_method;
 
 typedef struct dprop_launch {
@@ -309,8 +320,7 @@ typedef struct dprop_launch {
     uint32_t ctas_per_sm;        /* register budget: resident CTAs of 128
                                     threads per SM the kernel is compiled for,
                                     8 (64 registers), 12 (40) or 16 (32);
-                                    0 = 12.  The persistent grid is SMs times
-                                    this                                       */
+                                    0 = 12.  Plain method                     */
     uint32_t sort_tracks;        /* 1: process tracks ordered by direction
                                     (theta, phi) so that the lanes of a warp
                                     follow similar paths; results are still
@@ -325,6 +335,18 @@ typedef struct dprop_launch {
                                     reference's full-fp64 build); plain kernel,
                                     method and use_graph ignored.  Device API
                                     (dprop_propagate) only                     */
+    /* Persistent method only (0: the library default of each): */
+    uint32_t steps_per_round;    /* RK steps a track takes per round at most
+                                    (default 16)                               */
+    uint32_t rounds;             /* rounds of the phase kernels before the
+                                    tracks still alive finish in one kernel
+                                    (default 96)                               */
+    uint32_t yield_lanes;        /* tracks per warp: a warp of the step phase
+                                    ends its round once fewer than this many of
+                                    its 32 lanes can still step (default 8)    */
+    uint32_t surface_phase;      /* 1: the surface actors run in a phase
+                                    kernel of their own; 0: inside the step
+                                    phase (default)                           */
     uint32_t reserved[2];
 } dprop_launch;
 

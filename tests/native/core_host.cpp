@@ -14,6 +14,7 @@
 #include "core/convert.hpp"
 #include "core/direct.cuh"
 #include "core/helix.cuh"
+#include "core/phases.cuh"
 
 #include <algorithm>
 
@@ -202,6 +203,257 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
     }
     return 0;
 }
+template <typename S>
+void poison(track_state<S>& ts, loop_state<S>& ls) {
+    std::memset(static_cast<void*>(&ts), 0xff, sizeof(ts));
+    std::memset(static_cast<void*>(&ls), 0xff, sizeof(ls));
+}
+
+template <typename S>
+field_view<S> host_field(uint32_t field_kind, const double* b,
+                         const double* lo, const double* hi,
+                         const uint32_t* nn, const float* values,
+                         std::vector<float4>& nodes) {
+    field_view<S> f{};
+    if (field_kind == 0u) {
+        f.kind = 0u;
+        f.n_r = f.n_phi = f.n_z = 1u;
+        for (int i = 0; i < 3; ++i) {
+            f.b[i] = static_cast<S>(b[i]);
+        }
+        return f;
+    }
+    const uint64_t nn_all = static_cast<uint64_t>(nn[0]) * nn[1] * nn[2];
+    nodes.resize(nn_all);
+    for (uint64_t i = 0; i < nn_all; ++i) {
+        nodes[i] = float4{values[3 * i], values[3 * i + 1], values[3 * i + 2],
+                          0.f};
+    }
+    f.kind = 1u;
+    f.n_r = nn[0];
+    f.n_phi = nn[1];
+    f.n_z = nn[2];
+    f.r_lo = static_cast<S>(lo[0]);
+    f.r_step_inv =
+        nn[0] > 1 ? static_cast<S>((nn[0] - 1) / (hi[0] - lo[0])) : S(0);
+    f.phi_lo = static_cast<S>(lo[1]);
+    f.phi_step_inv = static_cast<S>(nn[1] / (2.0 * constant::pi));
+    f.z_lo = static_cast<S>(lo[2]);
+    f.z_step_inv =
+        nn[2] > 1 ? static_cast<S>((nn[2] - 1) / (hi[2] - lo[2])) : S(0);
+    f.nodes = nodes.data();
+    return f;
+}
+
+template <typename S, bool W, bool InlineSurf>
+int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
+                 const double* b, const double* lo, const double* hi,
+                 const uint32_t* nn, const float* values,
+                 const dprop_config* c, const double* const* trk, uint64_t n,
+                 const dprop_results* out, uint32_t rounds,
+                 uint32_t step_budget, uint32_t yield_min, uint32_t* stats) {
+    std::vector<float4> nodes;
+    const field_view<S> f =
+        host_field<S>(field_kind, b, lo, hi, nn, values, nodes);
+    const prop_cfg<S> cfg = make_prop_cfg<S>(*c);
+    const uint32_t cap = c->max_records;
+    std::vector<unsigned char> mem(carve_slots<S>(nullptr, n, W, nullptr) + 256);
+    slot_soa<S> s{};
+    void* base = reinterpret_cast<void*>(
+        (reinterpret_cast<uintptr_t>(mem.data()) + 255u) & ~uintptr_t(255u));
+    carve_slots<S>(base, n, W, &s);
+    // records, slot-major in S; widened at the end
+    std::vector<uint64_t> rbc(static_cast<size_t>(cap) * n, 0u);
+    std::vector<S> rb[6], rc[21];
+    S* bptr[6];
+    S* cptr[21];
+    for (int i = 0; i < 6; ++i) {
+        rb[i].assign(static_cast<size_t>(cap) * n, S(0));
+        bptr[i] = rb[i].data();
+    }
+    for (int i = 0; i < 21; ++i) {
+        rc[i].assign(static_cast<size_t>(cap) * n, S(0));
+        cptr[i] = rc[i].data();
+    }
+    std::vector<S> rp(static_cast<size_t>(cap) * n, S(0));
+    std::vector<uint8_t> rf(static_cast<size_t>(cap) * n, 0u);
+    record_sink<S> rec{};
+    rec.barcode = rbc.data();
+    rec.bound = bptr;
+    rec.cov = cptr;
+    rec.path = rp.data();
+    rec.flags = rf.data();
+    rec.n_tracks = n;
+    rec.capacity = cap;
+
+    auto emit = [&](const track_outputs<S>& o, uint64_t t) {
+        out->status[t] = o.status;
+        if (out->n_records) out->n_records[t] = o.n_records;
+        if (out->n_steps) out->n_steps[t] = o.n_steps;
+        if (out->n_trials) out->n_trials[t] = o.n_trials;
+        if (out->n_intersections) out->n_intersections[t] = o.n_isect;
+        if (out->n_transports) out->n_transports[t] = o.n_transport;
+        if (out->n_material) out->n_material[t] = o.n_material;
+        if (out->path_length)
+            static_cast<double*>(out->path_length)[t] = o.path_length;
+        for (int i = 0; i < 8; ++i) {
+            if (out->final_free[i])
+                static_cast<double*>(out->final_free[i])[t] = o.fin[i];
+        }
+    };
+
+    for (uint64_t t = 0; t < n; ++t) {
+        phase_init<S, W>(s, t, static_cast<uint32_t>(t),
+                         vec3<S>{static_cast<S>(trk[0][t]), static_cast<S>(trk[1][t]),
+                                 static_cast<S>(trk[2][t])},
+                         static_cast<S>(trk[3][t]),
+                         vec3<S>{static_cast<S>(trk[4][t]), static_cast<S>(trk[5][t]),
+                                 static_cast<S>(trk[6][t])},
+                         static_cast<S>(trk[7][t]), det, cfg);
+    }
+    std::vector<uint64_t> qf, qs, qn;
+    for (uint32_t r = 0; r <= rounds; ++r) {
+        qf.clear();
+        qs.clear();
+        qn.clear();
+        for (uint64_t slot = 0; slot < n; ++slot) {
+            const uint8_t pc = s.pc[slot];
+            if (pc == pc_surf) {
+                qs.push_back(slot);
+            } else if (pc == pc_nav) {
+                qn.push_back(slot);
+            } else if (pc != pc_done) {
+                qf.push_back(slot);
+            }
+        }
+        if (stats != nullptr) {
+            stats[3u * r + 0u] = static_cast<uint32_t>(qf.size());
+            stats[3u * r + 1u] = static_cast<uint32_t>(qs.size());
+            stats[3u * r + 2u] = static_cast<uint32_t>(qn.size());
+        }
+        if (r == rounds) {
+            // tail: everything still alive, every segment inline
+            for (uint64_t slot = 0; slot < n; ++slot) {
+                if (s.pc[slot] == pc_done) continue;
+                const track_outputs<S> o = phase_tail<S, W>(s, slot, det, f, cfg, rec);
+                emit(o, s.track[slot]);
+            }
+            break;
+        }
+        // fast phase, in groups of 32 queue entries
+        for (size_t g0 = 0; g0 < qf.size(); g0 += 32u) {
+            const size_t m = (qf.size() - g0) < 32u ? qf.size() - g0 : 32u;
+            track_state<S> ts[32];
+            loop_state<S> ls[32];
+            cand_window c0[32];
+            bool active[32];
+            for (size_t l = 0; l < m; ++l) {
+                poison(ts[l], ls[l]);
+                fast_load<S, W>(s, qf[g0 + l], ts[l], ls[l], c0[l]);
+                active[l] = true;
+            }
+            for (uint32_t it = 0;; ++it) {
+                uint32_t n_active = 0;
+                for (size_t l = 0; l < m; ++l) {
+                    if (!active[l]) continue;
+                    const uint8_t pc = fast_advance<S, W, InlineSurf>(
+                        ts[l], ls[l], c0[l], s, qf[g0 + l], det, f, cfg, rec);
+                    active[l] = machine_is_fast(pc);
+                    n_active += active[l] ? 1u : 0u;
+                }
+                if (n_active == 0u || it + 1u >= step_budget ||
+                    n_active < yield_min) {
+                    break;
+                }
+            }
+            for (size_t l = 0; l < m; ++l) {
+                const uint64_t slot = qf[g0 + l];
+                fast_store<S, W>(s, slot, ts[l], ls[l], c0[l]);
+                if (ls[l].pc == pc_done) {
+                    emit(fast_outputs(s, slot, ts[l], ls[l]), s.track[slot]);
+                }
+            }
+        }
+        for (const uint64_t slot : qs) {
+            phase_surf<S, W>(s, slot, det, f, cfg, rec);
+        }
+        for (const uint64_t slot : qn) {
+            phase_nav<S, W>(s, slot, det, cfg);
+        }
+    }
+    for (uint64_t t = 0; t < n; ++t) {
+        const uint32_t m = out->n_records ? (out->n_records[t] < cap ? out->n_records[t] : cap) : 0u;
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint64_t o = static_cast<uint64_t>(k) * n + t;
+            if (out->rec_barcode) out->rec_barcode[o] = rbc[o];
+            if (out->rec_flags) out->rec_flags[o] = rf[o];
+            if (out->rec_path) static_cast<double*>(out->rec_path)[o] = rp[o];
+            for (int i = 0; i < 6; ++i) {
+                if (out->rec_bound[i]) static_cast<double*>(out->rec_bound[i])[o] = rb[i][o];
+            }
+            for (int i = 0; i < 21; ++i) {
+                if (out->rec_cov[i]) static_cast<double*>(out->rec_cov[i])[o] = rc[i][o];
+            }
+        }
+    }
+    return 0;
+}
+
+// The round-based propagation of the phase kernels, simulated on the host
+// with the same phase bodies: every round classifies the slots by their next
+// segment first (as the queue builder does), then runs the fast phase (with
+// inline_surf, the surface actors inside it) over
+// groups of 32 slots with the kernel's yield rule (all lanes of a group stop
+// once fewer than yield_min of them are still in the fast phase, or after
+// step_budget steps), the surface actors and the navigation phase.  After
+// `rounds` rounds the remaining slots run the tail.  The local state is
+// filled with a poison byte before every load, so a segment reading a field
+// its phase does not load changes the results.  stats (optional, rounds + 1
+// entries per class) receives the queue sizes per round.
+template <typename S>
+int run_rounds(const dprop_detector_desc* desc, uint32_t field_kind,
+               const double* b, const double* lo, const double* hi,
+               const uint32_t* nn, const float* values, const dprop_config* c,
+               const double* const* trk, uint64_t n, const dprop_results* out,
+               uint32_t rounds, uint32_t step_budget, uint32_t yield_min,
+               bool inline_surf, uint32_t* stats) {
+    const std::string problem = validate_desc(desc);
+    if (!problem.empty()) {
+        g_err = problem;
+        return 1;
+    }
+    const host_tables<S> tables = convert_desc<S>(desc);
+    bool wires = false;
+    for (uint32_t i = 0; i < desc->n_surfaces; ++i) {
+        wires = wires || desc->surfaces[i].shape == DPROP_SHAPE_LINE ||
+                desc->surfaces[i].material_kind != 0u;
+    }
+    for (uint32_t i = 0; i < desc->n_slabs; ++i) {
+        wires = wires || desc->slabs[i].kind == DPROP_MATERIAL_ROD;
+    }
+    for (uint32_t i = 0; i < desc->n_grids; ++i) {
+        wires = wires || desc->grids[i].multi != 0u;
+    }
+    if (!wires) {
+        if (inline_surf) {
+            return run_rounds_w<S, false, true>(
+                tables.template view_as<false>(), field_kind, b, lo, hi, nn,
+                values, c, trk, n, out, rounds, step_budget, yield_min, stats);
+        }
+        return run_rounds_w<S, false, false>(
+            tables.template view_as<false>(), field_kind, b, lo, hi, nn,
+            values, c, trk, n, out, rounds, step_budget, yield_min, stats);
+    }
+    if (inline_surf) {
+        return run_rounds_w<S, true, true>(
+            tables.template view_as<true>(), field_kind, b, lo, hi, nn, values,
+            c, trk, n, out, rounds, step_budget, yield_min, stats);
+    }
+    return run_rounds_w<S, true, false>(
+        tables.template view_as<true>(), field_kind, b, lo, hi, nn, values, c,
+        trk, n, out, rounds, step_budget, yield_min, stats);
+}
+
 }  // namespace
 
 extern "C" {
@@ -216,6 +468,27 @@ int core_host_propagate(int precision_bytes, const dprop_detector_desc* desc,
         return run<double>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
     }
     return run<float>(desc, field_kind, b, lo, hi, nn, values, cfg, trk, n, out);
+}
+
+// The round-based propagation of the phase kernels (run_rounds above).
+int core_host_propagate_rounds(int precision_bytes,
+                               const dprop_detector_desc* desc,
+                               uint32_t field_kind, const double* b,
+                               const double* lo, const double* hi,
+                               const uint32_t* nn, const float* values,
+                               const dprop_config* cfg,
+                               const double* const* trk, uint64_t n,
+                               const dprop_results* out, uint32_t rounds,
+                               uint32_t step_budget, uint32_t yield_min,
+                               int inline_surf, uint32_t* stats) {
+    if (precision_bytes == 8) {
+        return run_rounds<double>(desc, field_kind, b, lo, hi, nn, values, cfg,
+                                  trk, n, out, rounds, step_budget, yield_min,
+                                  inline_surf != 0, stats);
+    }
+    return run_rounds<float>(desc, field_kind, b, lo, hi, nn, values, cfg,
+                             trk, n, out, rounds, step_budget, yield_min,
+                             inline_surf != 0, stats);
 }
 
 // Direct-navigation propagation (constant field b): as

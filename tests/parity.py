@@ -1,10 +1,10 @@
 """Shared parity checks between a propagation result and the oracle.
 
 Both results use the dprop_results layout (slot-major records).  The checks:
-  * per-track status equal;
-  * the sequence of recorded surface barcodes equal, except for a bounded
-    number of tracks (``max_seq_mismatch``) whose fp32 path grazes a mask
-    boundary and so legitimately crosses a different surface;
+  * per-track status and the sequence of recorded surface barcodes equal,
+    except for a bounded number of tracks (``max_seq_mismatch_frac``) whose
+    fp32 path grazes a mask boundary and so legitimately crosses a different
+    surface (and may then end differently);
   * on tracks with equal sequences, bound parameters and covariance at every
     transported surface within abs + rel tolerances.
 """
@@ -40,6 +40,9 @@ def compare(ref: dict, got: dict, *, max_seq_mismatch_frac: float,
     n_bad_seq = int((~seq_ok).sum())
     assert n_bad_seq <= max_seq_mismatch_frac * n + 1, (
         f"{n_bad_seq} of {n} tracks cross a different surface sequence")
+    n_bad_status = int((~status_ok).sum())
+    assert n_bad_status <= max_seq_mismatch_frac * n + 1, (
+        f"{n_bad_status} of {n} tracks end with a different status")
     good = np.where(seq_ok & status_ok)[0]
     cap = min(ref["rec_barcode"].shape[0], got["rec_barcode"].shape[0])
     nrec = np.minimum(ref["n_records"][good].astype(np.int64), cap)

@@ -32,10 +32,10 @@ def torch_cuda():
     return torch
 
 
-def _run_device(torch, det, field, cfg, trk, method=0):
+def _run_device(torch, det, field, cfg, trk, method=0, **launch):
     from detray_b200 import propagator
     dev = torch.tensor(trk, dtype=torch.float32, device="cuda")
-    lc = propagator.make_launch(method=method)
+    lc = propagator.make_launch(method=method, **launch)
     res = propagator.propagate(cfg, det, field, dev, launch=lc)
     torch.cuda.synchronize()
     out = {k: v.cpu().numpy() for k, v in res.tensors.items()}
@@ -49,7 +49,7 @@ def _setup(kind):
     if kind == "telescope":
         tables = geometry.load_geometry("telescope_10x1m_300um")
         cfg = abi.make_config(max_records=16)
-        trk = tracks.telescope_tracks(4000, seed=11)
+        trk = tracks.telescope_tracks(10000, seed=11)
     elif kind.startswith("wire"):
         tables = geometry.load_geometry(kind)
         cfg = abi.make_config(max_records=64, search_window=(3, 3),
@@ -78,24 +78,60 @@ def _oracle_detector(oracle, kind):
                                   "wire_chamber_10l_cells",
                                   "wire_chamber_10l_straws"])
 def test_device_vs_oracle(torch_cuda, oracle, kind):
+    """Both launch forms (plain; persistent, round-based, sorted) against the
+    same oracle run."""
     det, field, cfg, trk = _setup(kind)
     ref_det = _oracle_detector(oracle, kind)
     ref = oracle.propagate(ref_det, field.spec, cfg, trk)
-    got = _run_device(torch_cuda, det, field, cfg, trk)
-    summary = compare(ref, got, max_seq_mismatch_frac=1e-3, tol_abs=TOL_ABS,
-                      tol_rel=TOL_REL, cov_rel=COV_REL)
-    print(kind, summary)
+    for method, sort in ((0, 0), (1, 1)):
+        got = _run_device(torch_cuda, det, field, cfg, trk, method=method,
+                          sort_tracks=sort)
+        summary = compare(ref, got, max_seq_mismatch_frac=1e-3,
+                          tol_abs=TOL_ABS, tol_rel=TOL_REL, cov_rel=COV_REL)
+        print(kind, method, summary)
 
 
-def test_persistent_equals_plain(torch_cuda):
-    """Both launch forms run the same per-track code: identical results."""
-    det, field, cfg, trk = _setup("toy")
+def _assert_same_results(a, b, what):
+    for key in ["status", "n_records", "n_steps", "n_trials",
+                "n_intersections", "n_transports", "n_material",
+                "path_length", "final_free"]:
+        assert np.array_equal(a[key], b[key], equal_nan=a[key].dtype.kind == "f"), (what, key)
+    m = int(a["n_records"].max())
+    valid = np.arange(m)[:, None] < a["n_records"][None, :]
+    assert np.array_equal(a["rec_barcode"][:m][valid],
+                          b["rec_barcode"][:m][valid]), (what, "rec_barcode")
+    for key in ["rec_bound", "rec_cov"]:
+        assert np.array_equal(a[key][:, :m][:, valid],
+                              b[key][:, :m][:, valid]), (what, key)
+    assert np.array_equal(a["rec_path"][:m][valid], b["rec_path"][:m][valid])
+    assert np.array_equal(a["rec_flags"][:m][valid], b["rec_flags"][:m][valid])
+
+
+@pytest.mark.parametrize("kind", ["toy", "toy_map", "wire_chamber_10l_cells"])
+def test_persistent_equals_plain(torch_cuda, kind):
+    """The round-based phase kernels run the same per-track operations as
+    the plain kernel, cut into segments: every output is bit-identical, for
+    the surface actors inside the step phase or in their own phase, for few
+    or many rounds (the rest finishing in the tail kernel) and for any step
+    budget and yield rule."""
+    if kind == "toy_map":
+        from detray_b200 import abi, fields, geometry, propagator, tracks
+        det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
+        field = propagator.Field.grid(fields.solenoid_map())
+        cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                              estimate_scattering_noise=0)
+        trk = tracks.toy_tracks(20000, seed=31, pt_range=(0.1, 100.0))
+    else:
+        det, field, cfg, trk = _setup(kind)
     a = _run_device(torch_cuda, det, field, cfg, trk, method=0)
-    b = _run_device(torch_cuda, det, field, cfg, trk, method=1)
-    for key in ["status", "n_records", "n_trials", "path_length"]:
-        assert np.array_equal(a[key], b[key]), key
-    m = a["n_records"].max()
-    assert np.array_equal(a["rec_barcode"][:m], b["rec_barcode"][:m])
+    for launch in [dict(sort_tracks=1),
+                   dict(sort_tracks=1, surface_phase=1),
+                   dict(sort_tracks=0, rounds=5, steps_per_round=3,
+                        yield_lanes=30),
+                   dict(sort_tracks=1, rounds=400, steps_per_round=64,
+                        yield_lanes=1)]:
+        b = _run_device(torch_cuda, det, field, cfg, trk, method=1, **launch)
+        _assert_same_results(a, b, launch)
 
 
 def test_host_api_equals_device_api(torch_cuda):
