@@ -1372,7 +1372,8 @@ dprop_status dprop_propagate_host(const dprop_config* cfg,
 namespace {
 
 // Layout of the fixed scratch: four track-index-sized arrays (sort keys and
-// indices, in and out) followed by the radix-sort temporary storage.
+// indices, the two halves of each double buffer) followed by the radix-sort
+// temporary storage (digit histograms and look-back state only).
 constexpr size_t k_noalloc_array_bytes =
     static_cast<size_t>(DPROP_NOALLOC_MAX_TRACKS) * sizeof(uint32_t);
 constexpr size_t k_noalloc_temp_offset = 4 * k_noalloc_array_bytes;
@@ -1390,23 +1391,33 @@ constexpr int k_noalloc_max_devices = 64;
 void* g_noalloc_device_ptr[k_noalloc_max_devices] = {};
 std::mutex g_noalloc_mutex;
 
-// Device address of the scratch on the current device, looked up once per
-// device (the lookup may load the module, so it must not run inside a
-// stream capture).
-dprop_status noalloc_scratch(void** out) {
+// Device address of the scratch on the current device.  Outside a stream
+// capture it is looked up on every call (cheap once the module is loaded),
+// so that an address that changed - the module is loaded again after a
+// cudaDeviceReset - is picked up; inside a capture (where the lookup, which
+// may load the module, must not run) the address of the last call on this
+// device is used, so the first call on a device must come before any
+// capture.
+dprop_status noalloc_scratch(cudaStream_t stream, void** out) {
     int dev = 0;
     DPROP_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= k_noalloc_max_devices) {
         return fail(DPROP_E_INVALID, "propagate_noalloc: device index out of range");
     }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    DPROP_CUDA(cudaStreamIsCapturing(stream, &cap));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_device_ptr[dev] == nullptr) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
             return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
         }
         g_noalloc_device_ptr[dev] = p;
+    } else if (g_noalloc_device_ptr[dev] == nullptr) {
+        return fail(DPROP_E_INVALID,
+                    "propagate_noalloc: the first call on a device must not "
+                    "be inside a stream capture");
     }
     *out = g_noalloc_device_ptr[dev];
     return DPROP_OK;
@@ -1446,43 +1457,46 @@ extern "C" dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
         return fail(DPROP_E_INVALID,
                     "propagate_noalloc: missing track/status array");
     }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     void* scratch = nullptr;
-    s = noalloc_scratch(&scratch);
+    s = noalloc_scratch(stream, &scratch);
     if (s != DPROP_OK) {
         return s;
     }
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     const int ni = static_cast<int>(n);
+    char* base = static_cast<char*>(scratch);
+    // keys and indices ping-pong between the in and out arrays (the radix
+    // sort's double-buffer form), so its temporary storage holds only the
+    // digit histograms and look-back state, not another copy of each array
+    cub::DoubleBuffer<uint32_t> keys(
+        reinterpret_cast<uint32_t*>(base),
+        reinterpret_cast<uint32_t*>(base + k_noalloc_array_bytes));
+    cub::DoubleBuffer<uint32_t> order(
+        reinterpret_cast<uint32_t*>(base + 2 * k_noalloc_array_bytes),
+        reinterpret_cast<uint32_t*>(base + 3 * k_noalloc_array_bytes));
     size_t temp_bytes = 0;
-    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
-        nullptr, temp_bytes, static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
-        static_cast<uint32_t*>(nullptr), ni, 0, 20, stream));
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys,
+                                               order, ni, 0, 20, stream));
     if (temp_bytes > k_noalloc_temp_bytes) {
         return fail(DPROP_E_INVALID,
                     "propagate_noalloc: radix-sort storage exceeds the fixed "
                     "scratch");
     }
-    char* base = static_cast<char*>(scratch);
-    uint32_t* keys_in = reinterpret_cast<uint32_t*>(base);
-    uint32_t* keys_out = reinterpret_cast<uint32_t*>(base + k_noalloc_array_bytes);
-    uint32_t* idx_in = reinterpret_cast<uint32_t*>(base + 2 * k_noalloc_array_bytes);
-    uint32_t* idx_out = reinterpret_cast<uint32_t*>(base + 3 * k_noalloc_array_bytes);
     void* temp = base + k_noalloc_temp_offset;
 
     const io_ptrs<float> io = make_io<float>(*tracks, *results);
     const unsigned int key_grid = static_cast<unsigned int>((n + 255) / 256);
     direction_key_kernel<float><<<key_grid, 256, 0, stream>>>(
-        io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, keys_in, idx_in);
+        io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, keys.Current(),
+        order.Current());
     DPROP_CUDA(cudaGetLastError());
-    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in,
-                                               keys_out, idx_in, idx_out, ni,
-                                               0, 20, stream));
+    DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, order,
+                                               ni, 0, 20, stream));
     const prop_cfg<float> pc = make_prop_cfg<float>(*cfg);
     const unsigned int grid =
         static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
     launch_plain_mb<float, DPROP_MIN_BLOCKS>(grid, stream, det, field->view, pc,
-                                             io, n, idx_out);
+                                             io, n, order.Current());
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;
 }

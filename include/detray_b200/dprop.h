@@ -525,8 +525,11 @@ dprop_status dprop_validate_navigation(const dprop_scan_results* truth,
  *
  *  - At most DPROP_NOALLOC_MAX_TRACKS tracks per call; a larger batch is
  *    rejected with DPROP_E_INVALID (split it into several calls).
- *  - The first call on a device looks up that device's copy of the array;
- *    make that first call before capturing any stream into a CUDA graph.
+ *  - Each call outside a stream capture looks up the device's copy of the
+ *    array (a call inside a capture reuses the last address found on that
+ *    device); make the first call on a device before capturing any stream
+ *    into a CUDA graph, and call again outside a capture after a
+ *    cudaDeviceReset.
  *  - Every call uses the same array: calls whose GPU work overlaps (for
  *    instance on two streams at once) race on it, so the caller must order
  *    them, e.g. by issuing them on one stream.

@@ -9,8 +9,9 @@ propagation with its sort scratch in a fixed array inside the library.
 These tests call it through the C ABI and check, on two calls in a row with
 different tracks, that it returns exactly what the allocating entry point
 dprop_propagate returns for the same tracks (both run the same per-track
-code, so the tolerance is zero), that it allocates no device memory, and
-that batches above its fixed capacity are rejected with a clear error.
+code, so the tolerance is zero), that it allocates no device memory, that
+a batch of exactly its capacity fits, and that batches above its fixed
+capacity are rejected with a clear error.
 
 The file name sorts last so that a run stopping at the first failure has
 already run every other test.
@@ -87,6 +88,24 @@ def test_noalloc_matches_allocating_entry_point(setup):
             assert np.allclose(a, b, rtol=0.0, atol=0.0), (call, key)
     # the second call runs on warm code: it must not take device memory
     assert grown[1] == 0, f"device memory shrank by {grown[1]} bytes"
+
+
+def test_noalloc_takes_its_full_capacity(setup):
+    """A batch of exactly DPROP_NOALLOC_MAX_TRACKS tracks fits the fixed
+    scratch (sort keys, indices and the radix sort's temporary storage) and
+    gives the allocating entry point's results."""
+    torch, lib, det, field, cfg = setup
+    from detray_b200 import propagator, tracks
+    n = 262_144
+    trk = torch.tensor(tracks.toy_tracks(n, seed=303), dtype=torch.float32,
+                       device="cuda")
+    ref = _host(propagator.propagate(
+        cfg, det, field, trk, launch=propagator.make_launch(sort_tracks=1)))
+    res, _ = _noalloc(torch, lib, det, field, cfg, trk)
+    got = _host(res)
+    for key in ["status", "n_records", "n_steps", "path_length",
+                "final_free"]:
+        assert np.array_equal(ref[key], got[key]), key
 
 
 def test_noalloc_rejects_batches_above_capacity(setup):
