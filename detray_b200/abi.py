@@ -270,8 +270,7 @@ class Launch(C.Structure):
         ("steps_per_round", C.c_uint32),
         ("rounds", C.c_uint32),
         ("yield_lanes", C.c_uint32),
-        ("surface_phase", C.c_uint32),
-        ("reserved", C.c_uint32 * 2),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 

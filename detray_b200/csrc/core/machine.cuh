@@ -225,9 +225,9 @@ DPROP_HD uint8_t machine_light(track_state<S>& ts, loop_state<S>& ls,
     return pc;
 }
 
+// Segments of the step phase (the surface actors run inside it).
 DPROP_HD bool machine_is_fast(uint8_t pc) {
-    return pc == pc_act || pc == pc_act_tail || pc == pc_after_nav ||
-           pc == pc_step;
+    return pc != pc_nav && pc != pc_done;
 }
 
 // Run a track from its current segment to the end, every segment inline

@@ -61,7 +61,12 @@ struct nav_state {
     // candidate is reached the next index points one past the cache, and a
     // read there (which the reference does on its fixed-size array) finds
     // an unreachable candidate instead of leaving the state.
-    candidate<S> cand[k_cache + 1];
+    // The cache lives outside this struct, in an array of k_cache + 1
+    // candidates the owner binds here (nav_cache): indexed with the
+    // run-time cache index, an array inside the state would make the
+    // compiler keep the whole per-track state in the thread's stack instead
+    // of registers.
+    candidate<S>* cand;
     int8_t next;
     int8_t last;
     int8_t status;
@@ -129,6 +134,18 @@ struct nav_state {
         reason = why;
     }
 };
+
+// Storage of a candidate cache (k_cache candidates and the sentinel); bind
+// it to a state with bind_cache before the state is used.
+template <typename S>
+struct nav_cache {
+    candidate<S> c[k_cache + 1];
+};
+
+template <typename S>
+DPROP_HD void bind_cache(nav_state<S>& nav, nav_cache<S>& cache) {
+    nav.cand = cache.c;
+}
 
 // Track position and direction seen by the navigator
 template <typename S>

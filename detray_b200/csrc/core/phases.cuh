@@ -6,10 +6,10 @@
 // bit-identical to propagate_track.
 //
 //   phase_init   propagation start: track state, navigator initialisation
-//   fast phase   the loop's light segments and RK steps (with the
-//                high-trust navigation update) until the track needs the
-//                surface actors, the volume-level navigation update, or ends
-//   phase_surf   the surface actors (transport, material, setter, recorder)
+//   fast phase   the loop's light segments, RK steps (with the high-trust
+//                navigation update) and the surface actors (transport,
+//                material, setter, recorder) until the track needs the
+//                volume-level navigation update, or ends
 //   phase_nav    the navigation update's cache re-evaluation / volume switch
 //   phase_tail   the whole remaining loop inline
 #pragma once
@@ -22,9 +22,6 @@ template <bool W>
 constexpr uint32_t fast_groups() {
     return g_step | g_meta | g_loop | (W ? g_cyc : 0u);
 }
-constexpr uint32_t k_surf_load =
-    g_free | g_jac | g_pathdtds | g_meta | g_bound | g_loop | g_count;
-constexpr uint32_t k_surf_store = g_free | g_jac | g_meta | g_bound | g_count;
 constexpr uint32_t k_nav_load = g_free | g_meta | g_loop;
 constexpr uint32_t k_nav_store = g_meta | g_loop;
 
@@ -67,7 +64,9 @@ DPROP_HD void phase_init(const slot_soa<S>& s, uint64_t slot, uint32_t track,
                          vec3<S> pos, S time, vec3<S> dir, S qop,
                          const detector_view<S, W>& det,
                          const prop_cfg<S>& cfg) {
+    nav_cache<S> cache;
     track_state<S> ts;
+    bind_cache(ts.nav, cache);
     loop_state<S> ls;
     init_track_state(ts, pos, time, dir, qop, cfg);
     machine_init(ts, ls, det, cfg);
@@ -137,9 +136,9 @@ DPROP_HD void surf_inline(track_state<S>& ts, const slot_soa<S>& s,
     s.rec_count[slot] = rec.count;
 }
 
-// Light segments (with InlineSurf also the surface actors) and at most one
-// RK step; returns the next segment.
-template <typename S, bool W, bool InlineSurf>
+// Light segments, the surface actors and at most one RK step; returns the
+// next segment.
+template <typename S, bool W>
 DPROP_HD uint8_t fast_advance(track_state<S>& ts, loop_state<S>& ls,
                               cand_window& w, const slot_soa<S>& s,
                               uint64_t slot, const detector_view<S, W>& det,
@@ -147,12 +146,10 @@ DPROP_HD uint8_t fast_advance(track_state<S>& ts, loop_state<S>& ls,
                               const prop_cfg<S>& cfg, record_sink<S>& rec) {
     ensure_cands(s, slot, ts.nav, w);
     uint8_t pc = machine_light(ts, ls, det, cfg, ls.pc);
-    if constexpr (InlineSurf) {
-        if (pc == pc_surf) {
-            surf_inline(ts, s, slot, det, field, cfg, rec);
-            ensure_cands(s, slot, ts.nav, w);
-            pc = machine_light(ts, ls, det, cfg, pc_act_tail);
-        }
+    if (pc == pc_surf) {
+        surf_inline(ts, s, slot, det, field, cfg, rec);
+        ensure_cands(s, slot, ts.nav, w);
+        pc = machine_light(ts, ls, det, cfg, pc_act_tail);
     }
     if (pc == pc_step) {
         ensure_cands(s, slot, ts.nav, w);
@@ -173,37 +170,14 @@ DPROP_HD void fast_store(const slot_soa<S>& s, uint64_t slot,
     s.pc[slot] = ls.pc;
 }
 
-// ------------------------------------------------------------------ surf
-// The surface actors of slot `slot`; records go to rec (whose count and
-// track the phase sets from the slot).
-template <typename S, bool W>
-DPROP_HD void phase_surf(const slot_soa<S>& s, uint64_t slot,
-                         const detector_view<S, W>& det,
-                         const field_view<S>& field, const prop_cfg<S>& cfg,
-                         record_sink<S>& rec) {
-    track_state<S> ts;
-    loop_state<S> ls;
-    load_slot(s, slot, k_surf_load, ts, ls);
-    const int nx = ts.nav.next;
-    int lo, hi;
-    cand_range(nx - 1, nx, lo, hi);
-    for (int k = lo; k <= hi; ++k) {
-        load_cand(s, slot, k, ts.nav.cand[k]);
-    }
-    rec.count = s.rec_count[slot];
-    rec.track = s.track[slot];
-    const uint8_t pc = machine_surf(ts, det, field, cfg, rec, no_tape{});
-    store_slot(s, slot, k_surf_store, ts, ls);
-    s.rec_count[slot] = rec.count;
-    s.pc[slot] = pc;
-}
-
 // ------------------------------------------------------------------- nav
 template <typename S, bool W>
 DPROP_HD void phase_nav(const slot_soa<S>& s, uint64_t slot,
                         const detector_view<S, W>& det,
                         const prop_cfg<S>& cfg) {
+    nav_cache<S> cache;
     track_state<S> ts;
+    bind_cache(ts.nav, cache);
     loop_state<S> ls;
     load_slot(s, slot, k_nav_load, ts, ls);
     for (int k = 0; k <= k_cache; ++k) {
@@ -226,7 +200,9 @@ DPROP_HD track_outputs<S> phase_tail(const slot_soa<S>& s, uint64_t slot,
                                      const field_view<S>& field,
                                      const prop_cfg<S>& cfg,
                                      record_sink<S>& rec) {
+    nav_cache<S> cache;
     track_state<S> ts;
+    bind_cache(ts.nav, cache);
     loop_state<S> ls;
     load_slot(s, slot, g_step | g_meta | g_bound | g_loop | g_count |
                            (W ? g_cyc : 0u),

@@ -69,7 +69,9 @@ __global__ void __launch_bounds__(k_direct_block)
         qop = io.trk[7][t];
     }
 
+    nav_cache<float> cache;
     track_state<float> ts;
+    bind_cache(ts.nav, cache);
     init_track_state(ts, pos, time, dir, qop, cfg);
     ts.nav.direction = dio.direction;
 

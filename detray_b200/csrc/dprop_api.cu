@@ -1066,15 +1066,23 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
     r.rec_flags = reinterpret_cast<uint8_t*>(take(cap * m));
     const io_ptrs<float> io = make_io<float>(*tracks, r);
 
+    // plain: register budget (resident CTAs per SM) x direction sort;
+    // persistent: step-phase register budget x steps per round x tracks per
+    // warp (yield lanes) x rounds x direction sort
     struct cand {
-        uint32_t method, ctas, sort;
+        uint32_t method, ctas, sort, steps, yield, rounds;
     };
     const cand cands[DPROP_AUTOTUNE_CANDIDATES] = {
-        {DPROP_METHOD_PLAIN, 8, 1},       {DPROP_METHOD_PLAIN, 12, 1},
-        {DPROP_METHOD_PLAIN, 16, 1},      {DPROP_METHOD_PERSISTENT, 8, 1},
-        {DPROP_METHOD_PERSISTENT, 12, 1}, {DPROP_METHOD_PERSISTENT, 16, 1},
-        {DPROP_METHOD_PLAIN, 8, 0},       {DPROP_METHOD_PLAIN, 12, 0},
-        {DPROP_METHOD_PLAIN, 16, 0},      {DPROP_METHOD_PERSISTENT, 16, 0}};
+        {DPROP_METHOD_PLAIN, 8, 1, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 12, 1, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 16, 1, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 16, 0, 0, 0, 0},
+        {DPROP_METHOD_PERSISTENT, 3, 1, 16, 16, 64},
+        {DPROP_METHOD_PERSISTENT, 4, 1, 16, 16, 64},
+        {DPROP_METHOD_PERSISTENT, 5, 1, 16, 16, 64},
+        {DPROP_METHOD_PERSISTENT, 4, 1, 16, 8, 96},
+        {DPROP_METHOD_PERSISTENT, 4, 1, 64, 12, 64},
+        {DPROP_METHOD_PERSISTENT, 4, 0, 16, 16, 64}};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1085,6 +1093,9 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
         lc.method = cands[i].method;
         lc.ctas_per_sm = cands[i].ctas;
         lc.sort_tracks = cands[i].sort;
+        lc.steps_per_round = cands[i].steps;
+        lc.yield_lanes = cands[i].yield;
+        lc.rounds = cands[i].rounds;
         s = launch<float>(*cfg, &lc, det, field, io, m, stream);  // warm-up
         if (s != DPROP_OK) break;
         cudaEventRecord(e0, stream);
@@ -1115,6 +1126,9 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
     launch_out->method = cands[best_i].method;
     launch_out->ctas_per_sm = cands[best_i].ctas;
     launch_out->sort_tracks = cands[best_i].sort;
+    launch_out->steps_per_round = cands[best_i].steps;
+    launch_out->yield_lanes = cands[best_i].yield;
+    launch_out->rounds = cands[best_i].rounds;
     return DPROP_OK;
 }
 

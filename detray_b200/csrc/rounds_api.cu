@@ -12,16 +12,14 @@
 //   queue_count_kernel / queue_scatter_kernel
 //       read the one-byte next-segment array of all slots and write the
 //       slots of each phase, in slot (= direction) order, into the work
-//       queues of the step, surface and navigation phases;
+//       queues of the step and navigation phases;
 //   rounds_fast_kernel
 //       the step phase: RK steps with the high-trust navigation update,
-//       the path-limit aborter and (by default) the surface actors, until a
-//       track needs the volume-level navigation update or ends.  A warp
-//       stops its round once fewer than yield_lanes of its lanes can still
-//       step (a warp vote after every step), so that warps do not run on
-//       with a few lanes;
-//   rounds_surf_kernel (surface_phase = 1)
-//       the surface actors;
+//       the path-limit aborter and the surface actors (transport, material,
+//       setter, recorder), until a track needs the volume-level navigation
+//       update or ends.  A warp stops its round once fewer than yield_lanes
+//       of its lanes can still step (a warp vote after every step), so that
+//       warps do not run on with a few lanes;
 //   rounds_nav_kernel
 //       the navigation update's cache re-evaluation, volume switch and local
 //       navigation (grid and portal search), with all lanes of a warp doing
@@ -37,6 +35,8 @@
 
 #include <cub/block/block_scan.cuh>
 
+#include <type_traits>
+
 #include "api_common.cuh"
 #include "core/phases.cuh"
 #include "track_io.cuh"
@@ -50,8 +50,9 @@ static_assert(k_build_threads * 16 == static_cast<int>(k_queue_tile),
               "queue tile = 16 slots per thread");
 constexpr int k_phase_block = 128;
 
-// Queue of a segment: 0 step phase, 1 surface actors, 2 navigation, -1
-// ended.  merged: every live slot in queue 0 (the tail).
+// Queue of a segment: 0 step phase, 2 navigation, -1 ended (queue 1 holds
+// tracks waiting for the surface actors, which the step phase runs itself,
+// so it stays empty).  merged: every live slot in queue 0 (the tail).
 __device__ __forceinline__ int queue_of(uint32_t pc, bool merged) {
     if (pc == pc_done) {
         return -1;
@@ -261,13 +262,12 @@ __global__ void __launch_bounds__(k_phase_block)
     }
 }
 
-#ifndef DPROP_FAST_MIN_BLOCKS
-#define DPROP_FAST_MIN_BLOCKS 4
-#endif
-
-// The step phase.
-template <typename In, bool W, bool InlineSurf>
-__global__ void __launch_bounds__(k_phase_block, DPROP_FAST_MIN_BLOCKS)
+// The step phase, compiled for MinBlocks resident CTAs per SM: 3 (up to 168
+// registers: the state and the step's temporaries fit without spills), 4
+// (128) or 5 (102).  The best budget depends on the workload (more warps
+// hide the field map's gather latency), so it is a launch choice.
+template <typename In, bool W, int MinBlocks>
+__global__ void __launch_bounds__(k_phase_block, MinBlocks)
     rounds_fast_kernel(const __grid_constant__ detector_view<float, W> det,
                        const __grid_constant__ field_view<float> field,
                        const __grid_constant__ prop_cfg<float> cfg,
@@ -287,7 +287,9 @@ __global__ void __launch_bounds__(k_phase_block, DPROP_FAST_MIN_BLOCKS)
         const uint32_t idx = base + lane;
         const bool valid = idx < cnt;
         const uint64_t slot = valid ? queue[idx] : 0u;
+        nav_cache<float> cache;
         track_state<float> ts;
+        bind_cache(ts.nav, cache);
         loop_state<float> ls;
         cand_window win;
         if (valid) {
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(k_phase_block, DPROP_FAST_MIN_BLOCKS)
         bool active = valid;
         for (uint32_t it = 0;; ++it) {
             if (active) {
-                const uint8_t pc = fast_advance<float, W, InlineSurf>(
+                const uint8_t pc = fast_advance<float, W>(
                     ts, ls, win, s, slot, det, field, cfg, rec);
                 active = machine_is_fast(pc);
             }
@@ -314,32 +316,6 @@ __global__ void __launch_bounds__(k_phase_block, DPROP_FAST_MIN_BLOCKS)
                               fast_outputs(s, slot, ts, ls));
             }
         }
-    }
-}
-
-// The surface actors.
-template <typename In, bool W>
-__global__ void __launch_bounds__(k_phase_block, 4)
-    rounds_surf_kernel(const __grid_constant__ detector_view<float, W> det,
-                       const __grid_constant__ field_view<float> field,
-                       const __grid_constant__ prop_cfg<float> cfg,
-                       const __grid_constant__ api::io_ptrs<In> io,
-                       const __grid_constant__ slot_soa<float> s,
-                       const uint32_t* __restrict__ queue,
-                       const uint32_t* __restrict__ count, uint32_t* pull,
-                       uint64_t n) {
-    const uint32_t cnt = *count;
-    record_sink<float> rec = make_sink(io, n, cfg);
-    while (true) {
-        const uint32_t base = pull32(pull);
-        if (base >= cnt) {
-            break;
-        }
-        const uint32_t idx = base + (threadIdx.x & 31u);
-        if (idx < cnt) {
-            phase_surf<float, W>(s, queue[idx], det, field, cfg, rec);
-        }
-        __syncwarp();
     }
 }
 
@@ -441,7 +417,7 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, rounds_layout* out,
     return off;
 }
 
-template <typename In, bool W, bool InlineSurf>
+template <typename In, bool W, int FastBlocks>
 dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                               const field_view<float>& field,
                               const prop_cfg<float>& cfg,
@@ -451,11 +427,10 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                               uint32_t yield_lanes, cudaStream_t st) {
     const uint64_t n_pad = L.n_tiles * k_queue_tile;
     const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
-    unsigned int g_init = 0, g_fast = 0, g_surf = 0, g_nav = 0, g_tail = 0;
+    unsigned int g_init = 0, g_fast = 0, g_nav = 0, g_tail = 0;
     dprop_status s = DPROP_OK;
     if ((s = resident_grid(rounds_init_kernel<In, W>, &g_init)) != DPROP_OK ||
-        (s = resident_grid(rounds_fast_kernel<In, W, InlineSurf>, &g_fast)) != DPROP_OK ||
-        (s = resident_grid(rounds_surf_kernel<In, W>, &g_surf)) != DPROP_OK ||
+        (s = resident_grid(rounds_fast_kernel<In, W, FastBlocks>, &g_fast)) != DPROP_OK ||
         (s = resident_grid(rounds_nav_kernel<W>, &g_nav)) != DPROP_OK ||
         (s = resident_grid(rounds_tail_kernel<In, W>, &g_tail)) != DPROP_OK) {
         return s;
@@ -477,14 +452,9 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
             DPROP_CUDA(cudaGetLastError());
             break;
         }
-        rounds_fast_kernel<In, W, InlineSurf><<<g_fast, k_phase_block, 0, st>>>(
+        rounds_fast_kernel<In, W, FastBlocks><<<g_fast, k_phase_block, 0, st>>>(
             det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count, L.qs.pull, n,
             step_budget, yield_lanes);
-        if (!InlineSurf) {
-            rounds_surf_kernel<In, W><<<g_surf, k_phase_block, 0, st>>>(
-                det, field, cfg, io, L.slots, L.qs.q[1], L.qs.count + 1,
-                L.qs.pull + 1, n);
-        }
         rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
             det, cfg, L.slots, L.qs.q[2], L.qs.count + 2, L.qs.pull + 2);
         DPROP_CUDA(cudaGetLastError());
@@ -497,8 +467,8 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
 namespace dprop::api {
 
 constexpr uint32_t k_default_steps_per_round = 16u;
-constexpr uint32_t k_default_rounds = 96u;
-constexpr uint32_t k_default_yield_lanes = 8u;
+constexpr uint32_t k_default_rounds = 64u;
+constexpr uint32_t k_default_yield_lanes = 16u;
 
 size_t rounds_scratch_bytes(uint64_t n, bool wires) {
     return rounds_layout_bytes(n, wires, nullptr, nullptr) + 256u;
@@ -529,21 +499,32 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
         return fail(DPROP_E_INVALID,
                     "persistent method: rounds > 100000 or yield_lanes > 32");
     }
-    const bool inline_surf = !(lc && lc->surface_phase);
-    if (det->wires) {
-        const detector_view<float, true> dv = det->view_as<true>();
-        return inline_surf
-                   ? enqueue_rounds_w<In, true, true>(dv, field->view, cfg, io, n, order, L,
-                                                      rounds, budget, yield, stream)
-                   : enqueue_rounds_w<In, true, false>(dv, field->view, cfg, io, n, order, L,
-                                                       rounds, budget, yield, stream);
+    // register budget of the step phase: resident CTAs per SM 3, 4 or 5
+    const uint32_t fb = (lc && lc->ctas_per_sm) ? lc->ctas_per_sm : 4u;
+    if (fb < 3u || fb > 5u) {
+        return fail(DPROP_E_INVALID,
+                    "persistent method: ctas_per_sm must be 0, 3, 4 or 5");
     }
-    const detector_view<float, false> dv = det->view_as<false>();
-    return inline_surf
-               ? enqueue_rounds_w<In, false, true>(dv, field->view, cfg, io, n, order, L,
-                                                   rounds, budget, yield, stream)
-               : enqueue_rounds_w<In, false, false>(dv, field->view, cfg, io, n, order, L,
-                                                    rounds, budget, yield, stream);
+    auto go = [&](auto fast_blocks) -> dprop_status {
+        constexpr int FB = decltype(fast_blocks)::value;
+        if (det->wires) {
+            return enqueue_rounds_w<In, true, FB>(det->view_as<true>(),
+                                                  field->view, cfg, io, n,
+                                                  order, L, rounds, budget,
+                                                  yield, stream);
+        }
+        return enqueue_rounds_w<In, false, FB>(det->view_as<false>(),
+                                               field->view, cfg, io, n, order,
+                                               L, rounds, budget, yield,
+                                               stream);
+    };
+    if (fb == 3u) {
+        return go(std::integral_constant<int, 3>{});
+    }
+    if (fb == 5u) {
+        return go(std::integral_constant<int, 5>{});
+    }
+    return go(std::integral_constant<int, 4>{});
 }
 
 template dprop_status enqueue_rounds<float>(const dprop_launch*,

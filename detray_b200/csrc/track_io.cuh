@@ -78,7 +78,9 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     const S time = static_cast<S>(io.trk[3][t]);
     const S qop = static_cast<S>(io.trk[7][t]);
 
+    nav_cache<S> cache;
     track_state<S> ts;
+    bind_cache(ts.nav, cache);
     init_track_state(ts, pos, time, dir, qop, cfg);
 
     record_sink<S> rec;

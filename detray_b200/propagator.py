@@ -184,11 +184,11 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
                 ctas_per_sm: int = 0, sort_tracks: int = 0,
                 use_graph: int = 0, precision: int = 0,
                 steps_per_round: int = 0, rounds: int = 0,
-                yield_lanes: int = 0, surface_phase: int = 0) -> abi.Launch:
+                yield_lanes: int = 0) -> abi.Launch:
     """Launch shape; ``precision`` 8 runs the propagation in fp64 end to end
-    (double track tensors and results).  steps_per_round, rounds,
-    yield_lanes and surface_phase shape the persistent (round-based) method;
-    0 picks the library default."""
+    (double track tensors and results).  steps_per_round, rounds and
+    yield_lanes shape the persistent (round-based) method; 0 picks the
+    library default."""
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
@@ -199,7 +199,6 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
     lc.steps_per_round = steps_per_round
     lc.rounds = rounds
     lc.yield_lanes = yield_lanes
-    lc.surface_phase = surface_phase
     return lc
 
 
@@ -526,11 +525,14 @@ def propagate_host(cfg: abi.Config, det: Detector, field: Field,
     return res
 
 
+# the candidates dprop_autotune times, in its order:
+# (method, ctas_per_sm, sort_tracks, steps_per_round, yield_lanes, rounds)
 AUTOTUNE_CANDIDATES = [
-    ("plain", 8, 1), ("plain", 12, 1), ("plain", 16, 1),
-    ("persistent", 8, 1), ("persistent", 12, 1), ("persistent", 16, 1),
-    ("plain", 8, 0), ("plain", 12, 0), ("plain", 16, 0),
-    ("persistent", 16, 0)]
+    ("plain", 8, 1, 0, 0, 0), ("plain", 12, 1, 0, 0, 0),
+    ("plain", 16, 1, 0, 0, 0), ("plain", 16, 0, 0, 0, 0),
+    ("persistent", 3, 1, 16, 16, 64), ("persistent", 4, 1, 16, 16, 64),
+    ("persistent", 5, 1, 16, 16, 64), ("persistent", 4, 1, 16, 8, 96),
+    ("persistent", 4, 1, 64, 12, 64), ("persistent", 4, 0, 16, 16, 64)]
 
 
 def autotune(cfg: abi.Config, det: Detector, field: Field, tracks,

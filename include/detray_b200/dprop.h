@@ -302,11 +302,10 @@ typedef enum dprop_method {
                                     sorts the live tracks into the work
                                     queues of the step phase (RK steps,
                                     high-trust navigation, path-limit
-                                    aborter and - unless surface_phase - the
-                                    surface actors), the surface phase and
-                                    the navigation phase (cache
-                                    re-evaluation, volume switch), in
-                                    direction order, and persistent
+                                    aborter, surface actors) and the
+                                    navigation phase (cache re-evaluation,
+                                    volume switch), in direction order, and
+                                    persistent
                                     grid-stride kernels pull their tracks
                                     from those queues; after `rounds` rounds
                                     the tracks still alive finish in one
@@ -318,9 +317,11 @@ typedef struct dprop_launch {
     uint32_t method;             /* dprop_method                               */
     uint32_t block_size;         /* threads per CTA (0: default)               */
     uint32_t ctas_per_sm;        /* register budget: resident CTAs of 128
-                                    threads per SM the kernel is compiled for,
-                                    8 (64 registers), 12 (40) or 16 (32);
-                                    0 = 12.  Plain method                     */
+                                    threads per SM the kernel is compiled for.
+                                    Plain method: 8 (64 registers), 12 (40)
+                                    or 16 (32); 0 = 12.  Persistent method,
+                                    its step phase: 3 (168 registers), 4
+                                    (128) or 5 (102); 0 = 4                   */
     uint32_t sort_tracks;        /* 1: process tracks ordered by direction
                                     (theta, phi) so that the lanes of a warp
                                     follow similar paths; results are still
@@ -340,14 +341,11 @@ typedef struct dprop_launch {
                                     (default 16)                               */
     uint32_t rounds;             /* rounds of the phase kernels before the
                                     tracks still alive finish in one kernel
-                                    (default 96)                               */
+                                    (default 64)                               */
     uint32_t yield_lanes;        /* tracks per warp: a warp of the step phase
                                     ends its round once fewer than this many of
-                                    its 32 lanes can still step (default 8)    */
-    uint32_t surface_phase;      /* 1: the surface actors run in a phase
-                                    kernel of their own; 0: inside the step
-                                    phase (default)                           */
-    uint32_t reserved[2];
+                                    its 32 lanes can still step (default 16)   */
+    uint32_t reserved[3];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */
@@ -543,13 +541,17 @@ dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
                                      const dprop_results* results,
                                      uint64_t n_tracks, void* stream);
 
-/* Autotuner: times candidate launch forms - plain and persistent kernels at
- * the three register budgets (ctas_per_sm 8, 12, 16), with and without the
- * direction sort - on the first min(n_tracks, 262144) of the given device
- * tracks, and writes the fastest into *launch (method, ctas_per_sm,
- * sort_tracks; use_graph is left as given).  If timings_ms is not NULL it
- * receives one time per candidate (DPROP_AUTOTUNE_CANDIDATES entries).
- * Allocates temporary device result buffers for the trial runs. */
+/* Autotuner: times candidate launch forms - the plain kernel at the three
+ * register budgets (ctas_per_sm 8, 12, 16) with the direction sort and at 16
+ * without it; the persistent method with and without the sort over its
+ * step-phase register budget (ctas_per_sm 3, 4, 5), steps per round, tracks
+ * per warp (yield_lanes 8, 12, 16) and the number of rounds before the tail
+ * kernel - on the first min(n_tracks, 262144) of the given
+ * device tracks, and writes the fastest into *launch (method, ctas_per_sm,
+ * sort_tracks, steps_per_round, yield_lanes, rounds; use_graph is left as
+ * given).  If timings_ms is not NULL it receives one time per candidate
+ * (DPROP_AUTOTUNE_CANDIDATES entries).  Allocates temporary device result
+ * buffers for the trial runs. */
 #define DPROP_AUTOTUNE_CANDIDATES 10
 dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
                             const dprop_field* field,

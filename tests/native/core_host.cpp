@@ -83,7 +83,9 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
     const prop_cfg<S> cfg = make_prop_cfg<S>(*c);
     const uint32_t cap = c->max_records;
     for (uint64_t t = 0; t < n; ++t) {
+        nav_cache<S> cache;
         track_state<S> ts;
+        bind_cache(ts.nav, cache);
         bool start_ok = true;
         if (da != nullptr && da->start_barcode != nullptr) {
             S bs[6];
@@ -204,9 +206,11 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
     return 0;
 }
 template <typename S>
-void poison(track_state<S>& ts, loop_state<S>& ls) {
+void poison(track_state<S>& ts, loop_state<S>& ls, nav_cache<S>& cache) {
     std::memset(static_cast<void*>(&ts), 0xff, sizeof(ts));
     std::memset(static_cast<void*>(&ls), 0xff, sizeof(ls));
+    std::memset(static_cast<void*>(&cache), 0xff, sizeof(cache));
+    bind_cache(ts.nav, cache);
 }
 
 template <typename S>
@@ -245,7 +249,7 @@ field_view<S> host_field(uint32_t field_kind, const double* b,
     return f;
 }
 
-template <typename S, bool W, bool InlineSurf>
+template <typename S, bool W>
 int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
                  const double* b, const double* lo, const double* hi,
                  const uint32_t* nn, const float* values,
@@ -343,12 +347,13 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
         // fast phase, in groups of 32 queue entries
         for (size_t g0 = 0; g0 < qf.size(); g0 += 32u) {
             const size_t m = (qf.size() - g0) < 32u ? qf.size() - g0 : 32u;
+            nav_cache<S> cache[32];
             track_state<S> ts[32];
             loop_state<S> ls[32];
             cand_window c0[32];
             bool active[32];
             for (size_t l = 0; l < m; ++l) {
-                poison(ts[l], ls[l]);
+                poison(ts[l], ls[l], cache[l]);
                 fast_load<S, W>(s, qf[g0 + l], ts[l], ls[l], c0[l]);
                 active[l] = true;
             }
@@ -356,7 +361,7 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
                 uint32_t n_active = 0;
                 for (size_t l = 0; l < m; ++l) {
                     if (!active[l]) continue;
-                    const uint8_t pc = fast_advance<S, W, InlineSurf>(
+                    const uint8_t pc = fast_advance<S, W>(
                         ts[l], ls[l], c0[l], s, qf[g0 + l], det, f, cfg, rec);
                     active[l] = machine_is_fast(pc);
                     n_active += active[l] ? 1u : 0u;
@@ -373,9 +378,6 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
                     emit(fast_outputs(s, slot, ts[l], ls[l]), s.track[slot]);
                 }
             }
-        }
-        for (const uint64_t slot : qs) {
-            phase_surf<S, W>(s, slot, det, f, cfg, rec);
         }
         for (const uint64_t slot : qn) {
             phase_nav<S, W>(s, slot, det, cfg);
@@ -401,11 +403,10 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
 
 // The round-based propagation of the phase kernels, simulated on the host
 // with the same phase bodies: every round classifies the slots by their next
-// segment first (as the queue builder does), then runs the fast phase (with
-// inline_surf, the surface actors inside it) over
+// segment first (as the queue builder does), then runs the step phase over
 // groups of 32 slots with the kernel's yield rule (all lanes of a group stop
 // once fewer than yield_min of them are still in the fast phase, or after
-// step_budget steps), the surface actors and the navigation phase.  After
+// step_budget steps) and the navigation phase.  After
 // `rounds` rounds the remaining slots run the tail.  The local state is
 // filled with a poison byte before every load, so a segment reading a field
 // its phase does not load changes the results.  stats (optional, rounds + 1
@@ -416,7 +417,7 @@ int run_rounds(const dprop_detector_desc* desc, uint32_t field_kind,
                const uint32_t* nn, const float* values, const dprop_config* c,
                const double* const* trk, uint64_t n, const dprop_results* out,
                uint32_t rounds, uint32_t step_budget, uint32_t yield_min,
-               bool inline_surf, uint32_t* stats) {
+               uint32_t* stats) {
     const std::string problem = validate_desc(desc);
     if (!problem.empty()) {
         g_err = problem;
@@ -435,23 +436,14 @@ int run_rounds(const dprop_detector_desc* desc, uint32_t field_kind,
         wires = wires || desc->grids[i].multi != 0u;
     }
     if (!wires) {
-        if (inline_surf) {
-            return run_rounds_w<S, false, true>(
-                tables.template view_as<false>(), field_kind, b, lo, hi, nn,
-                values, c, trk, n, out, rounds, step_budget, yield_min, stats);
-        }
-        return run_rounds_w<S, false, false>(
-            tables.template view_as<false>(), field_kind, b, lo, hi, nn,
-            values, c, trk, n, out, rounds, step_budget, yield_min, stats);
+        return run_rounds_w<S, false>(tables.template view_as<false>(),
+                                      field_kind, b, lo, hi, nn, values, c,
+                                      trk, n, out, rounds, step_budget,
+                                      yield_min, stats);
     }
-    if (inline_surf) {
-        return run_rounds_w<S, true, true>(
-            tables.template view_as<true>(), field_kind, b, lo, hi, nn, values,
-            c, trk, n, out, rounds, step_budget, yield_min, stats);
-    }
-    return run_rounds_w<S, true, false>(
-        tables.template view_as<true>(), field_kind, b, lo, hi, nn, values, c,
-        trk, n, out, rounds, step_budget, yield_min, stats);
+    return run_rounds_w<S, true>(tables.template view_as<true>(), field_kind,
+                                 b, lo, hi, nn, values, c, trk, n, out,
+                                 rounds, step_budget, yield_min, stats);
 }
 
 }  // namespace
@@ -480,15 +472,15 @@ int core_host_propagate_rounds(int precision_bytes,
                                const double* const* trk, uint64_t n,
                                const dprop_results* out, uint32_t rounds,
                                uint32_t step_budget, uint32_t yield_min,
-                               int inline_surf, uint32_t* stats) {
+                               uint32_t* stats) {
     if (precision_bytes == 8) {
         return run_rounds<double>(desc, field_kind, b, lo, hi, nn, values, cfg,
                                   trk, n, out, rounds, step_budget, yield_min,
-                                  inline_surf != 0, stats);
+                                  stats);
     }
     return run_rounds<float>(desc, field_kind, b, lo, hi, nn, values, cfg,
                              trk, n, out, rounds, step_budget, yield_min,
-                             inline_surf != 0, stats);
+                             stats);
 }
 
 // Direct-navigation propagation (constant field b): as

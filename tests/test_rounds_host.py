@@ -1,8 +1,7 @@
 """The round-based propagation (the persistent method's phase kernels),
 simulated on the host with the same phase bodies and the same partial state
 loads: every track must end bit-identical to the one-shot propagation loop
-(propagate_track), whatever the round count, step budget, yield rule and
-placement of the surface actors.  State a phase does not load is filled with
+(propagate_track), whatever the round count, step budget and yield rule.  State a phase does not load is filled with
 a poison byte, so a segment that reads a field its phase does not load shows
 up as a mismatch."""
 import ctypes as C
@@ -28,7 +27,7 @@ def _field_args(fmap):
 
 
 def _run(core_host, oracle, det, trk, cfg, fmap, prec, rounds=None,
-         budget=16, yield_min=8, inline_surf=1):
+         budget=16, yield_min=8):
     n = trk.shape[1]
     res, r = oracle.alloc_results(n, cfg.max_records)
     trk = np.ascontiguousarray(trk)
@@ -44,7 +43,7 @@ def _run(core_host, oracle, det, trk, cfg, fmap, prec, rounds=None,
         rc = core_host.core_host_propagate_rounds(
             prec, C.byref(det.desc), kind, b, lo, hi, nn, vp, C.byref(cfg),
             ptrs, C.c_uint64(n), C.byref(r), rounds, budget, yield_min,
-            inline_surf, stats.ctypes.data_as(C.c_void_p))
+            stats.ctypes.data_as(C.c_void_p))
     assert rc == 0, core_host.core_host_last_error()
     return res, stats
 
@@ -95,20 +94,19 @@ def _case(oracle, kind):
 def test_rounds_equal_one_shot_loop(core_host, oracle, kind, prec):
     det, trk, cfg, fmap = _case(oracle, kind)
     ref, _ = _run(core_host, oracle, det, trk, cfg, fmap, prec)
-    # (rounds, step budget, yield lanes, surface actors inline)
-    for params in [(300, 16, 8, 1), (300, 4, 30, 0), (7, 3, 16, 1),
-                   (40, 1000, 1, 0)]:
+    # (rounds, step budget, yield lanes)
+    for params in [(300, 16, 8), (300, 4, 30), (7, 3, 16), (40, 1000, 1)]:
         got, stats = _run(core_host, oracle, det, trk, cfg, fmap, prec,
                           *params)
         _assert_identical(ref, got)
 
 
 def test_rounds_queue_statistics(core_host, oracle):
-    """The toy detector's tracks finish within a few dozen rounds with the
-    surface actors in the step phase, and the surface queue stays empty
-    then."""
+    """The toy detector's tracks finish within a few dozen rounds (the
+    surface actors run inside the step phase, so no track ever waits in the
+    surface queue)."""
     det, trk, cfg, fmap = _case(oracle, "toy")
-    _, stats = _run(core_host, oracle, det, trk, cfg, fmap, 4, 200, 16, 8, 1)
+    _, stats = _run(core_host, oracle, det, trk, cfg, fmap, 4, 200, 16, 8)
     q = stats.reshape(-1, 3)
     assert q[:, 1].sum() == 0
     live = np.nonzero(q.sum(axis=1))[0]
