@@ -57,8 +57,8 @@ def parse_args():
     p.add_argument("--no-sort", action="store_true",
                    help="propagate in input order instead of direction order")
     p.add_argument("--ctas", type=int, default=12, choices=(8, 12, 16),
-                   help="register budget (resident CTAs per SM) when "
-                        "--method is not auto")
+                   help="register budget (resident CTAs per SM) of the "
+                        "plain method when --method is plain")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true",
@@ -71,8 +71,37 @@ def parse_args():
                         "(telescope; toy in the solenoid map; toy + wire "
                         "chamber in fp32 and fp64) instead of the headline "
                         "line")
+    p.add_argument("--no-config3", action="store_true",
+                   help="skip the field-map configuration object")
+    p.add_argument("--dry-run", action="store_true",
+                   help="no GPU work: start the ranks (gloo without CUDA), "
+                        "shard the batch and print the line with the shard "
+                        "sizes (the CPU check of the multi-GPU launcher)")
     p.add_argument("--seed", type=int, default=20241203)
     return p.parse_args()
+
+
+def spawn_ranks(args) -> int | None:
+    """--gpus N > 1 outside a torchrun launch: start N ranks (one process per
+    GPU) through torch.distributed.run on this node and return their exit
+    code; inside a launch, check that the world size is N."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE "
+                             f"{world}")
+        return None
+    if args.gpus <= 1:
+        return None
+    import socket
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           f"--master-port={port}", str(Path(__file__).resolve()),
+           *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def workload_config():
@@ -288,9 +317,14 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available() and not args.dry_run:
+            torch.cuda.set_device(local)
+            dist.init_process_group(
+                "nccl", timeout=datetime.timedelta(seconds=120),
+                device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo",
+                                    timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -300,12 +334,18 @@ def barrier(world):
         dist.barrier()
 
 
+def _reduce_device():
+    import torch
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def max_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -315,7 +355,7 @@ def sum_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -432,20 +472,104 @@ def extra_rows(cfg, det, field, trk, res, stream, dev, steps=5, warmup=2,
     }
 
 
+def parity_sample(cfg, host_trk, res, k):
+    """Parity of the timed run on its own workload: the first k tracks of
+    the batch through the reference's fp64 CPU propagator (the oracle),
+    against the records the timed GPU run wrote for the same tracks.
+    Reports the fraction of tracks with the same status and surface sequence
+    and the per-quantity errors (_errors_vs_oracle)."""
+    from oracle import ref_oracle
+    from detray_b200.units import T
+    k = min(k, host_trk.shape[1])
+    ref = ref_oracle.propagate(ref_oracle.build_toy(),
+                               {"kind": "const", "b": (0.0, 0.0, 2.0 * T)},
+                               cfg, np.ascontiguousarray(host_trk[:, :k]),
+                               n_threads=host_threads())
+    t = res.tensors
+    got = {"status": t["status"][:k].cpu().numpy(),
+           "n_records": t["n_records"][:k].cpu().numpy(),
+           "rec_barcode": t["rec_barcode"][:, :k].cpu().numpy().view(np.uint64),
+           "rec_flags": t["rec_flags"][:, :k].cpu().numpy(),
+           "rec_bound": t["rec_bound"][:, :, :k].cpu().numpy(),
+           "rec_cov": t["rec_cov"][:, :, :k].cpu().numpy()}
+    out = _errors_vs_oracle(ref, got)
+    out["same_status"] = float((ref["status"] == got["status"]).mean())
+    out["oracle"] = "reference CPU propagator, fp64 build"
+    return out
+
+
+def config3_row(args, dev, stream, world):
+    """Benchmark configuration 3 on every rank: the toy detector in the
+    solenoid field map, 4 M muons with pT log-uniform in 0.1-100 GeV, fp32
+    with covariance transport and material: the plain one-track-per-thread
+    kernel (sorted, 32 registers), the persistent round-based method with
+    its defaults, and the autotuner's pick, each under a CUDA graph; times
+    are the max over ranks."""
+    import torch
+
+    from detray_b200 import abi, fields, geometry, propagator, tracks
+    n3 = 4_000_000
+    fmap = fields.solenoid_map()
+    det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"),
+                              dev.index)
+    field = propagator.Field.grid(fmap, dev.index)
+    cfg = workload_config()
+    trk = tracks.toy_tracks(n3, seed=args.seed + 3, pt_range=(0.1, 100.0))
+    dt = torch.tensor(trk, dtype=torch.float32, device=dev)
+    res = propagator.alloc_device_results(n3, cfg.max_records, dev)
+    forms = {"plain": propagator.make_launch(method=abi.METHOD_PLAIN,
+                                             sort_tracks=1, ctas_per_sm=16,
+                                             use_graph=1),
+             "persistent": propagator.make_launch(
+                 method=abi.METHOD_PERSISTENT, sort_tracks=1, use_graph=1)}
+    lc, tune = propagator.autotune(cfg, det, field, dt, use_graph=1,
+                                   stream=stream)
+    forms["autotuned"] = lc
+    ms = {}
+    for name, f in forms.items():
+        ms[name] = max_over_ranks(_time_device(
+            lambda f=f: propagator.propagate(cfg, det, field, dt, results=res,
+                                             launch=f, stream=stream),
+            dev, 5, 2), world)
+    status = np.bincount(res.tensors["status"].cpu().numpy(), minlength=7)
+    del res, dt
+    torch.cuda.empty_cache()
+    return {"workload": "toy_4brl_7edc_solenoid_map_4M_muons_pt0.1-100_eta4",
+            "tracks_per_gpu": n3, "ms": {k: round(v, 3) for k, v in ms.items()},
+            "tracks_per_s": {k: n3 * world / (v / 1e3) for k, v in ms.items()},
+            "autotuned": {"method": int(lc.method),
+                          "ctas_per_sm": int(lc.ctas_per_sm),
+                          "sort_tracks": int(lc.sort_tracks),
+                          "steps_per_round": int(lc.steps_per_round),
+                          "yield_lanes": int(lc.yield_lanes),
+                          "rounds": int(lc.rounds)},
+            "autotune_ms": [round(t, 3) for t in tune],
+            "track_status": status.tolist(),
+            "persistent_vs_plain": round(ms["plain"] / ms["persistent"], 4)}
+
+
 def run_ours(args):
     import torch
 
     from detray_b200 import abi, flops, geometry, propagator
     from detray_b200.units import T
 
+    from detray_b200 import sharding
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    n = args.tracks
     cfg = workload_config()
     det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"), local)
     field = propagator.Field.constant((0.0, 0.0, 2.0 * T), local)
-    host_trk = make_tracks(n, args.seed + rank)
+    # weak scaling: a global batch of args.tracks per GPU, split into
+    # contiguous work-balanced shards (no collective in the forward pass)
+    if world > 1:
+        host_trk, shard_range = sharding.shard(
+            make_tracks(args.tracks * world, args.seed), rank, world)
+        host_trk = np.ascontiguousarray(host_trk)
+    else:
+        host_trk, shard_range = make_tracks(args.tracks, args.seed), None
+    n = host_trk.shape[1]
     trk = torch.tensor(host_trk, dtype=torch.float32, device=dev)
     res = propagator.alloc_device_results(n, cfg.max_records, dev)
     stream = torch.cuda.current_stream(dev)
@@ -458,9 +582,10 @@ def run_ours(args):
     else:
         method = {"plain": abi.METHOD_PLAIN,
                   "persistent": abi.METHOD_PERSISTENT}[args.method]
+        ctas = args.ctas if method == abi.METHOD_PLAIN else 0
         lc = propagator.make_launch(method=method,
                                     sort_tracks=int(not args.no_sort),
-                                    ctas_per_sm=args.ctas, use_graph=1)
+                                    ctas_per_sm=ctas, use_graph=1)
     method = lc.method
 
     def step():
@@ -488,7 +613,7 @@ def run_ours(args):
     clk = clocks.stop()
     ms_local = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(ms_local, world)
-    total_tracks = n * world
+    total_tracks = int(sum_over_ranks(float(n), world))
     value = total_tracks / (ms / 1e3)
 
     # algorithmic work of one launch from the device event counters
@@ -508,20 +633,39 @@ def run_ours(args):
     except (OSError, ValueError):
         pass
     peak = flops.nominal_fp32_tflops(sm_count, peak_mhz)
-    traffic = None
+    method_name = {abi.METHOD_PLAIN: "plain",
+                   abi.METHOD_PERSISTENT: "persistent"}[method]
+    # DRAM bytes per track of one propagation with this method, from an ncu
+    # capture of every kernel of a smaller batch (scaled by tracks)
+    traffic, traffic_src = None, None
     prof = REPO / "profiles" / "propagate_toy_traffic.json"
     if prof.exists():
         try:
-            per_track = json.loads(prof.read_text())["dram_bytes_per_track"]
-            traffic = per_track * n
+            entry = json.loads(prof.read_text())[method_name]
+            traffic = entry["dram_bytes_per_track"] * n
+            traffic_src = entry["source"]
         except (OSError, ValueError, KeyError):
             traffic = None
+    rounds = int(lc.rounds) or 64
+    # our kernels per propagation (the radix sort itself is CUB's)
+    if method == abi.METHOD_PERSISTENT:
+        per_step = (int(lc.sort_tracks) + 1 + 2 * (rounds + 1) + 2 * rounds
+                    + 1)
+        kernels = ("direction key, init, per round the queue builder (2), "
+                   "step phase and navigation phase, then the queue builder "
+                   "and the tail")
+    else:
+        per_step = 1 + int(lc.sort_tracks)
+        kernels = "direction key, propagate_plain_kernel"
     roofline = {"bound": "fp32", "achieved": round(achieved, 4),
                 "peak": round(peak, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 5), "traffic": traffic,
+                "traffic_source": traffic_src,
                 "peak_source": f"nominal FP32 ({sm_count} SMs x 128 lanes x "
                                f"2 x {peak_mhz:.0f} MHz; no measured FP32 "
                                "peak on this pool)",
+                "scope": "the whole propagation call (all its kernels), "
+                         "CUDA events on its stream",
                 "flops_per_launch": fl, "kernel_ms": round(ms_local, 4)}
 
     # ---- end to end through the host-buffer API
@@ -569,11 +713,16 @@ def run_ours(args):
     if not args.no_extras:
         extras = extra_rows(cfg, det, field, trk, res, stream, dev)
 
-    cpu = None
+    cfg3 = None
+    if not args.no_config3:
+        cfg3 = config3_row(args, dev, stream, world)
+
+    cpu, errors = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_reference_rate(15.0, cfg, args.seed, 2_000_000,
                                      host_threads())
+            errors = parity_sample(cfg, host_trk, res, 4000)
         except (FileNotFoundError, OSError) as exc:
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
@@ -591,18 +740,24 @@ def run_ours(args):
                                   abi.METHOD_PERSISTENT: "persistent"}[method],
                        "sort_tracks": int(lc.sort_tracks),
                        "ctas_per_sm": int(lc.ctas_per_sm),
+                       "steps_per_round": int(lc.steps_per_round),
+                       "yield_lanes": int(lc.yield_lanes),
+                       "rounds": int(lc.rounds),
                        "cuda_graph": int(lc.use_graph),
+                       "shard": list(shard_range) if shard_range else None,
                        "autotune_ms": ([round(t, 3) for t in tune_ms]
                                        if tune_ms else None),
                        "parallelism": f"tracks sharded over {world} GPU(s)",
                        "l2": "per step ~1.5 GB of records written (> 126 MB "
                              "L2): inputs are re-read from HBM"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "errors_vs_fp64_oracle": errors,
+            "config3": cfg3,
             "adjoint": adj,
             "other_entry_points": extras,
-            # our kernels per step: the propagation kernel, plus the direction
-            # key kernel when sorting (the radix sort itself is CUB's)
-            "gpu_launches": args.steps * (1 + int(lc.sort_tracks)),
+            "gpu_launches": args.steps * per_step,
+            "gpu_launches_per_step": per_step,
+            "gpu_kernels": kernels,
             "clocks": clk,
             "track_status": status.tolist(),
             "mean_steps_per_track": round(mean_steps, 2),
@@ -648,6 +803,7 @@ def run_reference(args):
     dt = (time.perf_counter() - t0) / args.steps
     value = n / dt
     gpu = reference_gpu_row(args, cfg)
+    gpu3 = reference_gpu_config3(args, cfg) if not args.no_config3 else None
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -662,6 +818,7 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "reference_gpu": gpu,
+        "reference_gpu_config3": gpu3,
     }
     print(json.dumps(line), flush=True)
 
@@ -693,6 +850,37 @@ def reference_gpu_row(args, cfg):
                       "actor chain: parameter_updater with material "
                       "interactor), 256 threads, sm_100a, tracks ordered by "
                       "|pi/2 - theta| as in the reference benchmark, no "
+                      "records written"}
+
+
+def reference_gpu_config3(args, cfg):
+    """The reference's device propagation in benchmark configuration 3: its
+    tutorial kernel's actor chain (path-limit aborter, parameter updater
+    with the material interactor, tutorials/src/device/cuda/
+    propagation_kernel.cu), one thread per track, in the solenoid field map,
+    on the same 4 M tracks as our config3 object (ordered by |pi/2 - theta|
+    as the reference benchmark orders its input)."""
+    from oracle import ref_oracle
+    try:
+        import torch
+        if not (ref_oracle.gpu_available() and torch.cuda.is_available()):
+            return None
+        from detray_b200 import fields, tracks
+        n3 = 4_000_000
+        trk = tracks.toy_tracks(n3, seed=args.seed + 3, pt_range=(0.1, 100.0))
+        theta = np.arccos(np.clip(trk[6], -1.0, 1.0))
+        trk = trk[:, np.argsort(np.abs(0.5 * np.pi - theta), kind="stable")]
+        r = ref_oracle.gpu_toy_map_bench(cfg, fields.solenoid_map(), trk,
+                                         warmup=1, steps=3)
+    except (RuntimeError, OSError) as exc:
+        return {"unavailable": str(exc)}
+    return {"value": n3 / (r["ms_per_step"] / 1e3), "unit": UNIT,
+            "ms_per_step": round(r["ms_per_step"], 3), "tracks": n3,
+            "n_exited": r["n_exited"],
+            "workload": "toy_4brl_7edc_solenoid_map_4M_muons_pt0.1-100_eta4",
+            "kernel": "reference tutorial propagation kernel (path-limit "
+                      "aborter, parameter updater with material "
+                      "interactor), 64 threads per block, sm_100a, no "
                       "records written"}
 
 
@@ -903,8 +1091,34 @@ def run_sweep(args):
     print(json.dumps({"sweep": rows, "clocks": clk}), flush=True)
 
 
+def run_dry(args):
+    """The multi-GPU launcher without GPU work: every rank takes its
+    work-balanced shard of the global batch; rank 0 prints the line."""
+    from detray_b200 import sharding
+    world, rank, _ = dist_setup(args)
+    host_all = make_tracks(args.tracks * world, args.seed)
+    mine, (lo, hi) = sharding.shard(host_all, rank, world)
+    total = sum_over_ranks(float(mine.shape[1]), world)
+    biggest = max_over_ranks(float(mine.shape[1]), world)
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "metric": METRIC,
+                          "value": None, "unit": UNIT,
+                          "global_batch": int(total),
+                          "largest_shard": int(biggest),
+                          "rank0_range": [lo, hi]}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
+    rc = spawn_ranks(args)
+    if rc is not None:
+        sys.exit(rc)
+    if args.dry_run:
+        run_dry(args)
+        return
     if args.sweep:
         run_sweep(args)
         return

@@ -718,6 +718,10 @@ dprop_status propagate_host_jagged(const dprop_config& c,
     need += al256(chunk) + 7 * al256(chunk * 4) + 8 * al256(chunk * 4);  // per-track
     need += 2 * (al256(rec_slot * 8) + 28 * al256(rec_slot * 4) + al256(rec_slot));
     need += 6 * al256((chunk + 1) * 4) + al256(sort_temp) + al256(scan_temp);
+    const bool rounds = lc && lc->method == DPROP_METHOD_PERSISTENT;
+    const size_t rounds_bytes =
+        rounds ? al256(dprop::api::rounds_scratch_bytes(chunk, det->wires)) : 0;
+    need += rounds_bytes;
     for (int k = 0; k < n_slots; ++k) {
         const dprop_status s = ensure_pipe(g_pipe[k], k, need, chunk);
         if (s != DPROP_OK) {
@@ -727,6 +731,10 @@ dprop_status propagate_host_jagged(const dprop_config& c,
     auto carve = [&](int sl) {
         return carve_slot(g_pipe[sl].dev, chunk, rec_slot, with_cov, sort_temp,
                           scan_temp);
+    };
+    // the persistent method's slot arrays and queues: the tail of the block
+    auto rounds_scratch = [&](int sl) {
+        return static_cast<char*>(g_pipe[sl].dev) + (need - rounds_bytes);
     };
     cudaEvent_t inputs_ready = nullptr;
     DPROP_CUDA(cudaEventCreateWithFlags(&inputs_ready, cudaEventDisableTiming));
@@ -811,11 +819,26 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         dt.time = b.trk[3];
         dt.qop = b.trk[7];
         const io_ptrs<double> io = make_io<double>(dt, b.dr);
-        const unsigned int grid =
-            static_cast<unsigned int>((m + k_plain_block - 1) / k_plain_block);
-        launch_plain_mb<double, DPROP_MIN_BLOCKS>(grid, st, det, field->view,
-                                                  pcfg, io, m,
-                                                  sort ? b.idx_out : nullptr);
+        if (rounds) {
+            const dprop_status s = dprop::api::enqueue_rounds<double>(
+                lc, det, field, pcfg, io, m, sort ? b.idx_out : nullptr,
+                rounds_scratch(sl), rounds_bytes, st);
+            if (s != DPROP_OK) return s;
+        } else {
+            const unsigned int grid = static_cast<unsigned int>(
+                (m + k_plain_block - 1) / k_plain_block);
+            const int mb = occupancy_of(lc);
+            if (mb == 8) {
+                launch_plain_mb<double, 8>(grid, st, det, field->view, pcfg,
+                                           io, m, sort ? b.idx_out : nullptr);
+            } else if (mb == 16) {
+                launch_plain_mb<double, 16>(grid, st, det, field->view, pcfg,
+                                            io, m, sort ? b.idx_out : nullptr);
+            } else {
+                launch_plain_mb<double, 12>(grid, st, det, field->view, pcfg,
+                                            io, m, sort ? b.idx_out : nullptr);
+            }
+        }
         DPROP_CUDA(cudaGetLastError());
         // pack the records
         const unsigned int cg = static_cast<unsigned int>((m + 1 + 255) / 256);

@@ -387,7 +387,10 @@ dprop_status dprop_propagate(const dprop_config* cfg,
 /* Same, with host inputs (double precision, as dprop_tracks) and host
  * outputs (the result pointers then point to host memory, with the same
  * element types as on the device).  Copies in, propagates, copies out and
- * synchronises.  Uses library-owned device scratch, grown on demand. */
+ * synchronises.  Uses library-owned device scratch, grown on demand.  With
+ * jagged records (rec_offsets) the batch runs in chunks of up to 256 Ki
+ * tracks on four streams, each chunk with the launch's method, sort and
+ * register budget (use_graph is ignored there). */
 dprop_status dprop_propagate_host(const dprop_config* cfg,
                                   const dprop_launch* launch,
                                   const dprop_detector* det,

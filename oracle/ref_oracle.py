@@ -469,6 +469,37 @@ def gpu_toy_bench(cfg: abi.Config, bz: float, tracks: np.ndarray,
     return {"ms_per_step": ms.value, "n_exited": int(ok.value)}
 
 
+def gpu_toy_map_bench(cfg: abi.Config, fmap: dict, tracks: np.ndarray,
+                      warmup: int = 2, steps: int = 5) -> dict:
+    """Time the reference tutorial's CUDA propagation kernel (path-limit
+    aborter and parameter updater with the material interactor, built per
+    thread as in tutorials/src/device/cuda/propagation_kernel.cu; oracle/ref/
+    ref_gpu*.{cu,cpp}) on ``tracks`` through the toy detector in the field
+    map ``fmap`` (detray_b200.fields format).  Returns ms per launch and the
+    number of tracks whose propagate() returned true."""
+    lib = C.CDLL(str(REF_DIR / "libdetray_ref_gpu.so"))
+    lib.refgpu_last_error.restype = C.c_char_p
+    lib.refgpu_toy_map_bench.argtypes = [
+        C.POINTER(abi.Config), C.POINTER(C.c_double), C.POINTER(C.c_double),
+        C.POINTER(C.c_uint32), C.c_void_p, C.POINTER(C.c_void_p), C.c_uint64,
+        C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+    trk = np.ascontiguousarray(tracks, dtype=np.float64)
+    ptrs = (C.c_void_p * 8)(*[trk[i].ctypes.data for i in range(8)])
+    lo = (C.c_double * 3)(*fmap["lo"])
+    hi = (C.c_double * 3)(*fmap["hi"])
+    nn = (C.c_uint32 * 3)(*fmap["n"])
+    vals = np.ascontiguousarray(fmap["values"], dtype=np.float32)
+    ms = C.c_double()
+    ok = C.c_uint64()
+    rc = lib.refgpu_toy_map_bench(C.byref(cfg), lo, hi, nn,
+                                  vals.ctypes.data_as(C.c_void_p), ptrs,
+                                  trk.shape[1], warmup, steps, C.byref(ms),
+                                  C.byref(ok))
+    if rc != 0:
+        raise RuntimeError(lib.refgpu_last_error().decode())
+    return {"ms_per_step": ms.value, "n_exited": int(ok.value)}
+
+
 def json_available() -> bool:
     """The reference's JSON detector writer and reader (oracle/ref/
     ref_json.cpp, built when nlohmann/json is found)."""
