@@ -11,10 +11,12 @@
 //   meta   navigation state without the candidates: cache indices, status,
 //          trust, volume, external mask tolerance, direction, abort reason,
 //          intersection counter
-//   cand   the candidate cache, by cache index: a phase loads only the
-//          entries it reads (the step phase the target and the one after
-//          it, the surface actors the current surface and the target, the
-//          navigation phase all of them)
+//   cand   the candidate cache, the k_cache + 1 entries of a slot stored
+//          together (one 16-byte record each), so that the few entries a
+//          lane reads at its own run-time cache index share a cache line: a
+//          phase loads only the entries it reads (the step phase the current
+//          surface, the target and the one after it, the navigation phase
+//          all of them)
 //   bound  bound parameters, covariance and surface of the transporter
 //   loop   loop variables (iteration, stall counter, path before the step,
 //          flags, charge)
@@ -23,6 +25,8 @@
 //   pc     the next segment of each slot, one byte per slot in its own dense
 //          array (the queue builder reads only this)
 #pragma once
+
+#include <cstring>
 
 #include "machine.cuh"
 
@@ -73,10 +77,10 @@ struct slot_soa {
     S* direction;
     uint32_t* nav_misc;   // abort reason
     uint32_t* n_isect;
-    // cand: [k * n + slot]
-    S* cand_path;
-    uint32_t* cand_sf;
-    uint32_t* cand_info;  // volume_link | status << 16 | flags << 24
+    // cand: record k of slot s at [s * (k_cache + 1) + k]; float: path bits,
+    // surface, info, 0; double: path bits (low, high), surface, info; info
+    // = volume_link | status << 16 | flags << 24
+    uint4* cand;
     // bound
     S* bv[6];
     S* bcov[21];
@@ -137,9 +141,8 @@ size_t carve_slots(void* base, uint64_t n, bool with_cyc, slot_soa<S>* out) {
     s.direction = fs();
     s.nav_misc = f4();
     s.n_isect = f4();
-    s.cand_path = reinterpret_cast<S*>(take(9u * n * sizeof(S)));
-    s.cand_sf = reinterpret_cast<uint32_t*>(take(9u * n * 4u));
-    s.cand_info = reinterpret_cast<uint32_t*>(take(9u * n * 4u));
+    s.cand = reinterpret_cast<uint4*>(
+        take(static_cast<size_t>(k_cache + 1) * n * sizeof(uint4)));
     for (int i = 0; i < 6; ++i) s.bv[i] = fs();
     for (int i = 0; i < 21; ++i) s.bcov[i] = fs();
     s.bsf = f4();
@@ -165,27 +168,57 @@ size_t carve_slots(void* base, uint64_t n, bool with_cyc, slot_soa<S>* out) {
 }
 
 // ----------------------------------------------------------- candidates
+DPROP_HD uint32_t f32_bits(float v) {
+    uint32_t u;
+    memcpy(&u, &v, sizeof(u));
+    return u;
+}
+DPROP_HD float bits_f32(uint32_t u) {
+    float v;
+    memcpy(&v, &u, sizeof(v));
+    return v;
+}
+
+DPROP_HD void pack_path(float p, uint4& r) {
+    r.x = f32_bits(p);
+    r.w = 0u;
+}
+DPROP_HD void pack_path(double p, uint4& r) {
+    uint64_t u;
+    memcpy(&u, &p, sizeof(u));
+    r.x = static_cast<uint32_t>(u);
+    r.w = static_cast<uint32_t>(u >> 32);
+}
+DPROP_HD void unpack_path(const uint4& r, float& p) { p = bits_f32(r.x); }
+DPROP_HD void unpack_path(const uint4& r, double& p) {
+    const uint64_t u = static_cast<uint64_t>(r.x) |
+                       (static_cast<uint64_t>(r.w) << 32);
+    memcpy(&p, &u, sizeof(p));
+}
+
 template <typename S>
 DPROP_HD void load_cand(const slot_soa<S>& s, uint64_t slot, int k,
                         candidate<S>& c) {
-    const uint64_t o = static_cast<uint64_t>(k) * s.n + slot;
-    c.path = s.cand_path[o];
-    c.sf = s.cand_sf[o];
-    const uint32_t info = s.cand_info[o];
-    c.volume_link = static_cast<uint16_t>(info & 0xffffu);
-    c.status = static_cast<uint8_t>((info >> 16) & 0xffu);
-    c.flags = static_cast<uint8_t>(info >> 24);
+    const uint4 r = s.cand[slot * static_cast<uint64_t>(k_cache + 1) +
+                           static_cast<uint64_t>(k)];
+    unpack_path(r, c.path);
+    c.sf = r.y;
+    c.volume_link = static_cast<uint16_t>(r.z & 0xffffu);
+    c.status = static_cast<uint8_t>((r.z >> 16) & 0xffu);
+    c.flags = static_cast<uint8_t>(r.z >> 24);
 }
 
 template <typename S>
 DPROP_HD void store_cand(const slot_soa<S>& s, uint64_t slot, int k,
                          const candidate<S>& c) {
-    const uint64_t o = static_cast<uint64_t>(k) * s.n + slot;
-    s.cand_path[o] = c.path;
-    s.cand_sf[o] = c.sf;
-    s.cand_info[o] = static_cast<uint32_t>(c.volume_link) |
-                     (static_cast<uint32_t>(c.status) << 16) |
-                     (static_cast<uint32_t>(c.flags) << 24);
+    uint4 r;
+    pack_path(c.path, r);
+    r.y = c.sf;
+    r.z = static_cast<uint32_t>(c.volume_link) |
+          (static_cast<uint32_t>(c.status) << 16) |
+          (static_cast<uint32_t>(c.flags) << 24);
+    s.cand[slot * static_cast<uint64_t>(k_cache + 1) +
+           static_cast<uint64_t>(k)] = r;
 }
 
 // Candidate indices [lo, hi] clamped to the cache (including its sentinel).

@@ -1063,7 +1063,9 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
         return DPROP_OK;
     }
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    const uint64_t m = n < 262144u ? n : 262144u;
+    // at most 2^20 tracks: the persistent method's per-round costs are
+    // amortised over the batch, so a small sample would misjudge it
+    const uint64_t m = n < 1048576u ? n : 1048576u;
     const uint64_t cap = cfg->max_records;
     // temporary results for the trial runs
     const size_t per_track = 1 + 6 * 4 + 8 * 4 + 16;
@@ -1113,6 +1115,7 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
     int best_i = 1;
     for (int i = 0; i < DPROP_AUTOTUNE_CANDIDATES && s == DPROP_OK; ++i) {
         dprop_launch lc{};
+        lc.use_graph = launch_out->use_graph;
         lc.method = cands[i].method;
         lc.ctas_per_sm = cands[i].ctas;
         lc.sort_tracks = cands[i].sort;

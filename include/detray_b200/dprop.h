@@ -549,8 +549,9 @@ dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
  * without it; the persistent method with and without the sort over its
  * step-phase register budget (ctas_per_sm 3, 4, 5), steps per round, tracks
  * per warp (yield_lanes 8, 12, 16) and the number of rounds before the tail
- * kernel - on the first min(n_tracks, 262144) of the given
- * device tracks, and writes the fastest into *launch (method, ctas_per_sm,
+ * kernel - on the first min(n_tracks, 1048576) of the given
+ * device tracks (under a CUDA graph if launch->use_graph is set), and writes
+ * the fastest into *launch (method, ctas_per_sm,
  * sort_tracks, steps_per_round, yield_lanes, rounds; use_graph is left as
  * given).  If timings_ms is not NULL it receives one time per candidate
  * (DPROP_AUTOTUNE_CANDIDATES entries).  Allocates temporary device result

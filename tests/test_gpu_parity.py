@@ -279,16 +279,17 @@ def test_host_api_jagged_equals_device_api(torch_cuda):
 
 def test_graph_replay_and_autotune(torch_cuda):
     """A propagate call captured into a CUDA graph and replayed gives the
-    same results as the direct launch, plain and persistent (whose work
-    queue counter the graph keeps after the sort's scratch); the autotuner
-    returns one of its candidates and times all of them."""
+    same results as the direct launch, plain and persistent (whose slot
+    arrays and work queues the graph keeps after the sort's scratch); the
+    autotuner returns one of its candidates and times all of them."""
     from detray_b200 import abi, propagator
     det, field, cfg, trk = _setup("toy")
     a = _run_device(torch_cuda, det, field, cfg, trk, method=0)
     dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
     res = propagator.alloc_device_results(dev.shape[1], cfg.max_records, "cuda")
     for method, occ in ((abi.METHOD_PLAIN, 8), (abi.METHOD_PLAIN, 16),
-                        (abi.METHOD_PERSISTENT, 16)):
+                        (abi.METHOD_PERSISTENT, 3),
+                        (abi.METHOD_PERSISTENT, 4)):
         lc = propagator.make_launch(method=method, sort_tracks=1, use_graph=1,
                                     ctas_per_sm=occ)
         for _ in range(3):  # capture, then replays
