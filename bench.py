@@ -56,9 +56,12 @@ def parse_args():
                    default="auto")
     p.add_argument("--no-sort", action="store_true",
                    help="propagate in input order instead of direction order")
-    p.add_argument("--ctas", type=int, default=12, choices=(8, 12, 16),
-                   help="register budget (resident CTAs per SM) of the "
-                        "plain method when --method is plain")
+    p.add_argument("--ctas", type=int, default=0,
+                   choices=(0, 3, 4, 5, 8, 12, 16),
+                   help="register budget (resident CTAs per SM) when "
+                        "--method is not auto: 8, 12 or 16 for the plain "
+                        "method, 3, 4 or 5 for the persistent method's step "
+                        "phase; 0 = the method's default")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true",
@@ -582,7 +585,10 @@ def run_ours(args):
     else:
         method = {"plain": abi.METHOD_PLAIN,
                   "persistent": abi.METHOD_PERSISTENT}[args.method]
-        ctas = args.ctas if method == abi.METHOD_PLAIN else 0
+        ctas = args.ctas
+        if (method == abi.METHOD_PLAIN) != (ctas in (0, 8, 12, 16)):
+            raise SystemExit(f"bench.py: --ctas {ctas} does not apply to "
+                             f"--method {args.method}")
         lc = propagator.make_launch(method=method,
                                     sort_tracks=int(not args.no_sort),
                                     ctas_per_sm=ctas, use_graph=1)
