@@ -28,7 +28,7 @@ namespace {
 
 constexpr int k_adj_block = 128;
 
-template <int MinBlocks, bool W>
+template <int MinBlocks, bool W, bool Grad>
 __global__ void __launch_bounds__(k_adj_block, MinBlocks)
     propagate_adjoint_kernel(const __grid_constant__ detector_view<float, W> det,
                              const __grid_constant__ field_view<float> field,
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(k_adj_block, MinBlocks)
         return;
     }
     const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
-    api::run_one<float, true>(t, n, det, field, cfg, io, tv);
+    api::run_one<float, true, float, W, Grad>(t, n, det, field, cfg, io, tv);
 }
 
 struct backward_io {
@@ -103,11 +103,24 @@ void launch_adjoint_mb(unsigned int grid, cudaStream_t st,
                        const api::io_ptrs<float>& io,
                        const tape_view<float>& tv, uint64_t n,
                        const uint32_t* order) {
+    // with the field gradient: one register budget (8 CTAs per SM)
+    if (cfg.step.field_gradient) {
+        if (det->wires) {
+            propagate_adjoint_kernel<8, true, true>
+                <<<grid, k_adj_block, 0, st>>>(det->view_as<true>(), field,
+                                               cfg, io, tv, n, order);
+        } else {
+            propagate_adjoint_kernel<8, false, true>
+                <<<grid, k_adj_block, 0, st>>>(det->view_as<false>(), field,
+                                               cfg, io, tv, n, order);
+        }
+        return;
+    }
     if (det->wires) {
-        propagate_adjoint_kernel<MB, true><<<grid, k_adj_block, 0, st>>>(
+        propagate_adjoint_kernel<MB, true, false><<<grid, k_adj_block, 0, st>>>(
             det->view_as<true>(), field, cfg, io, tv, n, order);
     } else {
-        propagate_adjoint_kernel<MB, false><<<grid, k_adj_block, 0, st>>>(
+        propagate_adjoint_kernel<MB, false, false><<<grid, k_adj_block, 0, st>>>(
             det->view_as<false>(), field, cfg, io, tv, n, order);
     }
 }
@@ -127,10 +140,10 @@ dprop_status dprop_propagate_adjoint(const dprop_config* cfg,
     if (!cfg || !det || !field || !tracks || !results || !tape) {
         return fail(DPROP_E_INVALID, "propagate_adjoint: NULL argument");
     }
-    if (cfg->use_field_gradient || cfg->use_eloss_gradient) {
+    if (cfg->use_eloss_gradient) {
         return fail(DPROP_E_UNSUPPORTED,
-                    "propagate_adjoint: field/eloss gradients are not "
-                    "supported on the device path");
+                    "propagate_adjoint: use_eloss_gradient needs volume "
+                    "material, which the device path does not support");
     }
     if (cfg->max_iterations == 0u || cfg->max_records == 0u) {
         return fail(DPROP_E_INVALID,

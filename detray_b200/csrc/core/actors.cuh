@@ -117,9 +117,9 @@ DPROP_HD vec3<S> bound_to_free_pos(const detector_view<S, W>& det,
 }
 
 // free -> bound vector on a surface (free_to_bound_vector)
-template <typename S, bool W>
+template <typename S, bool W, bool Grad>
 DPROP_HD void free_to_bound(const detector_view<S, W>& det, const dev_surface& sf,
-                            const step_state<S>& st, S out[6]) {
+                            const step_state<S, Grad>& st, S out[6]) {
     const dev_transform<S>& trf = det.transforms[sf.transform];
     if (W && sf.shape == e_line) {
         const local2<S> l = line_bound_local(trf, st.pos, st.dir);
@@ -285,10 +285,10 @@ DPROP_HD_LINE axes2<S> line_dpos_dangle(const dev_transform<S>& trf,
 // the current (destination) free state.  Only rows 0..3 x cols 0..4 are
 // non-trivial (the q/p row and the time column are identity, as the
 // covariance-transport generator assumes); they are returned in G[4][5].
-template <typename S, bool W>
+template <typename S, bool W, bool Grad>
 DPROP_HD void full_jacobian(const detector_view<S, W>& det,
                             const bound_state<S>& dep, const dev_surface& dep_sf,
-                            const dev_surface& dst_sf, const step_state<S>& st,
+                            const dev_surface& dst_sf, const step_state<S, Grad>& st,
                             vec3<S> dtds, S G[4][5]) {
     // bound -> free at the departure surface
     const S ph = dep.v[2];
@@ -307,7 +307,7 @@ DPROP_HD void full_jacobian(const detector_view<S, W>& det,
     // pos rows: [p0 | p1 | A dd_phi | A dd_th | c | 0]
     // dir rows: [0 | 0 | B dd_phi | B dd_th | d | 0]
     // qop row:  [0 0 0 0 e 0]; time row: e5
-    const transport_jac<S>& J = st.jac;
+    const transport_jac<S, Grad>& J = st.jac;
     S m1p[3][5], m1d[3][5];
     const S p0a[3] = {p0.x, p0.y, p0.z};
     const S p1a[3] = {p1.x, p1.y, p1.z};
@@ -334,6 +334,12 @@ DPROP_HD void full_jacobian(const detector_view<S, W>& det,
         m1d[r][3] = b3;
         m1d[r][4] = da[r];
     }
+    // d(pos)/d(loc0, loc1, phi, theta) at the departure (the angle columns
+    // only for the line frame), which the gradient form carries through
+    // d(pos)/d(pos0) and d(dir)/d(pos0)
+    S bp[3][4] = {{p0a[0], p1a[0], S(0), S(0)},
+                  {p0a[1], p1a[1], S(0), S(0)},
+                  {p0a[2], p1a[2], S(0), S(0)}};
     if (W && dep_sf.shape == e_line) {
         // the line frame's position also moves with the angles
         const axes2<S> cd = line_dpos_dangle(det.transforms[dep_sf.transform],
@@ -344,6 +350,22 @@ DPROP_HD void full_jacobian(const detector_view<S, W>& det,
         for (int r = 0; r < 3; ++r) {
             m1p[r][2] += cpa[r];
             m1p[r][3] += cta[r];
+            bp[r][2] = cpa[r];
+            bp[r][3] = cta[r];
+        }
+    }
+    if constexpr (Grad) {
+        // m1p += (P - I) bp, m1d += Q bp
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 4; ++c) {
+                S a = S(0), b = S(0);
+                for (int k = 0; k < 3; ++k) {
+                    a += (J.P(r, k) - (r == k ? S(1) : S(0))) * bp[k][c];
+                    b += J.Q(r, k) * bp[k][c];
+                }
+                m1p[r][c] += a;
+                m1d[r][c] += b;
+            }
         }
     }
 
@@ -607,9 +629,9 @@ DPROP_HD bool interact(const detector_view<S, W>& det, const dev_surface& sf,
 }
 
 // estimate_external_mask_tolerance (noise_estimation.hpp:22-107)
-template <typename S>
+template <typename S, bool Grad>
 DPROP_HD void estimate_external_tol(nav_state<S>& nav, const bound_state<S>& b,
-                                    const step_state<S>& st,
+                                    const step_state<S, Grad>& st,
                                     const actor_cfg<S>& cfg, S q) {
     const S n = cfg.n_stddev;
     const S var0 = b.cov[tri6(0, 0)];

@@ -126,18 +126,24 @@ struct no_tape {
 // with respect to the initial free parameters (x, y, z, tx, ty, tz, q/p),
 // from the transport Jacobian accumulated since the start.  Same product as
 // full_jacobian, with B2F replaced by the identity on the free parameters.
-template <typename S, bool W>
+template <typename S, bool W, bool Grad>
 DPROP_HD void initial_jacobian(const detector_view<S, W>& det,
                                const dev_surface& dst_sf,
-                               const step_state<S>& st, vec3<S> dtds,
+                               const step_state<S, Grad>& st, vec3<S> dtds,
                                S K[5][7]) {
-    const transport_jac<S>& J = st.jac;
-    // M1 = J_t restricted to the columns pos (identity), dir (A, B), q/p
+    const transport_jac<S, Grad>& J = st.jac;
+    // M1 = J_t restricted to the columns pos (identity, or P and Q with the
+    // field gradient), dir (A, B), q/p
     S mp[3][7], md[3][7];
     for (int r = 0; r < 3; ++r) {
         for (int c = 0; c < 3; ++c) {
-            mp[r][c] = (r == c) ? S(1) : S(0);
-            md[r][c] = S(0);
+            if constexpr (Grad) {
+                mp[r][c] = J.P(r, c);
+                md[r][c] = J.Q(r, c);
+            } else {
+                mp[r][c] = (r == c) ? S(1) : S(0);
+                md[r][c] = S(0);
+            }
             mp[r][3 + c] = J.A(r, c);
             md[r][3 + c] = J.B(r, c);
         }

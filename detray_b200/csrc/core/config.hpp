@@ -14,6 +14,7 @@ prop_cfg<S> make_prop_cfg(const dprop_config& c) {
     p.step.rk_error_tol = static_cast<S>(c.rk_error_tol);
     p.step.max_rk_updates = c.max_rk_updates;
     p.step.do_covariance_transport = c.do_covariance_transport != 0;
+    p.step.field_gradient = c.use_field_gradient != 0;
     p.nav.isect.min_mask_tol = static_cast<S>(c.min_mask_tolerance);
     p.nav.isect.max_mask_tol = static_cast<S>(c.max_mask_tolerance);
     p.nav.isect.mask_tol_scalor = static_cast<S>(c.mask_tolerance_scalor);

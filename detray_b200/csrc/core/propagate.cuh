@@ -68,10 +68,11 @@ struct record_sink {
     }
 };
 
-// All per-track state of one propagation flow
-template <typename S>
+// All per-track state of one propagation flow; Grad: the transport Jacobian
+// includes the field gradient (use_field_gradient)
+template <typename S, bool Grad = false>
 struct track_state {
-    step_state<S> step;
+    step_state<S, Grad> step;
     nav_state<S> nav;
     bound_state<S> bound;
     S q;        // particle charge (sign of q/p)
@@ -80,10 +81,10 @@ struct track_state {
     uint32_t n_material;
 };
 
-template <typename S>
-DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
+template <typename S, bool Grad>
+DPROP_HD void init_track_state(track_state<S, Grad>& ts, vec3<S> pos, S time,
                                vec3<S> dir, S qop, const prop_cfg<S>& cfg) {
-    step_state<S>& st = ts.step;
+    step_state<S, Grad>& st = ts.step;
     st.pos = pos;
     st.dir = dir;
     st.qop = qop;
@@ -118,13 +119,13 @@ DPROP_HD void init_track_state(track_state<S>& ts, vec3<S> pos, S time,
 // adjoint_tape (adjoint mode) the derivative data of each transported record
 // goes to the tape, and the transport Jacobian restarts at the first
 // transported surface as well.
-template <typename S, bool W, typename Tape>
-DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
+template <typename S, bool W, typename Tape, bool Grad>
+DPROP_HD_COLD void run_surface_actors(track_state<S, Grad>& ts,
                                       const detector_view<S, W>& det,
                                       const field_view<S>& field,
                                       const prop_cfg<S>& cfg,
                                       record_sink<S>& rec, const Tape& tape) {
-    step_state<S>& st = ts.step;
+    step_state<S, Grad>& st = ts.step;
     nav_state<S>& nav = ts.nav;
     const uint32_t cur_sf = nav.current().sf;
     const dev_surface dst = det.surfaces[cur_sf];
@@ -226,9 +227,9 @@ DPROP_HD_COLD void run_surface_actors(track_state<S>& ts,
 }
 
 // pathlimit_aborter (aborters.hpp:23-76): the first actor of the chain.
-template <typename S>
-DPROP_HD void path_limit_aborter(track_state<S>& ts, const prop_cfg<S>& cfg) {
-    step_state<S>& st = ts.step;
+template <typename S, bool Grad>
+DPROP_HD void path_limit_aborter(track_state<S, Grad>& ts, const prop_cfg<S>& cfg) {
+    step_state<S, Grad>& st = ts.step;
     nav_state<S>& nav = ts.nav;
     if (!nav.finished()) {
         const S step_limit =
@@ -242,8 +243,8 @@ DPROP_HD void path_limit_aborter(track_state<S>& ts, const prop_cfg<S>& cfg) {
 }
 
 // Run the actor chain once (propagator.hpp:308).
-template <typename S, bool W, typename Tape>
-DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
+template <typename S, bool W, typename Tape, bool Grad>
+DPROP_HD void run_actors(track_state<S, Grad>& ts, const detector_view<S, W>& det,
                          const field_view<S>& field, const prop_cfg<S>& cfg,
                          record_sink<S>& rec, const Tape& tape) {
     path_limit_aborter(ts, cfg);
@@ -254,8 +255,8 @@ DPROP_HD void run_actors(track_state<S>& ts, const detector_view<S, W>& det,
 }
 
 // stepper_rk_policy: downgrade the navigation trust after a step
-template <typename S>
-DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S>& st) {
+template <typename S, bool Grad>
+DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S, Grad>& st) {
     const S d = nav.dist();
     if (fabs(d) <= S(unit::um)) {
         nav.set_high_trust();
@@ -292,8 +293,8 @@ DPROP_HD uint32_t scalar_bits(double v) {
 #endif
     return static_cast<uint32_t>(u) ^ static_cast<uint32_t>(u >> 32);
 }
-template <typename S>
-DPROP_HD uint32_t state_key(const step_state<S>& st) {
+template <typename S, bool Grad>
+DPROP_HD uint32_t state_key(const step_state<S, Grad>& st) {
     uint32_t h = scalar_bits(st.pos.x);
     h = h * 0x9e3779b1u ^ scalar_bits(st.pos.y);
     h = h * 0x9e3779b1u ^ scalar_bits(st.pos.z);
@@ -330,7 +331,8 @@ struct cycle_search {
     double path0 = 0.;
     S time0 = S(0);
 
-    DPROP_HD void save(const step_state<S>& st) {
+    template <bool Grad>
+    DPROP_HD void save(const step_state<S, Grad>& st) {
         abs0 = st.abs_path_length;
         path0 = st.path_length;
         time0 = st.time;
@@ -341,8 +343,8 @@ struct cycle_search {
 // Called after every step.  Built with DPROP_NO_CYCLE_SKIP it does nothing
 // and every cycle is stepped out as the reference does (the test build that
 // checks the two agree).
-template <typename S>
-DPROP_HD void skip_cycles(cycle_search<S>& c, step_state<S>& st,
+template <typename S, bool Grad>
+DPROP_HD void skip_cycles(cycle_search<S>& c, step_state<S, Grad>& st,
                           S path_limit) {
 #if defined(DPROP_NO_CYCLE_SKIP)
     return;
@@ -401,8 +403,8 @@ struct caching_navigation {
 
 // dprop_track_status code of a track whose propagation loop has ended
 // (propagator.hpp:389-399 and the abort reasons).
-template <typename S>
-DPROP_HD uint8_t track_status(const track_state<S>& ts, bool out_of_budget) {
+template <typename S, bool Grad>
+DPROP_HD uint8_t track_status(const track_state<S, Grad>& ts, bool out_of_budget) {
     const nav_state<S>& nav = ts.nav;
     if (out_of_budget) {
         return 4u;  // DPROP_TRK_MAX_ITER
@@ -425,13 +427,13 @@ DPROP_HD uint8_t track_status(const track_state<S>& ts, bool out_of_budget) {
 
 // Propagate one track to the end with the navigation policy Nav (init and
 // update of the propagator's navigator); returns a dprop_track_status code.
-template <typename S, bool W, typename Tape, typename Nav>
-DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
+template <typename S, bool W, typename Tape, typename Nav, bool Grad>
+DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S, Grad>& ts,
                                       const detector_view<S, W>& det,
                                       const field_view<S>& field,
                                       const prop_cfg<S>& cfg,
                                       record_sink<S>& rec, const Tape& tape) {
-    step_state<S>& st = ts.step;
+    step_state<S, Grad>& st = ts.step;
     nav_state<S>& nav = ts.nav;
 
     navigator.init(nav, det, track_view<S>{st.pos, st.dir}, cfg.nav);
@@ -498,8 +500,8 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S>& ts,
 }
 
 // Propagate one track with the caching navigator.
-template <typename S, bool W, typename Tape = no_tape>
-DPROP_HD uint8_t propagate_track(track_state<S>& ts,
+template <typename S, bool W, typename Tape = no_tape, bool Grad>
+DPROP_HD uint8_t propagate_track(track_state<S, Grad>& ts,
                                  const detector_view<S, W>& det,
                                  const field_view<S>& field,
                                  const prop_cfg<S>& cfg, record_sink<S>& rec,

@@ -20,15 +20,20 @@ namespace dprop {
 // Non-trivial blocks of the 8x8 free transport Jacobian (25 values):
 //   A = d(pos)/d(dir0), B = d(dir)/d(dir0), c = d(pos)/d(qop0),
 //   d = d(dir)/d(qop0), e = d(qop)/d(qop0); everything else is identity.
+// With the field gradient (Grad = true, the reference's 43-entry Jacobian,
+// codegen/transport_jacobian.hpp) also P = d(pos)/d(pos0) and
+// Q = d(dir)/d(pos0), which the gradient of an inhomogeneous field makes
+// differ from the identity and zero.  Kept out of the default form so that
+// kernels without the gradient do not carry 18 more live values.
 template <typename S>
-struct transport_jac {
+struct transport_jac_blocks {
     mat33<S> A;
     mat33<S> B;
     vec3<S> c;
     vec3<S> d;
     S e;
 
-    DPROP_HD void reset() {
+    DPROP_HD void reset_blocks() {
         for (int i = 0; i < 9; ++i) {
             A.m[i] = S(0);
         }
@@ -39,16 +44,38 @@ struct transport_jac {
     }
 };
 
+template <typename S, bool Grad = false>
+struct transport_jac : transport_jac_blocks<S> {
+    static constexpr bool gradient = false;
+    DPROP_HD void reset() { this->reset_blocks(); }
+};
+
+template <typename S>
+struct transport_jac<S, true> : transport_jac_blocks<S> {
+    static constexpr bool gradient = true;
+    mat33<S> P;
+    mat33<S> Q;
+    DPROP_HD void reset() {
+        this->reset_blocks();
+        P = identity33<S>();
+        for (int i = 0; i < 9; ++i) {
+            Q.m[i] = S(0);
+        }
+    }
+};
+
 template <typename S>
 struct step_cfg {
     S min_stepsize;
     S rk_error_tol;
     uint32_t max_rk_updates;
     bool do_covariance_transport;
+    bool field_gradient;  // use_field_gradient: kernels with Grad = true
 };
 
-// Per-track stepper state (rk_stepper::state + base_stepper::state)
-template <typename S>
+// Per-track stepper state (rk_stepper::state + base_stepper::state); Grad:
+// the transport Jacobian includes the field gradient.
+template <typename S, bool Grad = false>
 struct step_state {
     vec3<S> pos;
     vec3<S> dir;
@@ -61,7 +88,7 @@ struct step_state {
     vec3<S> dtds;            // dt/ds at the end of the last step
     S dqopds;
     S constraint;            // min over the step constraints (accuracy, aborter)
-    transport_jac<S> jac;
+    transport_jac<S, Grad> jac;
     uint32_t n_trials;
     uint32_t n_steps;
 };
@@ -72,8 +99,8 @@ DPROP_HD S step_size_scaling(S tol, S err) {
 }
 
 // dt/ds of the state when no step was taken yet (rk_stepper::state::dtds)
-template <typename S>
-DPROP_HD vec3<S> current_dtds(const step_state<S>& st,
+template <typename S, bool Grad>
+DPROP_HD vec3<S> current_dtds(const step_state<S, Grad>& st,
                               const field_view<S>& field) {
     if (st.path_length == 0.) {
         const vec3<S> b = field_at(field, st.pos);
@@ -82,9 +109,102 @@ DPROP_HD vec3<S> current_dtds(const step_state<S>& st,
     return st.dtds;
 }
 
-// One adaptive RKN4 step towards a surface at (signed) distance dist.
+// Central-difference gradient of the field, dB/dr (column i = dB/dr_i),
+// with the reference's offset of 0.1 mm as a float literal
+// (rk_stepper::evaluate_field_gradient, rk_stepper.hpp:958-997).
 template <typename S>
-DPROP_HD bool rk_step(step_state<S>& st, S dist, const step_cfg<S>& cfg,
+DPROP_HD mat33<S> field_gradient(const field_view<S>& field, vec3<S> p) {
+    const S delta = static_cast<S>(0.1f) * S(unit::mm);
+    const S inv = S(1) / (S(2) * delta);
+    mat33<S> g;
+    for (int i = 0; i < 3; ++i) {
+        const vec3<S> e{i == 0 ? delta : S(0), i == 1 ? delta : S(0),
+                        i == 2 ? delta : S(0)};
+        const vec3<S> b1 = field_at(field, p + e);
+        const vec3<S> b2 = field_at(field, p - e);
+        const vec3<S> d = (b1 - b2) * inv;
+        g(0, i) = d.x;
+        g(1, i) = d.y;
+        g(2, i) = d.z;
+    }
+    return g;
+}
+
+template <typename S>
+DPROP_HD mat33<S> matmul33(const mat33<S>& a, const mat33<S>& b) {
+    mat33<S> r;
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) {
+            S v = S(0);
+            for (int k = 0; k < 3; ++k) {
+                v += a(i, k) * b(k, j);
+            }
+            r(i, j) = v;
+        }
+    }
+    return r;
+}
+
+// d(k_n)/d(r_1) of the four RKN stages with the field gradient (the
+// reference's with-gradient transport, rk_stepper.hpp:872-938): k_n =
+// qop (t_n x B(r_n)), so dk_n/dr_1 = qop (dt_n/dr_1 x B_n) - qop (dB_n/dr_n
+// dr_n/dr_1 (x) t_n) with the stage tables dt_n/dr_1 and dr_n/dr_1; returns
+// dF/dr = I + h^2/6 (dk1 + dk2 + dk3) and dG/dr = h/6 (dk1 + 2 (dk2 + dk3)
+// + dk4).
+template <typename S>
+DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
+                                      vec3<S> pos1, vec3<S> pos2, S h, S qop,
+                                      vec3<S> t0, vec3<S> t1, vec3<S> t2,
+                                      vec3<S> t3, vec3<S> b_middle,
+                                      vec3<S> b_last, mat33<S>& dFdr,
+                                      mat33<S>& dGdr) {
+    const S half_h = h * S(0.5);
+    const S h2 = h * h;
+    const mat33<S> I = identity33<S>();
+    const mat33<S> g_ini = field_gradient(field, pos);
+    const mat33<S> g_mid = field_gradient(field, pos1);
+    const mat33<S> g_fin = field_gradient(field, pos2);
+    mat33<S> k1 = colwise_cross(g_ini, t0);
+    for (int i = 0; i < 9; ++i) {
+        k1.m[i] *= -qop;
+    }
+    // dr_2/dr_1 = dr_3/dr_1 = I + h^2/8 dk1/dr1
+    mat33<S> r23;
+    for (int i = 0; i < 9; ++i) {
+        r23.m[i] = I.m[i] + h2 * S(0.125) * k1.m[i];
+    }
+    const mat33<S> gr23 = matmul33(g_mid, r23);
+    auto stage = [&](const mat33<S>& prev, S f, vec3<S> b, const mat33<S>& gr,
+                     vec3<S> t) {
+        mat33<S> a;
+        for (int i = 0; i < 9; ++i) {
+            a.m[i] = f * prev.m[i];
+        }
+        const mat33<S> x = colwise_cross(a, b);
+        const mat33<S> y = colwise_cross(gr, t);
+        mat33<S> r;
+        for (int i = 0; i < 9; ++i) {
+            r.m[i] = qop * x.m[i] - qop * y.m[i];
+        }
+        return r;
+    };
+    const mat33<S> k2 = stage(k1, half_h, b_middle, gr23, t1);
+    const mat33<S> k3 = stage(k2, half_h, b_middle, gr23, t2);
+    mat33<S> r4;
+    for (int i = 0; i < 9; ++i) {
+        r4.m[i] = I.m[i] + h2 * S(0.5) * k3.m[i];
+    }
+    const mat33<S> k4 = stage(k3, h, b_last, matmul33(g_fin, r4), t3);
+    const S h_6 = h * static_cast<S>(1. / 6.);
+    for (int i = 0; i < 9; ++i) {
+        dFdr.m[i] = I.m[i] + h * h_6 * (k1.m[i] + k2.m[i] + k3.m[i]);
+        dGdr.m[i] = h_6 * (k1.m[i] + S(2) * (k2.m[i] + k3.m[i]) + k4.m[i]);
+    }
+}
+
+// One adaptive RKN4 step towards a surface at (signed) distance dist.
+template <typename S, bool Grad>
+DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
                       bool do_reset, const field_view<S>& field) {
     const S um = S(unit::um);
     if (fabs(dist) < um) {
@@ -209,43 +329,101 @@ DPROP_HD bool rk_step(step_state<S>& st, S dist, const step_cfg<S>& cfg,
         }
 
         // J <- D * J on the non-trivial blocks
-        transport_jac<S>& J = st.jac;
-        mat33<S> nA, nB;
-        vec3<S> nc, nd;
-        for (int r = 0; r < 3; ++r) {
-            for (int c = 0; c < 3; ++c) {
-                S a = J.A(r, c);
-                S b = S(0);
-                for (int k = 0; k < 3; ++k) {
-                    a += dFdt(r, k) * J.B(k, c);
-                    b += dGdt(r, k) * J.B(k, c);
+        transport_jac<S, Grad>& J = st.jac;
+        if constexpr (Grad) {
+            // position columns: P' = dFdr P + dFdt Q, Q' = dGdr P + dGdt Q;
+            // the direction and q/p columns take dFdr / dGdr below.  The
+            // field gradients are taken where the reference takes them: it
+            // advances the track before the Jacobian (rk_stepper.hpp:511-519)
+            // and offsets the three points from the advanced position
+            // (rk_stepper.hpp:885-897), so they lie one step further along
+            // than the stages of the step
+            const vec3<S> base = st.pos;
+            const vec3<S> pos1 = base + half_h * t0 + (h * h * S(0.125)) * k0;
+            const vec3<S> pos2 = base + h * t0 + (h * h * S(0.5)) * k2;
+            mat33<S> dFdr, dGdr;
+            rk_position_derivatives(field, base, pos1, pos2, h, qop, t0, t1,
+                                    t2, t3, b_middle, b_last, dFdr, dGdr);
+            mat33<S> nP, nQ;
+            for (int r = 0; r < 3; ++r) {
+                for (int c = 0; c < 3; ++c) {
+                    S p = S(0), q = S(0);
+                    for (int k = 0; k < 3; ++k) {
+                        p += dFdr(r, k) * J.P(k, c) + dFdt(r, k) * J.Q(k, c);
+                        q += dGdr(r, k) * J.P(k, c) + dGdt(r, k) * J.Q(k, c);
+                    }
+                    nP(r, c) = p;
+                    nQ(r, c) = q;
                 }
-                nA(r, c) = a;
-                nB(r, c) = b;
             }
-        }
-        const S jd[3] = {J.d.x, J.d.y, J.d.z};
-        const S fq[3] = {dFdqop.x, dFdqop.y, dFdqop.z};
-        const S gq[3] = {dGdqop.x, dGdqop.y, dGdqop.z};
-        const S jc[3] = {J.c.x, J.c.y, J.c.z};
-        S ncv[3], ndv[3];
-        for (int r = 0; r < 3; ++r) {
-            S a = jc[r] + fq[r] * J.e;
-            S b = gq[r] * J.e;
-            for (int k = 0; k < 3; ++k) {
-                a += dFdt(r, k) * jd[k];
-                b += dGdt(r, k) * jd[k];
+            mat33<S> nA, nB;
+            S ncv[3], ndv[3];
+            const S jc[3] = {J.c.x, J.c.y, J.c.z};
+            const S jd[3] = {J.d.x, J.d.y, J.d.z};
+            const S fq[3] = {dFdqop.x, dFdqop.y, dFdqop.z};
+            const S gq[3] = {dGdqop.x, dGdqop.y, dGdqop.z};
+            for (int r = 0; r < 3; ++r) {
+                for (int c = 0; c < 3; ++c) {
+                    S a = S(0), b = S(0);
+                    for (int k = 0; k < 3; ++k) {
+                        a += dFdr(r, k) * J.A(k, c) + dFdt(r, k) * J.B(k, c);
+                        b += dGdr(r, k) * J.A(k, c) + dGdt(r, k) * J.B(k, c);
+                    }
+                    nA(r, c) = a;
+                    nB(r, c) = b;
+                }
+                S a = fq[r] * J.e, b = gq[r] * J.e;
+                for (int k = 0; k < 3; ++k) {
+                    a += dFdr(r, k) * jc[k] + dFdt(r, k) * jd[k];
+                    b += dGdr(r, k) * jc[k] + dGdt(r, k) * jd[k];
+                }
+                ncv[r] = a;
+                ndv[r] = b;
             }
-            ncv[r] = a;
-            ndv[r] = b;
+            J.P = nP;
+            J.Q = nQ;
+            J.A = nA;
+            J.B = nB;
+            J.c = {ncv[0], ncv[1], ncv[2]};
+            J.d = {ndv[0], ndv[1], ndv[2]};
+        } else {
+            mat33<S> nA, nB;
+            vec3<S> nc, nd;
+            for (int r = 0; r < 3; ++r) {
+                for (int c = 0; c < 3; ++c) {
+                    S a = J.A(r, c);
+                    S b = S(0);
+                    for (int k = 0; k < 3; ++k) {
+                        a += dFdt(r, k) * J.B(k, c);
+                        b += dGdt(r, k) * J.B(k, c);
+                    }
+                    nA(r, c) = a;
+                    nB(r, c) = b;
+                }
+            }
+            const S jd[3] = {J.d.x, J.d.y, J.d.z};
+            const S fq[3] = {dFdqop.x, dFdqop.y, dFdqop.z};
+            const S gq[3] = {dGdqop.x, dGdqop.y, dGdqop.z};
+            const S jc[3] = {J.c.x, J.c.y, J.c.z};
+            S ncv[3], ndv[3];
+            for (int r = 0; r < 3; ++r) {
+                S a = jc[r] + fq[r] * J.e;
+                S b = gq[r] * J.e;
+                for (int k = 0; k < 3; ++k) {
+                    a += dFdt(r, k) * jd[k];
+                    b += dGdt(r, k) * jd[k];
+                }
+                ncv[r] = a;
+                ndv[r] = b;
+            }
+            nc = {ncv[0], ncv[1], ncv[2]};
+            nd = {ndv[0], ndv[1], ndv[2]};
+            J.A = nA;
+            J.B = nB;
+            J.c = nc;
+            J.d = nd;
+            // J.e unchanged: dqopqop = 1
         }
-        nc = {ncv[0], ncv[1], ncv[2]};
-        nd = {ndv[0], ndv[1], ndv[2]};
-        J.A = nA;
-        J.B = nB;
-        J.c = nc;
-        J.d = nd;
-        // J.e unchanged: dqopqop = 1
     }
     return true;
 }

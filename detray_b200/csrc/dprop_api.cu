@@ -158,7 +158,8 @@ constexpr int k_plain_block = DPROP_BLOCK;
 // thread (the rest spills to L1).  More resident warps hide more of the
 // navigation's memory and instruction-fetch latency; the best budget depends
 // on the workload (constant field vs field map), so it is a launch choice.
-template <typename In, int MinBlocks = DPROP_MIN_BLOCKS, bool W = true>
+template <typename In, int MinBlocks = DPROP_MIN_BLOCKS, bool W = true,
+          bool Grad = false>
 __global__ void __launch_bounds__(k_plain_block, MinBlocks)
     propagate_plain_kernel(const __grid_constant__ detector_view<float, W> det,
                            const __grid_constant__ field_view<float> field,
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(k_plain_block, MinBlocks)
         return;
     }
     const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
-    run_one(t, n, det, field, cfg, io);
+    run_one<In, false, float, W, Grad>(t, n, det, field, cfg, io);
 }
 
 }  // namespace
@@ -245,12 +246,26 @@ using dprop::api::sort_scratch_bytes;
 namespace {
 
 // The plain kernel for a detector: without the wire-surface code unless the
-// detector needs it.
+// detector needs it.  With the field gradient (use_field_gradient) the
+// kernel carries the 18 position-column entries of the transport Jacobian;
+// it is built for one register budget (8 CTAs per SM, 64 registers).
 template <typename In, int MB>
 void launch_plain_mb(unsigned int grid, cudaStream_t st,
                      const dprop_detector* det,
                      const field_view<float>& field, const prop_cfg<float>& cfg,
                      const io_ptrs<In>& io, uint64_t n, const uint32_t* order) {
+    if (cfg.step.field_gradient) {
+        if (det->wires) {
+            propagate_plain_kernel<In, 8, true, true>
+                <<<grid, k_plain_block, 0, st>>>(det->view_as<true>(), field,
+                                                 cfg, io, n, order);
+        } else {
+            propagate_plain_kernel<In, 8, false, true>
+                <<<grid, k_plain_block, 0, st>>>(det->view_as<false>(), field,
+                                                 cfg, io, n, order);
+        }
+        return;
+    }
     if (det->wires) {
         propagate_plain_kernel<In, MB, true><<<grid, k_plain_block, 0, st>>>(
             det->view_as<true>(), field, cfg, io, n, order);
@@ -460,10 +475,6 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
 dprop_status check_config(const dprop_config* cfg) {
     if (!cfg) {
         return fail(DPROP_E_INVALID, "config is NULL");
-    }
-    if (cfg->use_field_gradient) {
-        return fail(DPROP_E_UNSUPPORTED,
-                    "use_field_gradient is not supported on the device path");
     }
     if (cfg->use_eloss_gradient) {
         return fail(DPROP_E_UNSUPPORTED,

@@ -23,7 +23,7 @@ namespace {
 
 constexpr int k_f64_block = 128;
 
-template <int MinBlocks>
+template <int MinBlocks, bool Grad = false>
 __global__ void __launch_bounds__(k_f64_block, MinBlocks)
     propagate_fp64_kernel(const __grid_constant__ detector_view<double> det,
                           const __grid_constant__ field_view<double> field,
@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(k_f64_block, MinBlocks)
         return;
     }
     const uint64_t t = order ? static_cast<uint64_t>(order[i]) : i;
-    api::run_one(t, n, det, field, cfg, io);
+    api::run_one<double, false, double, true, Grad>(t, n, det, field, cfg, io);
 }
 
 // library-owned grow-only sort scratch of fp64 launches
@@ -88,7 +88,10 @@ dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
     const prop_cfg<double> pc = make_prop_cfg<double>(c);
     const unsigned int grid =
         static_cast<unsigned int>((n + k_f64_block - 1) / k_f64_block);
-    if (occupancy_of(lc) >= 12) {
+    if (c.use_field_gradient) {
+        propagate_fp64_kernel<8, true><<<grid, k_f64_block, 0, stream>>>(
+            det->view_d(), field->view_d, pc, io, n, order);
+    } else if (occupancy_of(lc) >= 12) {
         propagate_fp64_kernel<12><<<grid, k_f64_block, 0, stream>>>(
             det->view_d(), field->view_d, pc, io, n, order);
     } else {

@@ -483,6 +483,11 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
     if (n > 0xffffff00ull) {
         return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
     }
+    if (cfg.step.field_gradient) {
+        return fail(DPROP_E_UNSUPPORTED,
+                    "persistent method: use_field_gradient runs with the "
+                    "plain method only");
+    }
     if (scratch_bytes < rounds_scratch_bytes(n, det->wires)) {
         return fail(DPROP_E_INVALID, "persistent method: scratch too small");
     }

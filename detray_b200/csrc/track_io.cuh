@@ -61,8 +61,10 @@ io_ptrs<In, S> make_io(const dprop_tracks& t, const dprop_results& r) {
 
 // One track from its inputs to its results, in arithmetic type S.  With
 // Adjoint the propagation also writes the derivative tape of track t
-// (adjoint.cuh).
-template <typename In, bool Adjoint = false, typename S = float, bool W>
+// (adjoint.cuh); with Grad the transport Jacobian includes the field
+// gradient.
+template <typename In, bool Adjoint = false, typename S = float, bool W,
+          bool Grad = false>
 __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
                                         const detector_view<S, W>& det,
                                         const field_view<S>& field,
@@ -79,7 +81,7 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     const S qop = static_cast<S>(io.trk[7][t]);
 
     nav_cache<S> cache;
-    track_state<S> ts;
+    track_state<S, Grad> ts;
     bind_cache(ts.nav, cache);
     init_track_state(ts, pos, time, dir, qop, cfg);
 

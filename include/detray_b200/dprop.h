@@ -222,7 +222,13 @@ typedef struct dprop_config {
     uint32_t max_rk_updates;
     uint8_t use_mean_loss;
     uint8_t use_eloss_gradient;
-    uint8_t use_field_gradient;
+    uint8_t use_field_gradient;  /* transport Jacobian with the field's
+                                    gradient (d(pos)/d(pos0), d(dir)/d(pos0)
+                                    from central differences of the field,
+                                    rk_stepper.hpp:872-997): plain method and
+                                    adjoint mode, 64 registers; the
+                                    persistent method and the direct
+                                    navigator reject it                   */
     uint8_t do_covariance_transport;
     /* intersection::config */
     float min_mask_tolerance;
@@ -603,7 +609,9 @@ dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
  * The q/p row and time column of the Jacobians are identity (the reference's
  * convention), so time derivatives pass straight through.  Step sizes and
  * navigation decisions are constants of the derivative; the field map's
- * gradient is not differentiated (as in the reference's Jacobian). */
+ * gradient enters through the position columns of the transport Jacobian
+ * when cfg->use_field_gradient is set (the reference's with-gradient
+ * Jacobian), and is left out otherwise (its default). */
 #define DPROP_TAPE_RECORD_FLOATS 27u
 #define DPROP_TAPE_TRACK_FLOATS 35u
 

@@ -40,8 +40,8 @@ struct direct_args {
     const double* const* start_bound;
 };
 
-template <typename S>
-int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
+template <typename S, bool Grad = false>
+int run_g(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
         const double* lo, const double* hi, const uint32_t* nn,
         const float* values, const dprop_config* c, const double* const* trk,
         uint64_t n, const dprop_results* out, double* tape_rec = nullptr,
@@ -84,7 +84,7 @@ int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
     const uint32_t cap = c->max_records;
     for (uint64_t t = 0; t < n; ++t) {
         nav_cache<S> cache;
-        track_state<S> ts;
+        track_state<S, Grad> ts;
         bind_cache(ts.nav, cache);
         bool start_ok = true;
         if (da != nullptr && da->start_barcode != nullptr) {
@@ -399,6 +399,22 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
         }
     }
     return 0;
+}
+
+// run_g with the transport Jacobian including the field gradient when the
+// configuration asks for it (use_field_gradient).
+template <typename S>
+int run(const dprop_detector_desc* desc, uint32_t field_kind, const double* b,
+        const double* lo, const double* hi, const uint32_t* nn,
+        const float* values, const dprop_config* c, const double* const* trk,
+        uint64_t n, const dprop_results* out, double* tape_rec = nullptr,
+        double* tape_init = nullptr, const direct_args* da = nullptr) {
+    if (c->use_field_gradient) {
+        return run_g<S, true>(desc, field_kind, b, lo, hi, nn, values, c, trk,
+                              n, out, tape_rec, tape_init, da);
+    }
+    return run_g<S, false>(desc, field_kind, b, lo, hi, nn, values, c, trk, n,
+                           out, tape_rec, tape_init, da);
 }
 
 // The round-based propagation of the phase kernels, simulated on the host

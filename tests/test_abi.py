@@ -106,7 +106,7 @@ def test_argument_validation_without_device(lib):
                                        None, 0, None) == abi.DPROP_E_INVALID
     assert lib.dprop_backward(None, None, None, None, None, None, 0,
                               None) == abi.DPROP_E_INVALID
-    cfg = abi.make_config(use_field_gradient=1)
+    cfg = abi.make_config(use_eloss_gradient=1)
     assert lib.dprop_propagate(C.byref(cfg), None, None, None, None, None, 0,
                                None) == abi.DPROP_E_UNSUPPORTED
     assert lib.dprop_propagate_direct(None, None, None, None, None, None, 0,

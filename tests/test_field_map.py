@@ -163,3 +163,33 @@ def test_loopers_reach_path_limit(core_host, oracle, solenoid):
     # the signed path length never exceeds the limit on the absolute path
     # (curling tracks also step backwards onto surfaces they overstepped)
     assert np.all(np.abs(got["path_length"]) <= 5000.0 + 1.0)
+
+
+def test_field_gradient_transport_matches_reference(core_host, oracle,
+                                                    solenoid):
+    """use_field_gradient in the solenoid map: the transport Jacobian with
+    the field's gradient (position columns from central differences of the
+    field at the three RKN points) gives the reference's covariances (the
+    oracle runs the reference's with-gradient rk_stepper); without it the
+    covariances differ where the map varies."""
+    from detray_b200 import abi, tracks
+    det = oracle.build_toy()
+    trk = tracks.toy_tracks(800, seed=23, pt_range=(0.5, 10.0),
+                            eta_range=(-3.0, 3.0))
+    tight = {"loc0": 1e-6, "loc1": 1e-6, "phi": 1e-8, "theta": 1e-8,
+             "qop": 1e-11, "time": 1e-12}
+    cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                          estimate_scattering_noise=0, use_field_gradient=1)
+    ref = oracle.propagate(det, solenoid, cfg, trk)
+    got = _core_in_map(core_host, oracle, det, solenoid, cfg, trk)
+    s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=tight,
+                tol_rel=1e-6, cov_rel=1e-5)
+    assert s["seq_mismatch"] == 0
+    cfg0 = abi.make_config(max_records=32, search_window=(3, 3),
+                           estimate_scattering_noise=0)
+    plain = _core_in_map(core_host, oracle, det, solenoid, cfg0, trk)
+    m = (np.arange(32)[:, None] < got["n_records"][None, :]) & \
+        ((got["rec_flags"] & 1) > 0)
+    dcov = np.abs(plain["rec_cov"][0][m] - got["rec_cov"][0][m]) / \
+        np.abs(got["rec_cov"][0][m])
+    assert dcov.max() > 1e-4  # the gradient changes the transported errors

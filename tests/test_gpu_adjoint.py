@@ -17,6 +17,10 @@ from tests import adjoint_host as ah
 
 pytestmark = pytest.mark.gpu
 
+# device float32 gradient against fp64 finite differences: relative, with a
+# floor of 1e-3 of the component's rms
+TOL_FD = 5e-3
+
 
 @pytest.fixture(scope="module")
 def torch_cuda():
@@ -173,3 +177,50 @@ def test_adjoint_edge_cases(torch_cuda):
                                      C.byref(propagator.tracks_struct(dev)),
                                      C.byref(r.struct), C.byref(bad), 4, None)
     assert rc == abi.DPROP_E_INVALID
+
+
+def test_device_gradients_in_field_map_match_finite_differences(torch_cuda,
+                                                                core_host):
+    """Benchmark configuration 4 in small: the toy detector in the solenoid
+    field map with use_field_gradient (the transport Jacobian carries the
+    field's gradient).  The device's float32 gradients with respect to the
+    initial position, direction and q/p, for a random linear loss on the
+    recorded bound parameters, against fp64 central finite differences of
+    the host core's forward propagation, every component of every track
+    whose records agree (steps capped at 2 mm so that the landing error of
+    the forward stays below the tolerance)."""
+    from detray_b200 import abi, fields, geometry, propagator, tracks
+    from tests.test_adjoint_host import STEPS, _analytic, _perturbed
+    fmap = fields.solenoid_map()
+    tables = geometry.load_geometry("toy_4brl_7edc")
+    det = propagator.Detector(tables)
+    field = propagator.Field.grid(fmap)
+    cfg = abi.make_config(max_records=32, search_window=(3, 3),
+                          step_constraint=2.0, use_field_gradient=1)
+    trk = tracks.toy_tracks(48, seed=12, pt_range=(0.5, 50.0),
+                            eta_range=(-2.5, 2.5), pt_log_uniform=False)
+    href, _ = ah.forward(core_host, tables, cfg, trk, field=fmap)
+    W = ah.random_weights(href, cfg.max_records, seed=3)
+    _, dres, dfree, _ = _device_adjoint(torch_cuda, cfg, det, field, trk, W)
+    same_dev = ah.same_records(
+        href, {"n_records": dres["n_records"].astype(np.uint32),
+               "rec_barcode": dres["rec_barcode"]})
+    checked = 0
+    worst = 0.0
+    for which in (0, 1, 2, "phi", "theta", 7):
+        h = STEPS[which]
+        rp, _ = ah.forward(core_host, tables, cfg, _perturbed(trk, which, h),
+                           field=fmap, adjoint=False)
+        rm, _ = ah.forward(core_host, tables, cfg, _perturbed(trk, which, -h),
+                           field=fmap, adjoint=False)
+        ok = ah.same_records(rp, rm) & same_dev
+        fd = ah.loss_difference(rp, rm, W) / (2 * h)
+        an = _analytic(dfree.astype(np.float64), trk, which)
+        scale = np.sqrt(np.mean(fd[ok] ** 2)) + 1e-30
+        err = np.abs(an - fd)[ok] / (np.abs(fd[ok]) + 1e-3 * scale)
+        print(which, float(err.max()))
+        worst = max(worst, float(err.max()))
+        checked += int(ok.sum())
+        assert (err < TOL_FD).all(), (which, float(err.max()))
+    assert checked >= 6 * 40
+    print("worst", worst)

@@ -195,7 +195,7 @@ def test_empty_batch_and_invalid_arguments(torch_cuda):
     rc = lib.dprop_propagate(C.byref(cfg), None, None, field.handle,
                              C.byref(ts), C.byref(res.struct), 1, None)
     assert rc == abi.DPROP_E_INVALID
-    bad = abi.make_config(use_field_gradient=1)
+    bad = abi.make_config(use_eloss_gradient=1)
     rc = lib.dprop_propagate(C.byref(bad), None, det.handle, field.handle,
                              C.byref(ts), C.byref(res.struct), 1, None)
     assert rc == abi.DPROP_E_UNSUPPORTED
