@@ -200,7 +200,7 @@ DPROP_HD uint8_t machine_step(track_state<S>& ts, loop_state<S>& ls,
         ls.stall = 0u;
     }
     if constexpr (W) {
-        skip_cycles(ls.cyc, st, cfg.act.path_limit);
+        skip_cycles(ls.cyc, st, nav.dist(), cfg.act.path_limit);
     }
     return machine_nav_fast(ts, ls, det, cfg);
 }

@@ -272,8 +272,9 @@ DPROP_HD void rk_policy(nav_state<S>& nav, const step_state<S, Grad>& st) {
     }
 }
 
-// 32-bit key of the exact bit pattern of the free state (position,
-// direction, q/p): equal states give equal keys; different ones almost
+// 32-bit key of the exact bit pattern of the state that decides the next
+// step: position, direction, q/p, the step sizes and the distance to the
+// navigation target.  Equal states give equal keys; different ones almost
 // never do.
 DPROP_HD uint32_t scalar_bits(float v) {
 #if defined(__CUDA_ARCH__)
@@ -294,14 +295,17 @@ DPROP_HD uint32_t scalar_bits(double v) {
     return static_cast<uint32_t>(u) ^ static_cast<uint32_t>(u >> 32);
 }
 template <typename S, bool Grad>
-DPROP_HD uint32_t state_key(const step_state<S, Grad>& st) {
+DPROP_HD uint32_t state_key(const step_state<S, Grad>& st, S target) {
     uint32_t h = scalar_bits(st.pos.x);
     h = h * 0x9e3779b1u ^ scalar_bits(st.pos.y);
     h = h * 0x9e3779b1u ^ scalar_bits(st.pos.z);
     h = h * 0x85ebca6bu ^ scalar_bits(st.dir.x);
     h = h * 0x85ebca6bu ^ scalar_bits(st.dir.y);
     h = h * 0x85ebca6bu ^ scalar_bits(st.dir.z);
-    return h * 0xc2b2ae35u ^ scalar_bits(st.qop);
+    h = h * 0xc2b2ae35u ^ scalar_bits(st.qop);
+    h = h * 0x27d4eb2fu ^ scalar_bits(st.step_size);
+    h = h * 0x27d4eb2fu ^ scalar_bits(st.next_step_size);
+    return h * 0x165667b1u ^ scalar_bits(target);
 }
 
 // Exact cycles of the stepping (not in the reference).  A looper whose
@@ -345,7 +349,7 @@ struct cycle_search {
 // checks the two agree).
 template <typename S, bool Grad>
 DPROP_HD void skip_cycles(cycle_search<S>& c, step_state<S, Grad>& st,
-                          S path_limit) {
+                          S target, S path_limit) {
 #if defined(DPROP_NO_CYCLE_SKIP)
     return;
 #endif
@@ -356,7 +360,7 @@ DPROP_HD void skip_cycles(cycle_search<S>& c, step_state<S, Grad>& st,
     if (!(fabs(st.step_size) < S(1)) || c.hits == cycle_search<S>::k_done) {
         return;
     }
-    const uint32_t key = state_key(st);
+    const uint32_t key = state_key(st, target);
     ++c.lam;
     if (key == c.key) {
         c.hits = (c.lam == c.period) ? c.hits + 1u : 1u;
@@ -488,7 +492,7 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S, Grad>& ts,
             // tracks of the toy detector, where the search costs 3-4 % of
             // the propagation time.
             if constexpr (W) {
-                skip_cycles(cyc, st, cfg.act.path_limit);
+                skip_cycles(cyc, st, nav.dist(), cfg.act.path_limit);
             }
         }
         is_init = navigator.update(nav, det, track_view<S>{st.pos, st.dir},

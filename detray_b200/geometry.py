@@ -8,7 +8,7 @@ descriptor that ``dprop_detector_create`` consumes.
 
 Benchmark geometries ship as ``detray_b200/geometries/*.npz``; they are the
 reference's own toy and telescope builders flattened by the product adapter
-(see geometries/make_geometries.py).
+(see oracle/geometries/make_geometries.py).
 """
 from __future__ import annotations
 
@@ -38,7 +38,8 @@ def dtype_of(ctype) -> np.dtype:
 
 
 def read_raw_tables(path) -> dict:
-    """Read the raw table file written by geometries/export_geometry.cpp."""
+    """Read the raw table file written by oracle/geometries/export_geometry.cpp
+    (the geometry regeneration step)."""
     data = Path(path).read_bytes()
     header = np.frombuffer(data[:48], dtype=np.uint32)
     if header[0] != 0x4F454744:

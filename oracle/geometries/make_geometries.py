@@ -1,8 +1,10 @@
-"""Regenerate the committed benchmark geometries (build-time step).
+"""Regenerate the committed benchmark geometries (build-time step, not part
+of the product).
 
 Compiles export_geometry.cpp against the detray headers of a reference
-checkout (path in $DETRAY_REF, default /root/reference) and packs the tables
-of the benchmark detectors into compressed .npz files next to this script:
+checkout (path given by --ref or $DETRAY_REF) and the vecmem stand-in
+oracle/shim, and packs the tables of the benchmark detectors into the
+compressed .npz files the product loads (detray_b200/geometries/):
 
   toy_4brl_7edc.npz          toy barrel + endcap detector, 4 barrel layers,
                              7 endcap discs per side, 0.15 mm Si modules
@@ -26,6 +28,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
+OUT = REPO / "detray_b200" / "geometries"
 sys.path.insert(0, str(REPO))
 
 from detray_b200 import geometry  # noqa: E402
@@ -42,7 +45,7 @@ TELESCOPE_POSITIONS = [str(50.0 * i) for i in range(10)]
 
 def build_exporter(ref: Path, out: Path) -> None:
     cmd = ["g++", "-std=c++20", "-O3", "-march=x86-64-v3", "-w", "-DDETRAY_ALGEBRA_ARRAY=1",
-           "-DDETRAY_CUSTOM_SCALARTYPE=double", f"-I{HERE / 'shim'}",
+           "-DDETRAY_CUSTOM_SCALARTYPE=double", f"-I{HERE.parent / 'shim'}",
            f"-I{ref / 'core/include'}",
            f"-I{ref / 'plugins/algebra/array/include'}",
            f"-I{ref / 'detectors/include'}", f"-I{ref / 'tests/include'}",
@@ -52,7 +55,12 @@ def build_exporter(ref: Path, out: Path) -> None:
 
 
 def main() -> None:
-    ref = Path(os.environ.get("DETRAY_REF", "/root/reference"))
+    args = sys.argv[1:]
+    ref = (Path(args[args.index("--ref") + 1]) if "--ref" in args
+           else Path(os.environ.get("DETRAY_REF", "")))
+    if not (ref / "core" / "include" / "detray").exists():
+        raise SystemExit("give the reference checkout: --ref PATH or "
+                         "DETRAY_REF=PATH")
     with tempfile.TemporaryDirectory() as tmp:
         exe = Path(tmp) / "export_geometry"
         build_exporter(ref, exe)
@@ -61,7 +69,7 @@ def main() -> None:
             extra = TELESCOPE_POSITIONS if args[0] == "telescope" else args[4:]
             subprocess.run([str(exe), *args[:4], str(raw), *extra], check=True)
             tables = geometry.read_raw_tables(raw)
-            geometry.save_npz(tables, HERE / f"{name}.npz")
+            geometry.save_npz(tables, OUT / f"{name}.npz")
             print(f"wrote {name}.npz: "
                   + ", ".join(f"{k}={len(v)}" for k, v in tables.items()))
 

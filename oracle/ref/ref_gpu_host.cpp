@@ -4,7 +4,7 @@
  * Host driver of the reference's own CUDA propagation kernel (ref_gpu.cu),
  * compiled from the reference's headers where they lie in the reference
  * checkout.  vecmem (not vendored) is replaced by the stand-in under
- * detray_b200/geometries/shim, whose view types carry device annotations
+ * oracle/shim, whose view types carry device annotations
  * under nvcc; the toy detector is built by the reference's own builder into
  * CUDA managed memory, so that its host views are valid in device code (as
  * in the reference benchmark's managed-memory variant); covfie's constant

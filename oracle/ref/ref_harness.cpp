@@ -6,7 +6,7 @@
  *
  * This file compiles the reference detray propagator itself (its headers,
  * where they lie in the reference checkout, plus the host-only vecmem stand-in
- * in detray_b200/geometries/shim) into a shared library with a small C interface:
+ * in oracle/shim) into a shared library with a small C interface:
  *
  *   - ref_build_toy / ref_build_telescope: the reference's own detector
  *     builders (tests/include/detray/test/common/build_toy_detector.hpp:1237,

@@ -18,6 +18,7 @@ Usage: python tests/golden/make_golden.py [reference checkout]
 from __future__ import annotations
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -52,7 +53,10 @@ def bethe_cases(ref: Path) -> list[dict]:
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
-    ref = Path(argv[0]) if argv else Path("/root/reference")
+    ref = Path(argv[0]) if argv else Path(os.environ.get("DETRAY_REF", ""))
+    if not (ref / "tests").exists():
+        raise SystemExit("give the reference checkout: make_golden.py PATH "
+                         "or DETRAY_REF=PATH")
     cases = bethe_cases(ref)
     (HERE / "bethe_pdg.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(f"bethe_pdg.json: {len(cases)} cases")
