@@ -130,7 +130,7 @@ DPROP_HD void surf_inline(track_state<S>& ts, const slot_soa<S>& s,
     loop_state<S> unused;
     load_slot(s, slot, g_bound | g_count, ts, unused);
     rec.count = s.rec_count[slot];
-    rec.track = s.track[slot];
+    rec.track = rec.stage ? slot : s.track[slot];
     machine_surf(ts, det, field, cfg, rec, no_tape{});
     store_slot(s, slot, g_bound | g_count, ts, unused);
     s.rec_count[slot] = rec.count;
@@ -212,9 +212,10 @@ DPROP_HD track_outputs<S> phase_tail(const slot_soa<S>& s, uint64_t slot,
     }
     ls.pc = s.pc[slot];
     rec.count = s.rec_count[slot];
-    rec.track = s.track[slot];
+    rec.track = rec.stage ? slot : s.track[slot];
     machine_run(ts, ls, det, field, cfg, rec);
     s.pc[slot] = pc_done;
+    s.rec_count[slot] = rec.count;
     return make_outputs(ts, ls, rec.count);
 }
 

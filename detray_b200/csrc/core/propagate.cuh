@@ -26,9 +26,22 @@ struct prop_cfg {
     uint32_t max_iterations;
 };
 
+// Words of one staged record: barcode, 6 bound parameters, 21 covariance
+// entries, path and flags, padded to a whole number of 16-byte vectors.
+template <typename S>
+constexpr int staged_record_words() {
+    return sizeof(S) == 4 ? 32 : 64;
+}
+
 // Where a track writes its records: slot-major arrays, index k * n + t.
 // bound and cov point at the caller's arrays of 6 and 21 component pointers
 // (in a kernel: the launch parameters, so no per-thread copy is made).
+// With stage set, records go instead to a staging area of contiguous
+// records, record k of row `track` at (track * capacity + k) *
+// staged_record_words(): a lane then writes whole cache lines, where the
+// slot-major arrays indexed by the input track would take one sector per
+// field when neighbouring lanes hold unrelated input indices
+// (unstage_records converts them afterwards).
 template <typename S>
 struct record_sink {
     uint64_t* barcode;
@@ -40,8 +53,41 @@ struct record_sink {
     uint64_t track;
     uint32_t capacity;
     uint32_t count;
+    uint32_t* stage;
+
+    DPROP_HD void write_staged(uint64_t bc, const S* b, const S* c, S p,
+                               uint8_t fl) {
+        constexpr int nw = staged_record_words<S>();
+        constexpr int ws = static_cast<int>(sizeof(S) / 4);
+        uint32_t w[nw];
+        memcpy(w, &bc, sizeof(bc));
+        memcpy(w + 2, b, 6 * sizeof(S));
+        memcpy(w + 2 + 6 * ws, c, 21 * sizeof(S));
+        memcpy(w + 2 + 27 * ws, &p, sizeof(S));
+        w[2 + 28 * ws] = fl;
+        for (int i = 3 + 28 * ws; i < nw; ++i) {
+            w[i] = 0u;
+        }
+        uint4* dst = reinterpret_cast<uint4*>(
+            stage + (track * capacity + count) * static_cast<uint64_t>(nw));
+        for (int i = 0; i < nw / 4; ++i) {
+            uint4 v;
+            v.x = w[4 * i];
+            v.y = w[4 * i + 1];
+            v.z = w[4 * i + 2];
+            v.w = w[4 * i + 3];
+            dst[i] = v;
+        }
+    }
 
     DPROP_HD void write(uint64_t bc, const S* b, const S* c, S p, uint8_t fl) {
+        if (stage != nullptr) {
+            if (count < capacity) {
+                write_staged(bc, b, c, p, fl);
+            }
+            ++count;
+            return;
+        }
         if (count < capacity) {
             const uint64_t o = static_cast<uint64_t>(count) * n_tracks + track;
             barcode[o] = bc;
@@ -67,6 +113,41 @@ struct record_sink {
         ++count;
     }
 };
+
+// The `count` staged records of staging row `row` written to the
+// slot-major arrays of `out` as track `track` (out.stage unset): the same
+// writes record_sink::write makes, so the results are those of writing
+// directly.
+template <typename S>
+DPROP_HD void unstage_records(const uint32_t* stage, uint64_t row,
+                              uint32_t count, uint64_t track,
+                              record_sink<S> out) {
+    constexpr int nw = staged_record_words<S>();
+    constexpr int ws = static_cast<int>(sizeof(S) / 4);
+    const uint32_t m = count < out.capacity ? count : out.capacity;
+    out.track = track;
+    out.stage = nullptr;
+    for (uint32_t k = 0; k < m; ++k) {
+        const uint4* src = reinterpret_cast<const uint4*>(
+            stage + (row * out.capacity + k) * static_cast<uint64_t>(nw));
+        uint32_t w[nw];
+        for (int i = 0; i < nw / 4; ++i) {
+            const uint4 v = src[i];
+            w[4 * i] = v.x;
+            w[4 * i + 1] = v.y;
+            w[4 * i + 2] = v.z;
+            w[4 * i + 3] = v.w;
+        }
+        uint64_t bc;
+        S b[6], c[21], p;
+        memcpy(&bc, w, sizeof(bc));
+        memcpy(b, w + 2, 6 * sizeof(S));
+        memcpy(c, w + 2 + 6 * ws, 21 * sizeof(S));
+        memcpy(&p, w + 2 + 27 * ws, sizeof(S));
+        out.count = k;
+        out.write(bc, b, c, p, static_cast<uint8_t>(w[2 + 28 * ws]));
+    }
+}
 
 // All per-track state of one propagation flow; Grad: the transport Jacobian
 // includes the field gradient (use_field_gradient)

@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(k_direct_block)
     rec.n_tracks = n;
     rec.track = t;
     rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
+    rec.stage = nullptr;
     rec.count = 0u;
 
     uint8_t status = DPROP_TRK_NO_SURFACE;

@@ -361,6 +361,8 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     }
     const bool sort = launch_cfg && launch_cfg->sort_tracks;
     const bool persistent = launch_cfg && launch_cfg->method == DPROP_METHOD_PERSISTENT;
+    const uint32_t rec_cap =
+        dprop::api::staged_capacity(make_prop_cfg<float>(c), io);
     if (!(launch_cfg && launch_cfg->use_graph)) {
         launch_scratch scr{};
         if (sort) {
@@ -379,7 +381,8 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
             scr.sort_bytes = need;
         }
         if (persistent) {
-            const size_t need = dprop::api::rounds_scratch_bytes(n, det->wires);
+            const size_t need =
+                dprop::api::rounds_scratch_bytes(n, det->wires, rec_cap);
             if (g_rounds.bytes < need) {
                 if (g_rounds.buf) {
                     DPROP_CUDA(cudaStreamSynchronize(stream));
@@ -427,7 +430,8 @@ dprop_status launch(const dprop_config& c, const dprop_launch* launch_cfg,
     e.key = key;
     const size_t sort_bytes = sort ? sort_scratch_bytes(n) : 0;
     const size_t rounds_bytes =
-        persistent ? dprop::api::rounds_scratch_bytes(n, det->wires) : 0;
+        persistent ? dprop::api::rounds_scratch_bytes(n, det->wires, rec_cap)
+                   : 0;
     // The radix sort's temporary size carries the sort's alignment padding
     // and is usually odd: the persistent method's arrays after it start at
     // the next 256-byte boundary (an atomic on an unaligned word is a device
@@ -731,7 +735,9 @@ dprop_status propagate_host_jagged(const dprop_config& c,
     need += 6 * al256((chunk + 1) * 4) + al256(sort_temp) + al256(scan_temp);
     const bool rounds = lc && lc->method == DPROP_METHOD_PERSISTENT;
     const size_t rounds_bytes =
-        rounds ? al256(dprop::api::rounds_scratch_bytes(chunk, det->wires)) : 0;
+        rounds ? al256(dprop::api::rounds_scratch_bytes(
+                     chunk, det->wires, static_cast<uint32_t>(cap)))
+               : 0;
     need += rounds_bytes;
     for (int k = 0; k < n_slots; ++k) {
         const dprop_status s = ensure_pipe(g_pipe[k], k, need, chunk);

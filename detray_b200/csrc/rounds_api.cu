@@ -193,7 +193,8 @@ __global__ void __launch_bounds__(k_build_threads)
 
 template <typename In>
 __device__ __forceinline__ record_sink<float> make_sink(
-    const api::io_ptrs<In>& io, uint64_t n, const prop_cfg<float>& cfg) {
+    const api::io_ptrs<In>& io, uint64_t n, const prop_cfg<float>& cfg,
+    uint32_t* stage) {
     record_sink<float> rec;
     rec.barcode = io.rec_barcode;
     rec.bound = io.rec_bound;
@@ -204,6 +205,7 @@ __device__ __forceinline__ record_sink<float> make_sink(
     rec.track = 0u;
     rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
     rec.count = 0u;
+    rec.stage = stage;
     return rec;
 }
 
@@ -234,14 +236,16 @@ __device__ __forceinline__ uint32_t pull32(uint32_t* pull) {
 }
 
 // Propagation start of every slot; pads the next-segment array to whole
-// tiles with ended slots.
+// tiles with ended slots.  inv (with staged records) receives the slot of
+// each input track.
 template <typename In, bool W>
 __global__ void __launch_bounds__(k_phase_block)
     rounds_init_kernel(const __grid_constant__ detector_view<float, W> det,
                        const __grid_constant__ prop_cfg<float> cfg,
                        const __grid_constant__ api::io_ptrs<In> io,
                        const __grid_constant__ slot_soa<float> s, uint64_t n,
-                       uint64_t n_pad, const uint32_t* __restrict__ order) {
+                       uint64_t n_pad, const uint32_t* __restrict__ order,
+                       uint32_t* __restrict__ inv) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t slot = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
          slot < n_pad; slot += stride) {
@@ -250,6 +254,9 @@ __global__ void __launch_bounds__(k_phase_block)
             continue;
         }
         const uint64_t t = order ? static_cast<uint64_t>(order[slot]) : slot;
+        if (inv) {
+            inv[t] = static_cast<uint32_t>(slot);
+        }
         const vec3<float> pos{static_cast<float>(io.trk[0][t]),
                               static_cast<float>(io.trk[1][t]),
                               static_cast<float>(io.trk[2][t])};
@@ -275,10 +282,11 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
                        const __grid_constant__ slot_soa<float> s,
                        const uint32_t* __restrict__ queue,
                        const uint32_t* __restrict__ count, uint32_t* pull,
-                       uint64_t n, uint32_t step_budget, uint32_t yield_lanes) {
+                       uint64_t n, uint32_t step_budget, uint32_t yield_lanes,
+                       uint32_t* stage) {
     const uint32_t cnt = *count;
     const unsigned lane = threadIdx.x & 31u;
-    record_sink<float> rec = make_sink(io, n, cfg);
+    record_sink<float> rec = make_sink(io, n, cfg, stage);
     while (true) {
         const uint32_t base = pull32(pull);
         if (base >= cnt) {
@@ -351,9 +359,9 @@ __global__ void __launch_bounds__(k_phase_block, 8)
                        const __grid_constant__ slot_soa<float> s,
                        const uint32_t* __restrict__ queue,
                        const uint32_t* __restrict__ count, uint32_t* pull,
-                       uint64_t n) {
+                       uint64_t n, uint32_t* stage) {
     const uint32_t cnt = *count;
-    record_sink<float> rec = make_sink(io, n, cfg);
+    record_sink<float> rec = make_sink(io, n, cfg, stage);
     while (true) {
         const uint32_t base = pull32(pull);
         if (base >= cnt) {
@@ -367,6 +375,24 @@ __global__ void __launch_bounds__(k_phase_block, 8)
             write_outputs(io, s.track[slot], o);
         }
         __syncwarp();
+    }
+}
+
+// Staged records to the public slot-major arrays, one thread per input
+// track: consecutive threads write consecutive words of every array.
+template <typename In>
+__global__ void __launch_bounds__(k_phase_block)
+    rounds_unstage_kernel(const __grid_constant__ prop_cfg<float> cfg,
+                          const __grid_constant__ api::io_ptrs<In> io,
+                          const uint32_t* __restrict__ rec_count,
+                          const uint32_t* __restrict__ inv,
+                          const uint32_t* __restrict__ stage, uint64_t n) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const record_sink<float> out = make_sink(io, n, cfg, nullptr);
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         t < n; t += stride) {
+        const uint64_t slot = inv[t];
+        unstage_records<float>(stage, slot, rec_count[slot], t, out);
     }
 }
 
@@ -387,13 +413,16 @@ struct rounds_layout {
     slot_soa<float> slots;
     queue_set qs;
     uint64_t n_tiles;
+    uint32_t* inv;    // slot of each input track (staged records only)
+    uint32_t* stage;  // staged records, rec_cap per slot (or null)
 };
 
 size_t al256(size_t b) { return (b + 255u) & ~size_t(255u); }
 
-// Scratch layout: slot arrays, three queues, counters and tile counts.
-size_t rounds_layout_bytes(uint64_t n, bool wires, rounds_layout* out,
-                           void* base) {
+// Scratch layout: slot arrays, three queues, counters and tile counts, and
+// with rec_cap > 0 the record staging area and the input -> slot map.
+size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
+                           rounds_layout* out, void* base) {
     const uint64_t n_tiles = queue_tiles(n);
     slot_soa<float> s{};
     const size_t slot_bytes = carve_slots<float>(base, n, wires, &s);
@@ -409,10 +438,20 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, rounds_layout* out,
     off += 256;
     qs.tiles = reinterpret_cast<uint32_t*>(p + off);
     off += al256(3u * n_tiles * 4u);
+    uint32_t* inv = nullptr;
+    uint32_t* stage = nullptr;
+    if (rec_cap > 0u) {
+        inv = reinterpret_cast<uint32_t*>(p + off);
+        off += al256(n * 4u);
+        stage = reinterpret_cast<uint32_t*>(p + off);
+        off += al256(n * rec_cap * (4u * staged_record_words<float>()));
+    }
     if (out) {
         out->slots = s;
         out->qs = qs;
         out->n_tiles = n_tiles;
+        out->inv = inv;
+        out->stage = stage;
     }
     return off;
 }
@@ -436,7 +475,7 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
         return s;
     }
     rounds_init_kernel<In, W><<<g_init, k_phase_block, 0, st>>>(
-        det, cfg, io, L.slots, n, n_pad, order);
+        det, cfg, io, L.slots, n, n_pad, order, L.inv);
     DPROP_CUDA(cudaGetLastError());
     for (uint32_t r = 0; r <= rounds; ++r) {
         const int merged = (r == rounds) ? 1 : 0;
@@ -448,13 +487,18 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
         if (merged) {
             rounds_tail_kernel<In, W><<<g_tail, k_phase_block, 0, st>>>(
                 det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count,
-                L.qs.pull, n);
+                L.qs.pull, n, L.stage);
             DPROP_CUDA(cudaGetLastError());
+            if (L.stage != nullptr) {
+                rounds_unstage_kernel<In><<<g_init, k_phase_block, 0, st>>>(
+                    cfg, io, L.slots.rec_count, L.inv, L.stage, n);
+                DPROP_CUDA(cudaGetLastError());
+            }
             break;
         }
         rounds_fast_kernel<In, W, FastBlocks><<<g_fast, k_phase_block, 0, st>>>(
             det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count, L.qs.pull, n,
-            step_budget, yield_lanes);
+            step_budget, yield_lanes, L.stage);
         rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
             det, cfg, L.slots, L.qs.q[2], L.qs.count + 2, L.qs.pull + 2);
         DPROP_CUDA(cudaGetLastError());
@@ -470,8 +514,8 @@ constexpr uint32_t k_default_steps_per_round = 16u;
 constexpr uint32_t k_default_rounds = 64u;
 constexpr uint32_t k_default_yield_lanes = 16u;
 
-size_t rounds_scratch_bytes(uint64_t n, bool wires) {
-    return rounds_layout_bytes(n, wires, nullptr, nullptr) + 256u;
+size_t rounds_scratch_bytes(uint64_t n, bool wires, uint32_t rec_cap) {
+    return rounds_layout_bytes(n, wires, rec_cap, nullptr, nullptr) + 256u;
 }
 
 template <typename In>
@@ -488,13 +532,14 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                     "persistent method: use_field_gradient runs with the "
                     "plain method only");
     }
-    if (scratch_bytes < rounds_scratch_bytes(n, det->wires)) {
+    const uint32_t rec_cap = staged_capacity(cfg, io);
+    if (scratch_bytes < rounds_scratch_bytes(n, det->wires, rec_cap)) {
         return fail(DPROP_E_INVALID, "persistent method: scratch too small");
     }
     void* base = reinterpret_cast<void*>(
         (reinterpret_cast<uintptr_t>(scratch) + 255u) & ~uintptr_t(255u));
     rounds_layout L{};
-    rounds_layout_bytes(n, det->wires, &L, base);
+    rounds_layout_bytes(n, det->wires, rec_cap, &L, base);
     const uint32_t rounds = (lc && lc->rounds) ? lc->rounds : k_default_rounds;
     const uint32_t budget = (lc && lc->steps_per_round) ? lc->steps_per_round
                                                         : k_default_steps_per_round;

@@ -94,6 +94,7 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
     rec.n_tracks = n;
     rec.track = t;
     rec.capacity = (io.rec_barcode != nullptr) ? cfg.max_records : 0u;
+    rec.stage = nullptr;
     rec.count = 0u;
 
     uint8_t status;
@@ -125,8 +126,16 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
 // Round-based propagation (rounds_api.cu): device scratch bytes for n
 // tracks, and the enqueue of the whole propagation on a stream (no
 // allocation, no synchronisation; order is the direction-sorted track order
-// or NULL).
-size_t rounds_scratch_bytes(uint64_t n, bool wires);
+// or NULL).  rec_cap: records per track staged in the scratch (0 when no
+// records are requested, see staged_capacity).
+size_t rounds_scratch_bytes(uint64_t n, bool wires, uint32_t rec_cap);
+
+// Records per track the round-based propagation stages in its scratch: the
+// configuration's capacity when the caller asks for records.
+template <typename S, typename In>
+uint32_t staged_capacity(const prop_cfg<S>& cfg, const io_ptrs<In>& io) {
+    return io.rec_barcode != nullptr ? cfg.max_records : 0u;
+}
 
 template <typename In>
 dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,

@@ -289,6 +289,17 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
     rec.flags = rf.data();
     rec.n_tracks = n;
     rec.capacity = cap;
+    // records staged per slot as in the kernels, converted at the end; the
+    // slots hold the tracks in reverse order so that the conversion's
+    // slot -> track mapping is exercised
+    std::vector<uint32_t> stage(static_cast<size_t>(cap) * n *
+                                    staged_record_words<S>() +
+                                4u);
+    uint32_t* stage_base = reinterpret_cast<uint32_t*>(
+        (reinterpret_cast<uintptr_t>(stage.data()) + 15u) & ~uintptr_t(15u));
+    record_sink<S> direct = rec;
+    direct.stage = nullptr;
+    rec.stage = stage_base;
 
     auto emit = [&](const track_outputs<S>& o, uint64_t t) {
         out->status[t] = o.status;
@@ -307,7 +318,7 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
     };
 
     for (uint64_t t = 0; t < n; ++t) {
-        phase_init<S, W>(s, t, static_cast<uint32_t>(t),
+        phase_init<S, W>(s, n - 1u - t, static_cast<uint32_t>(t),
                          vec3<S>{static_cast<S>(trk[0][t]), static_cast<S>(trk[1][t]),
                                  static_cast<S>(trk[2][t])},
                          static_cast<S>(trk[3][t]),
@@ -382,6 +393,10 @@ int run_rounds_w(const detector_view<S, W>& det, uint32_t field_kind,
         for (const uint64_t slot : qn) {
             phase_nav<S, W>(s, slot, det, cfg);
         }
+    }
+    for (uint64_t t = 0; t < n; ++t) {
+        const uint64_t slot = n - 1u - t;
+        unstage_records<S>(stage_base, slot, s.rec_count[slot], t, direct);
     }
     for (uint64_t t = 0; t < n; ++t) {
         const uint32_t m = out->n_records ? (out->n_records[t] < cap ? out->n_records[t] : cap) : 0u;
