@@ -509,6 +509,22 @@ def parity_sample(cfg, host_trk, res, k):
     return out
 
 
+def launch_fields(lc):
+    """The launch shape the autotuner chose, as printed in the line.  A warp
+    always carries 32 tracks, one per lane, in both methods; yield_lanes is
+    the persistent step phase's lower bound of live tracks per warp."""
+    return {"method": {0: "plain", 1: "persistent"}.get(int(lc.method),
+                                                        int(lc.method)),
+            "block_size": int(lc.block_size) or 128,
+            "ctas_per_sm": int(lc.ctas_per_sm),
+            "sort_tracks": int(lc.sort_tracks),
+            "tracks_per_warp": 32,
+            "steps_per_round": int(lc.steps_per_round),
+            "yield_lanes": int(lc.yield_lanes),
+            "rounds": int(lc.rounds),
+            "sort_interval": int(lc.sort_interval)}
+
+
 def config3_row(args, dev, stream, world):
     """Benchmark configuration 3 on every rank: the toy detector in the
     solenoid field map, 4 M muons with pT log-uniform in 0.1-100 GeV, fp32
@@ -548,12 +564,7 @@ def config3_row(args, dev, stream, world):
     return {"workload": "toy_4brl_7edc_solenoid_map_4M_muons_pt0.1-100_eta4",
             "tracks_per_gpu": n3, "ms": {k: round(v, 3) for k, v in ms.items()},
             "tracks_per_s": {k: n3 * world / (v / 1e3) for k, v in ms.items()},
-            "autotuned": {"method": int(lc.method),
-                          "ctas_per_sm": int(lc.ctas_per_sm),
-                          "sort_tracks": int(lc.sort_tracks),
-                          "steps_per_round": int(lc.steps_per_round),
-                          "yield_lanes": int(lc.yield_lanes),
-                          "rounds": int(lc.rounds)},
+            "autotuned": launch_fields(lc),
             "autotune_ms": [round(t, 3) for t in tune],
             "track_status": status.tolist(),
             "persistent_vs_plain": round(ms["plain"] / ms["persistent"], 4)}
@@ -752,11 +763,8 @@ def run_ours(args):
                        "global_batch": total_tracks,
                        "method": {abi.METHOD_PLAIN: "plain",
                                   abi.METHOD_PERSISTENT: "persistent"}[method],
-                       "sort_tracks": int(lc.sort_tracks),
-                       "ctas_per_sm": int(lc.ctas_per_sm),
-                       "steps_per_round": int(lc.steps_per_round),
-                       "yield_lanes": int(lc.yield_lanes),
-                       "rounds": int(lc.rounds),
+                       **{k: v for k, v in launch_fields(lc).items()
+                          if k != "method"},
                        "cuda_graph": int(lc.use_graph),
                        "shard": list(shard_range) if shard_range else None,
                        "autotune_ms": ([round(t, 3) for t in tune_ms]
@@ -1035,9 +1043,7 @@ def run_sweep(args):
                                             for k, v in forms.items()},
                  "tracks_per_s": {k: n3 / (v / 1e3)
                                   for k, v in forms.items()},
-                 "autotuned": {"method": int(lc.method),
-                               "ctas_per_sm": int(lc.ctas_per_sm),
-                               "sort_tracks": int(lc.sort_tracks)},
+                 "autotuned": launch_fields(lc),
                  "dtype": "f32"})
     del res, dt
 

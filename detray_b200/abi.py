@@ -270,7 +270,8 @@ class Launch(C.Structure):
         ("steps_per_round", C.c_uint32),
         ("rounds", C.c_uint32),
         ("yield_lanes", C.c_uint32),
-        ("reserved", C.c_uint32 * 3),
+        ("sort_interval", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 

@@ -76,7 +76,14 @@ struct record_sink {
             v.y = w[4 * i + 1];
             v.z = w[4 * i + 2];
             v.w = w[4 * i + 3];
+#ifdef __CUDA_ARCH__
+            // read once, by the conversion after the propagation: streaming
+            // store, so that the records do not push the detector tables,
+            // the field map and the slot state out of L2
+            __stcs(dst + i, v);
+#else
             dst[i] = v;
+#endif
         }
     }
 
@@ -132,7 +139,11 @@ DPROP_HD void unstage_records(const uint32_t* stage, uint64_t row,
             stage + (row * out.capacity + k) * static_cast<uint64_t>(nw));
         uint32_t w[nw];
         for (int i = 0; i < nw / 4; ++i) {
+#ifdef __CUDA_ARCH__
+            const uint4 v = __ldcs(src + i);
+#else
             const uint4 v = src[i];
+#endif
             w[4 * i] = v.x;
             w[4 * i + 1] = v.y;
             w[4 * i + 2] = v.z;

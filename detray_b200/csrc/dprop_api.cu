@@ -152,6 +152,12 @@ __global__ void direction_key_kernel(const In* __restrict__ dx,
 #define DPROP_MIN_BLOCKS 12
 #endif
 constexpr int k_plain_block = DPROP_BLOCK;
+// Largest CTA a plain launch may use (dprop_launch.block_size): the kernels
+// are compiled for it, with the resident-CTA count scaled so that the
+// register budget is the one of MinBlocks CTAs of k_plain_block threads.
+constexpr int k_plain_max_block = 256;
+static_assert(k_plain_max_block % k_plain_block == 0,
+              "the largest plain CTA is a multiple of the default one");
 
 // One instantiation per register budget: MinBlocks resident CTAs of 128
 // threads per SM -> 8: 64 registers, 12: 40 registers, 16: 32 registers per
@@ -160,7 +166,8 @@ constexpr int k_plain_block = DPROP_BLOCK;
 // on the workload (constant field vs field map), so it is a launch choice.
 template <typename In, int MinBlocks = DPROP_MIN_BLOCKS, bool W = true,
           bool Grad = false>
-__global__ void __launch_bounds__(k_plain_block, MinBlocks)
+__global__ void __launch_bounds__(
+    k_plain_max_block, MinBlocks * k_plain_block / k_plain_max_block)
     propagate_plain_kernel(const __grid_constant__ detector_view<float, W> det,
                            const __grid_constant__ field_view<float> field,
                            const __grid_constant__ prop_cfg<float> cfg,
@@ -250,29 +257,68 @@ namespace {
 // kernel carries the 18 position-column entries of the transport Jacobian;
 // it is built for one register budget (8 CTAs per SM, 64 registers).
 template <typename In, int MB>
-void launch_plain_mb(unsigned int grid, cudaStream_t st,
-                     const dprop_detector* det,
+void launch_plain_mb(int block, cudaStream_t st, const dprop_detector* det,
                      const field_view<float>& field, const prop_cfg<float>& cfg,
                      const io_ptrs<In>& io, uint64_t n, const uint32_t* order) {
+    const unsigned int grid =
+        static_cast<unsigned int>((n + block - 1) / block);
     if (cfg.step.field_gradient) {
         if (det->wires) {
             propagate_plain_kernel<In, 8, true, true>
-                <<<grid, k_plain_block, 0, st>>>(det->view_as<true>(), field,
-                                                 cfg, io, n, order);
+                <<<grid, block, 0, st>>>(det->view_as<true>(), field, cfg, io,
+                                         n, order);
         } else {
             propagate_plain_kernel<In, 8, false, true>
-                <<<grid, k_plain_block, 0, st>>>(det->view_as<false>(), field,
-                                                 cfg, io, n, order);
+                <<<grid, block, 0, st>>>(det->view_as<false>(), field, cfg,
+                                         io, n, order);
         }
         return;
     }
     if (det->wires) {
-        propagate_plain_kernel<In, MB, true><<<grid, k_plain_block, 0, st>>>(
+        propagate_plain_kernel<In, MB, true><<<grid, block, 0, st>>>(
             det->view_as<true>(), field, cfg, io, n, order);
     } else {
-        propagate_plain_kernel<In, MB, false><<<grid, k_plain_block, 0, st>>>(
+        propagate_plain_kernel<In, MB, false><<<grid, block, 0, st>>>(
             det->view_as<false>(), field, cfg, io, n, order);
     }
+}
+
+// Threads per CTA of a plain launch: dprop_launch.block_size, a multiple of
+// 32 up to k_plain_max_block (0: k_plain_block); -1 if invalid.
+int plain_block_of(const dprop_launch* lc) {
+    const uint32_t b = lc ? lc->block_size : 0u;
+    if (b == 0u) {
+        return k_plain_block;
+    }
+    if (b % 32u != 0u || b > static_cast<uint32_t>(k_plain_max_block)) {
+        return -1;
+    }
+    return static_cast<int>(b);
+}
+
+// The plain kernel at the launch's register budget and block size.
+template <typename In>
+dprop_status launch_plain(const dprop_launch* lc, cudaStream_t st,
+                          const dprop_detector* det,
+                          const field_view<float>& field,
+                          const prop_cfg<float>& cfg, const io_ptrs<In>& io,
+                          uint64_t n, const uint32_t* order) {
+    const int block = plain_block_of(lc);
+    if (block < 0) {
+        return fail(DPROP_E_INVALID,
+                    "plain method: block_size must be a multiple of 32 up to "
+                    "256");
+    }
+    const int mb = occupancy_of(lc);
+    if (mb == 8) {
+        launch_plain_mb<In, 8>(block, st, det, field, cfg, io, n, order);
+    } else if (mb == 16) {
+        launch_plain_mb<In, 16>(block, st, det, field, cfg, io, n, order);
+    } else {
+        launch_plain_mb<In, 12>(block, st, det, field, cfg, io, n, order);
+    }
+    DPROP_CUDA(cudaGetLastError());
+    return DPROP_OK;
 }
 
 // Scratch one propagation launch needs besides inputs and outputs.
@@ -295,7 +341,6 @@ dprop_status enqueue_propagation(const dprop_config& c,
                                  const launch_scratch& scr) {
     const prop_cfg<float> cfg = make_prop_cfg<float>(c);
     const uint32_t method = launch_cfg ? launch_cfg->method : DPROP_METHOD_PLAIN;
-    const int mb = occupancy_of(launch_cfg);
     const uint32_t* order = nullptr;
     if (launch_cfg && launch_cfg->sort_tracks) {
         const dprop_status s = dprop::api::enqueue_sort<In>(
@@ -310,19 +355,9 @@ dprop_status enqueue_propagation(const dprop_config& c,
         return dprop::api::enqueue_rounds<In>(launch_cfg, det, field, cfg, io,
                                               n, order, scr.rounds,
                                               scr.rounds_bytes, stream);
-    } else {
-        const unsigned int g =
-            static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
-        if (mb == 8) {
-            launch_plain_mb<In, 8>(g, stream, det, field->view, cfg, io, n, order);
-        } else if (mb == 12) {
-            launch_plain_mb<In, 12>(g, stream, det, field->view, cfg, io, n, order);
-        } else {
-            launch_plain_mb<In, 16>(g, stream, det, field->view, cfg, io, n, order);
-        }
     }
-    DPROP_CUDA(cudaGetLastError());
-    return DPROP_OK;
+    return launch_plain<In>(launch_cfg, stream, det, field->view, cfg, io, n,
+                            order);
 }
 
 // ------------------------------------------------------------ CUDA graphs
@@ -842,19 +877,10 @@ dprop_status propagate_host_jagged(const dprop_config& c,
                 rounds_scratch(sl), rounds_bytes, st);
             if (s != DPROP_OK) return s;
         } else {
-            const unsigned int grid = static_cast<unsigned int>(
-                (m + k_plain_block - 1) / k_plain_block);
-            const int mb = occupancy_of(lc);
-            if (mb == 8) {
-                launch_plain_mb<double, 8>(grid, st, det, field->view, pcfg,
-                                           io, m, sort ? b.idx_out : nullptr);
-            } else if (mb == 16) {
-                launch_plain_mb<double, 16>(grid, st, det, field->view, pcfg,
-                                            io, m, sort ? b.idx_out : nullptr);
-            } else {
-                launch_plain_mb<double, 12>(grid, st, det, field->view, pcfg,
-                                            io, m, sort ? b.idx_out : nullptr);
-            }
+            const dprop_status s = launch_plain<double>(
+                lc, st, det, field->view, pcfg, io, m,
+                sort ? b.idx_out : nullptr);
+            if (s != DPROP_OK) return s;
         }
         DPROP_CUDA(cudaGetLastError());
         // pack the records
@@ -1108,23 +1134,27 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
     r.rec_flags = reinterpret_cast<uint8_t*>(take(cap * m));
     const io_ptrs<float> io = make_io<float>(*tracks, r);
 
-    // plain: register budget (resident CTAs per SM) x direction sort;
-    // persistent: step-phase register budget x steps per round x tracks per
-    // warp (yield lanes) x rounds x direction sort
+    // plain: register budget (resident CTAs per SM) x block size x
+    // direction sort; persistent: step-phase register budget x steps per
+    // round x tracks per warp (yield lanes) x rounds x volume re-sort
+    // interval x direction sort
     struct cand {
-        uint32_t method, ctas, sort, steps, yield, rounds;
+        uint32_t method, block, ctas, sort, steps, yield, rounds, interval;
     };
     const cand cands[DPROP_AUTOTUNE_CANDIDATES] = {
-        {DPROP_METHOD_PLAIN, 8, 1, 0, 0, 0},
-        {DPROP_METHOD_PLAIN, 12, 1, 0, 0, 0},
-        {DPROP_METHOD_PLAIN, 16, 1, 0, 0, 0},
-        {DPROP_METHOD_PLAIN, 16, 0, 0, 0, 0},
-        {DPROP_METHOD_PERSISTENT, 3, 1, 16, 16, 64},
-        {DPROP_METHOD_PERSISTENT, 4, 1, 16, 16, 64},
-        {DPROP_METHOD_PERSISTENT, 5, 1, 16, 16, 64},
-        {DPROP_METHOD_PERSISTENT, 4, 1, 16, 8, 96},
-        {DPROP_METHOD_PERSISTENT, 4, 1, 64, 12, 64},
-        {DPROP_METHOD_PERSISTENT, 4, 0, 16, 16, 64}};
+        {DPROP_METHOD_PLAIN, 128, 8, 1, 0, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 128, 12, 1, 0, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 128, 16, 1, 0, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 256, 16, 1, 0, 0, 0, 0},
+        {DPROP_METHOD_PLAIN, 128, 16, 0, 0, 0, 0, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 3, 1, 16, 16, 64, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 3, 1, 16, 16, 64, 1},
+        {DPROP_METHOD_PERSISTENT, 128, 4, 1, 16, 16, 64, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 4, 1, 16, 16, 64, 2},
+        {DPROP_METHOD_PERSISTENT, 128, 5, 1, 16, 16, 64, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 4, 1, 16, 8, 96, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 4, 1, 64, 12, 64, 0},
+        {DPROP_METHOD_PERSISTENT, 128, 4, 0, 16, 16, 64, 0}};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1134,6 +1164,8 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
         dprop_launch lc{};
         lc.use_graph = launch_out->use_graph;
         lc.method = cands[i].method;
+        lc.block_size = cands[i].block;
+        lc.sort_interval = cands[i].interval;
         lc.ctas_per_sm = cands[i].ctas;
         lc.sort_tracks = cands[i].sort;
         lc.steps_per_round = cands[i].steps;
@@ -1167,6 +1199,8 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
         return s;
     }
     launch_out->method = cands[best_i].method;
+    launch_out->block_size = cands[best_i].block;
+    launch_out->sort_interval = cands[best_i].interval;
     launch_out->ctas_per_sm = cands[best_i].ctas;
     launch_out->sort_tracks = cands[best_i].sort;
     launch_out->steps_per_round = cands[best_i].steps;
@@ -1550,10 +1584,9 @@ extern "C" dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
     DPROP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, order,
                                                ni, 0, 20, stream));
     const prop_cfg<float> pc = make_prop_cfg<float>(*cfg);
-    const unsigned int grid =
-        static_cast<unsigned int>((n + k_plain_block - 1) / k_plain_block);
-    launch_plain_mb<float, DPROP_MIN_BLOCKS>(grid, stream, det, field->view, pc,
-                                             io, n, order.Current());
+    launch_plain_mb<float, DPROP_MIN_BLOCKS>(k_plain_block, stream, det,
+                                             field->view, pc, io, n,
+                                             order.Current());
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;
 }

@@ -25,6 +25,13 @@
 //       navigation (grid and portal search), with all lanes of a warp doing
 //       it at once.
 //
+// Every sort_interval rounds (dprop_launch.sort_interval, 0: never) both
+// queues are re-sorted by volume before the phases run (queue_key_kernel +
+// a stable 8-bit radix sort): the step phase by the volume a track is in,
+// the navigation phase by the volume it enters, so that the lanes of a warp
+// intersect the same kinds of surfaces and walk the same grids and portal
+// lists.  Inside a volume the slot (direction) order stays.
+//
 // Each phase kernel is persistent: a grid of the SMs' resident CTAs whose
 // warps pull 32 queue entries at a time from a device counter until the
 // queue is empty.  After `rounds` rounds, rounds_tail_kernel runs the tracks
@@ -34,6 +41,7 @@
 #include <cuda_runtime.h>
 
 #include <cub/block/block_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <type_traits>
 
@@ -85,6 +93,40 @@ __device__ __forceinline__ void unpack16(uint4 v, uint32_t* b) {
         for (int j = 0; j < 4; ++j) {
             b[4 * i + j] = (w[i] >> (8 * j)) & 0xffu;
         }
+    }
+}
+
+// Sort key of each queue entry: the volume the track's next phase works in
+// (for a track on a portal in the navigation queue, the volume the portal
+// leads to), 0xff past the queue's end.
+__global__ void __launch_bounds__(k_build_threads)
+    queue_key_kernel(const uint32_t* __restrict__ q,
+                     const uint32_t* __restrict__ count,
+                     const __grid_constant__ slot_soa<float> s,
+                     uint8_t* __restrict__ keys, uint64_t n, int nav_queue) {
+    const uint32_t cnt = *count;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         i < n; i += stride) {
+        if (i >= cnt) {
+            keys[i] = 0xffu;
+            continue;
+        }
+        const uint64_t slot = q[i];
+        uint32_t vol = s.volume[slot];
+        if (nav_queue) {
+            const uint32_t nb = s.nav_bytes[slot];
+            const int next = static_cast<int>(nb & 0xffu);
+            const int8_t status = static_cast<int8_t>((nb >> 16) & 0xffu);
+            if (status == e_on_portal && next >= 1 && next <= k_cache + 1) {
+                candidate<float> c;
+                load_cand(s, slot, next - 1, c);
+                if (c.volume_link != static_cast<uint16_t>(k_invalid_link)) {
+                    vol = c.volume_link;
+                }
+            }
+        }
+        keys[i] = static_cast<uint8_t>(vol % 255u);
     }
 }
 
@@ -413,6 +455,11 @@ struct rounds_layout {
     slot_soa<float> slots;
     queue_set qs;
     uint64_t n_tiles;
+    uint8_t* keys[2];        // volume re-sort: keys in, keys out
+    uint32_t* nav_sorted;    // the navigation queue re-sorted (the step
+                             // queue goes to the unused queue 1)
+    void* sort_temp;
+    size_t sort_temp_bytes;
     uint32_t* inv;    // slot of each input track (staged records only)
     uint32_t* stage;  // staged records, rec_cap per slot (or null)
 };
@@ -438,6 +485,20 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
     off += 256;
     qs.tiles = reinterpret_cast<uint32_t*>(p + off);
     off += al256(3u * n_tiles * 4u);
+    uint8_t* keys[2];
+    for (int k = 0; k < 2; ++k) {
+        keys[k] = reinterpret_cast<uint8_t*>(p + off);
+        off += al256(n);
+    }
+    uint32_t* nav_sorted = reinterpret_cast<uint32_t*>(p + off);
+    off += al256(n * 4u);
+    size_t temp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, static_cast<const uint8_t*>(nullptr),
+        static_cast<uint8_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+        static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 8);
+    void* sort_temp = p + off;
+    off += al256(temp_bytes);
     uint32_t* inv = nullptr;
     uint32_t* stage = nullptr;
     if (rec_cap > 0u) {
@@ -452,6 +513,11 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
         out->n_tiles = n_tiles;
         out->inv = inv;
         out->stage = stage;
+        out->keys[0] = keys[0];
+        out->keys[1] = keys[1];
+        out->nav_sorted = nav_sorted;
+        out->sort_temp = sort_temp;
+        out->sort_temp_bytes = temp_bytes;
     }
     return off;
 }
@@ -463,7 +529,8 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                               const api::io_ptrs<In>& io, uint64_t n,
                               const uint32_t* order, const rounds_layout& L,
                               uint32_t rounds, uint32_t step_budget,
-                              uint32_t yield_lanes, cudaStream_t st) {
+                              uint32_t yield_lanes, uint32_t sort_interval,
+                              cudaStream_t st) {
     const uint64_t n_pad = L.n_tiles * k_queue_tile;
     const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
     unsigned int g_init = 0, g_fast = 0, g_nav = 0, g_tail = 0;
@@ -496,11 +563,30 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
             }
             break;
         }
+        const uint32_t* q_fast = L.qs.q[0];
+        const uint32_t* q_nav = L.qs.q[2];
+        if (sort_interval > 0u && r > 0u && r % sort_interval == 0u) {
+            const unsigned int kg = static_cast<unsigned int>(
+                (n + k_build_threads - 1) / k_build_threads);
+            for (int k = 0; k < 2; ++k) {
+                const int qi = 2 * k;  // step queue 0, navigation queue 2
+                uint32_t* dst = k == 0 ? L.qs.q[1] : L.nav_sorted;
+                queue_key_kernel<<<kg, k_build_threads, 0, st>>>(
+                    L.qs.q[qi], L.qs.count + qi, L.slots, L.keys[0], n, k);
+                DPROP_CUDA(cudaGetLastError());
+                size_t tb = L.sort_temp_bytes;
+                DPROP_CUDA(cub::DeviceRadixSort::SortPairs(
+                    L.sort_temp, tb, L.keys[0], L.keys[1], L.qs.q[qi], dst,
+                    static_cast<int>(n), 0, 8, st));
+            }
+            q_fast = L.qs.q[1];
+            q_nav = L.nav_sorted;
+        }
         rounds_fast_kernel<In, W, FastBlocks><<<g_fast, k_phase_block, 0, st>>>(
-            det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count, L.qs.pull, n,
+            det, field, cfg, io, L.slots, q_fast, L.qs.count, L.qs.pull, n,
             step_budget, yield_lanes, L.stage);
         rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
-            det, cfg, L.slots, L.qs.q[2], L.qs.count + 2, L.qs.pull + 2);
+            det, cfg, L.slots, q_nav, L.qs.count + 2, L.qs.pull + 2);
         DPROP_CUDA(cudaGetLastError());
     }
     return DPROP_OK;
@@ -524,7 +610,7 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                             const prop_cfg<float>& cfg, const io_ptrs<In>& io,
                             uint64_t n, const uint32_t* order, void* scratch,
                             size_t scratch_bytes, cudaStream_t stream) {
-    if (n > 0xffffff00ull) {
+    if (n > 0x7fffffffull) {
         return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
     }
     if (cfg.step.field_gradient) {
@@ -545,9 +631,14 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                                                         : k_default_steps_per_round;
     const uint32_t yield = (lc && lc->yield_lanes) ? lc->yield_lanes
                                                    : k_default_yield_lanes;
+    const uint32_t sort_interval = lc ? lc->sort_interval : 0u;
     if (rounds > 100000u || yield > 32u) {
         return fail(DPROP_E_INVALID,
                     "persistent method: rounds > 100000 or yield_lanes > 32");
+    }
+    if (lc && lc->block_size != 0u && lc->block_size != k_phase_block) {
+        return fail(DPROP_E_INVALID,
+                    "persistent method: block_size must be 0 or 128");
     }
     // register budget of the step phase: resident CTAs per SM 3, 4 or 5
     const uint32_t fb = (lc && lc->ctas_per_sm) ? lc->ctas_per_sm : 4u;
@@ -561,12 +652,12 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
             return enqueue_rounds_w<In, true, FB>(det->view_as<true>(),
                                                   field->view, cfg, io, n,
                                                   order, L, rounds, budget,
-                                                  yield, stream);
+                                                  yield, sort_interval, stream);
         }
         return enqueue_rounds_w<In, false, FB>(det->view_as<false>(),
                                                field->view, cfg, io, n, order,
                                                L, rounds, budget, yield,
-                                               stream);
+                                               sort_interval, stream);
     };
     if (fb == 3u) {
         return go(std::integral_constant<int, 3>{});

@@ -59,6 +59,20 @@ def read_raw_tables(path) -> dict:
     return out
 
 
+def write_raw_tables(tables: dict, path) -> None:
+    """Write tables (as load_geometry returns them) to a raw table file, the
+    form read_raw_tables and the C++ dprop::read_raw_tables read."""
+    header = np.zeros(12, np.uint32)
+    header[0] = 0x4F454744
+    header[1] = abi.DPROP_ABI_VERSION
+    parts = []
+    for i, (name, ctype) in enumerate(TABLES):
+        arr = np.ascontiguousarray(tables[name], dtype=dtype_of(ctype))
+        header[2 + i] = arr.shape[0]
+        parts.append(arr.tobytes())
+    Path(path).write_bytes(header.tobytes() + b"".join(parts))
+
+
 def save_npz(tables: dict, path) -> None:
     np.savez_compressed(path, **{k: tables[k] for k, _ in TABLES})
 

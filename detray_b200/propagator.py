@@ -184,11 +184,11 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
                 ctas_per_sm: int = 0, sort_tracks: int = 0,
                 use_graph: int = 0, precision: int = 0,
                 steps_per_round: int = 0, rounds: int = 0,
-                yield_lanes: int = 0) -> abi.Launch:
+                yield_lanes: int = 0, sort_interval: int = 0) -> abi.Launch:
     """Launch shape; ``precision`` 8 runs the propagation in fp64 end to end
-    (double track tensors and results).  steps_per_round, rounds and
-    yield_lanes shape the persistent (round-based) method; 0 picks the
-    library default."""
+    (double track tensors and results).  steps_per_round, rounds,
+    yield_lanes and sort_interval shape the persistent (round-based) method;
+    0 picks the library default (sort_interval 0: no re-sort by volume)."""
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
@@ -199,6 +199,7 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
     lc.steps_per_round = steps_per_round
     lc.rounds = rounds
     lc.yield_lanes = yield_lanes
+    lc.sort_interval = sort_interval
     return lc
 
 
@@ -525,14 +526,21 @@ def propagate_host(cfg: abi.Config, det: Detector, field: Field,
     return res
 
 
-# the candidates dprop_autotune times, in its order:
-# (method, ctas_per_sm, sort_tracks, steps_per_round, yield_lanes, rounds)
+# the candidates dprop_autotune times, in its order: (method, block_size,
+# ctas_per_sm, sort_tracks, steps_per_round, yield_lanes, rounds,
+# sort_interval)
 AUTOTUNE_CANDIDATES = [
-    ("plain", 8, 1, 0, 0, 0), ("plain", 12, 1, 0, 0, 0),
-    ("plain", 16, 1, 0, 0, 0), ("plain", 16, 0, 0, 0, 0),
-    ("persistent", 3, 1, 16, 16, 64), ("persistent", 4, 1, 16, 16, 64),
-    ("persistent", 5, 1, 16, 16, 64), ("persistent", 4, 1, 16, 8, 96),
-    ("persistent", 4, 1, 64, 12, 64), ("persistent", 4, 0, 16, 16, 64)]
+    ("plain", 128, 8, 1, 0, 0, 0, 0), ("plain", 128, 12, 1, 0, 0, 0, 0),
+    ("plain", 128, 16, 1, 0, 0, 0, 0), ("plain", 256, 16, 1, 0, 0, 0, 0),
+    ("plain", 128, 16, 0, 0, 0, 0, 0),
+    ("persistent", 128, 3, 1, 16, 16, 64, 0),
+    ("persistent", 128, 3, 1, 16, 16, 64, 1),
+    ("persistent", 128, 4, 1, 16, 16, 64, 0),
+    ("persistent", 128, 4, 1, 16, 16, 64, 2),
+    ("persistent", 128, 5, 1, 16, 16, 64, 0),
+    ("persistent", 128, 4, 1, 16, 8, 96, 0),
+    ("persistent", 128, 4, 1, 64, 12, 64, 0),
+    ("persistent", 128, 4, 0, 16, 16, 64, 0)]
 
 
 def autotune(cfg: abi.Config, det: Detector, field: Field, tracks,

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "detray_b200/dprop.h"
+#include "detray_b200/flat_tables.hpp"
 
 #include <cstdint>
 #include <cstdio>
@@ -27,40 +28,6 @@
 #include <vector>
 
 namespace dprop {
-
-/// Owning flat tables; desc() hands out a view valid while *this lives.
-struct flat_detector {
-    std::vector<dprop_volume_desc> volumes;
-    std::vector<dprop_surface_desc> surfaces;
-    std::vector<dprop_mask_desc> masks;
-    std::vector<dprop_transform_desc> transforms;
-    std::vector<dprop_slab_desc> slabs;
-    std::vector<uint32_t> bf_surfaces;
-    std::vector<dprop_grid_desc> grids;
-    std::vector<uint32_t> grid_bins;
-
-    dprop_detector_desc desc() const {
-        dprop_detector_desc d{};
-        d.abi_version = DPROP_ABI_VERSION;
-        d.n_volumes = static_cast<uint32_t>(volumes.size());
-        d.n_surfaces = static_cast<uint32_t>(surfaces.size());
-        d.n_masks = static_cast<uint32_t>(masks.size());
-        d.n_transforms = static_cast<uint32_t>(transforms.size());
-        d.n_slabs = static_cast<uint32_t>(slabs.size());
-        d.n_bf_surfaces = static_cast<uint32_t>(bf_surfaces.size());
-        d.n_grids = static_cast<uint32_t>(grids.size());
-        d.n_grid_bins = static_cast<uint32_t>(grid_bins.size());
-        d.volumes = volumes.data();
-        d.surfaces = surfaces.data();
-        d.masks = masks.data();
-        d.transforms = transforms.data();
-        d.slabs = slabs.data();
-        d.bf_surfaces = bf_surfaces.data();
-        d.grids = grids.data();
-        d.grid_bins = grid_bins.data();
-        return d;
-    }
-};
 
 namespace adapter_detail {
 
@@ -371,46 +338,6 @@ dprop_transform_desc copy_transform(const transform_t& trf) {
 }
 
 }  // namespace adapter_detail
-
-/// Write the flat tables to a raw table file: a 12-word u32 header ("DGEO",
-/// DPROP_ABI_VERSION, the eight table lengths, two zero words) followed by
-/// the tables in declaration order of dprop_detector_desc.  Returns 0 on
-/// success.
-inline int write_raw_tables(const flat_detector& t, const char* path) {
-    std::FILE* f = std::fopen(path, "wb");
-    if (!f) {
-        return 1;
-    }
-    const uint32_t header[12] = {0x4f454744u,
-                                 DPROP_ABI_VERSION,
-                                 static_cast<uint32_t>(t.volumes.size()),
-                                 static_cast<uint32_t>(t.surfaces.size()),
-                                 static_cast<uint32_t>(t.masks.size()),
-                                 static_cast<uint32_t>(t.transforms.size()),
-                                 static_cast<uint32_t>(t.slabs.size()),
-                                 static_cast<uint32_t>(t.bf_surfaces.size()),
-                                 static_cast<uint32_t>(t.grids.size()),
-                                 static_cast<uint32_t>(t.grid_bins.size()),
-                                 0u,
-                                 0u};
-    bool ok = std::fwrite(header, sizeof(uint32_t), 12, f) == 12u;
-    auto put = [&](const auto& v) {
-        if (!v.empty()) {
-            ok = ok && std::fwrite(v.data(), sizeof(v[0]), v.size(), f) ==
-                           v.size();
-        }
-    };
-    put(t.volumes);
-    put(t.surfaces);
-    put(t.masks);
-    put(t.transforms);
-    put(t.slabs);
-    put(t.bf_surfaces);
-    put(t.grids);
-    put(t.grid_bins);
-    ok = (std::fclose(f) == 0) && ok;
-    return ok ? 0 : 1;
-}
 
 /// Flatten a host detray detector into the tables of the C ABI.
 template <typename detector_t>

@@ -73,7 +73,7 @@ typedef enum dprop_track_status {
  * All indices are 0-based positions in the arrays below.  Tables are given
  * in double precision on the host; the library stores its own device copy. */
 
-/* Mask shapes on the path (geometry/shapes/*.hpp). */
+/* Mask shapes on the path (the headers of geometry/shapes). */
 typedef enum dprop_shape {
     DPROP_SHAPE_RECTANGLE = 0,     /* rectangle2D: v0 half_x, v1 half_y                 */
     DPROP_SHAPE_TRAPEZOID = 1,     /* trapezoid2D: v0 hl_x(-y), v1 hl_x(+y), v2 hl_y, v3 1/(2 hl_y) */
@@ -321,7 +321,10 @@ typedef enum dprop_method {
 
 typedef struct dprop_launch {
     uint32_t method;             /* dprop_method                               */
-    uint32_t block_size;         /* threads per CTA (0: default)               */
+    uint32_t block_size;         /* threads per CTA.  Plain method: a multiple
+                                    of 32 up to 256, 0 = 128 (the register
+                                    budget stays the one ctas_per_sm names).
+                                    Persistent method: 0 or 128                */
     uint32_t ctas_per_sm;        /* register budget: resident CTAs of 128
                                     threads per SM the kernel is compiled for.
                                     Plain method: 8 (64 registers), 12 (40)
@@ -351,7 +354,10 @@ typedef struct dprop_launch {
     uint32_t yield_lanes;        /* tracks per warp: a warp of the step phase
                                     ends its round once fewer than this many of
                                     its 32 lanes can still step (default 16)   */
-    uint32_t reserved[3];
+    uint32_t sort_interval;      /* re-sort the live tracks of both phases by
+                                    volume every sort_interval rounds (0:
+                                    never, the default)                       */
+    uint32_t reserved[2];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */
@@ -551,18 +557,19 @@ dprop_status dprop_propagate_noalloc(const dprop_config* cfg,
                                      uint64_t n_tracks, void* stream);
 
 /* Autotuner: times candidate launch forms - the plain kernel at the three
- * register budgets (ctas_per_sm 8, 12, 16) with the direction sort and at 16
- * without it; the persistent method with and without the sort over its
- * step-phase register budget (ctas_per_sm 3, 4, 5), steps per round, tracks
- * per warp (yield_lanes 8, 12, 16) and the number of rounds before the tail
- * kernel - on the first min(n_tracks, 1048576) of the given
+ * register budgets (ctas_per_sm 8, 12, 16) with the direction sort, at 16
+ * with 256-thread blocks and at 16 without the sort; the persistent method
+ * with and without the sort over its step-phase register budget
+ * (ctas_per_sm 3, 4, 5), steps per round, tracks per warp (yield_lanes 8,
+ * 12, 16), the volume re-sort interval (0, 1, 2) and the number of rounds
+ * before the tail kernel - on the first min(n_tracks, 1048576) of the given
  * device tracks (under a CUDA graph if launch->use_graph is set), and writes
- * the fastest into *launch (method, ctas_per_sm,
- * sort_tracks, steps_per_round, yield_lanes, rounds; use_graph is left as
+ * the fastest into *launch (method, block_size, ctas_per_sm, sort_tracks,
+ * steps_per_round, yield_lanes, rounds, sort_interval; use_graph is left as
  * given).  If timings_ms is not NULL it receives one time per candidate
  * (DPROP_AUTOTUNE_CANDIDATES entries).  Allocates temporary device result
  * buffers for the trial runs. */
-#define DPROP_AUTOTUNE_CANDIDATES 10
+#define DPROP_AUTOTUNE_CANDIDATES 13
 dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
                             const dprop_field* field,
                             const dprop_tracks* tracks, uint64_t n_tracks,

@@ -304,10 +304,59 @@ def test_graph_replay_and_autotune(torch_cuda):
     assert lc.method in (abi.METHOD_PLAIN, abi.METHOD_PERSISTENT)
     if lc.method == abi.METHOD_PLAIN:
         assert lc.ctas_per_sm in (8, 12, 16)
+        assert lc.block_size in (128, 256)
     else:
         assert lc.ctas_per_sm in (3, 4, 5)
         assert lc.yield_lanes in (8, 12, 16) and lc.rounds > 0
+        assert lc.sort_interval in (0, 1, 2)
+    chosen = ({0: "plain", 1: "persistent"}[lc.method], lc.block_size,
+              lc.ctas_per_sm, lc.sort_tracks, lc.steps_per_round,
+              lc.yield_lanes, lc.rounds, lc.sort_interval)
+    assert chosen in propagator.AUTOTUNE_CANDIDATES
+    assert len(times) == len(propagator.AUTOTUNE_CANDIDATES)
     assert all(t > 0 for t in times)
+
+
+def test_launch_shape_does_not_change_results(torch_cuda):
+    """Block size (plain) and the volume re-sort interval (persistent) only
+    reorder the work: every output is bit-identical to the default launch
+    of the same method, under a graph and without."""
+    from detray_b200 import abi, fields, propagator
+    det, _, cfg, trk = _setup("toy")
+    field = propagator.Field.grid(fields.solenoid_map())
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+
+    def run(**kw):
+        res = propagator.propagate(cfg, det, field, dev,
+                                   launch=propagator.make_launch(**kw))
+        torch_cuda.cuda.synchronize()
+        return {k: v.cpu().numpy() for k, v in res.tensors.items()}
+
+    def same(a, b):
+        for k in a:
+            assert np.array_equal(a[k], b[k], equal_nan=True), k
+
+    base = run(method=abi.METHOD_PLAIN, sort_tracks=1, ctas_per_sm=16)
+    for blk in (32, 64, 96, 256):
+        same(base, run(method=abi.METHOD_PLAIN, sort_tracks=1,
+                       ctas_per_sm=16, block_size=blk))
+    base = run(method=abi.METHOD_PERSISTENT, sort_tracks=1, ctas_per_sm=4)
+    for si, graph in ((1, 0), (2, 1), (3, 0), (1, 1)):
+        same(base, run(method=abi.METHOD_PERSISTENT, sort_tracks=1,
+                       ctas_per_sm=4, sort_interval=si, use_graph=graph,
+                       steps_per_round=4))
+    # wire surfaces (the exact-cycle search state travels with the slots)
+    det, field, cfg, trk = _setup("wire_chamber_10l_cells")
+    dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
+    base = run(method=abi.METHOD_PERSISTENT, sort_tracks=1, ctas_per_sm=3)
+    same(base, run(method=abi.METHOD_PERSISTENT, sort_tracks=1,
+                   ctas_per_sm=3, sort_interval=1))
+    with pytest.raises(propagator.PropagationError):
+        run(method=abi.METHOD_PLAIN, block_size=48)
+    with pytest.raises(propagator.PropagationError):
+        run(method=abi.METHOD_PLAIN, block_size=512)
+    with pytest.raises(propagator.PropagationError):
+        run(method=abi.METHOD_PERSISTENT, block_size=256)
 
 
 @pytest.mark.parametrize("kind", ["toy", "toy_maps", "wire_chamber_10l_cells"])
