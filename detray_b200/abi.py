@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-DPROP_ABI_VERSION = 2
+DPROP_ABI_VERSION = 3
 DPROP_INVALID_INDEX = 0xFFFFFFFF
 DPROP_INVALID_LINK = 0xFFFF
 
@@ -135,6 +135,7 @@ class VolumeDesc(C.Structure):
         ("bf_begin", C.c_uint32),
         ("bf_end", C.c_uint32),
         ("grid", C.c_uint32),
+        ("material", C.c_uint32),
     ]
 
 

@@ -103,9 +103,13 @@ def build_core_host(force: bool = False, stepped: bool = False) -> Path:
     return out
 
 
-def build_oracle(ref: Path | None = None) -> bool:
-    """Compile the reference oracle if the reference checkout exists."""
-    ref = ref or Path(os.environ.get("DETRAY_REF", "/root/reference"))
+def build_oracle(ref: Path | str | None = None) -> bool:
+    """Compile the reference oracle from the reference checkout at ``ref``
+    (or $DETRAY_REF); does nothing if neither names a checkout."""
+    ref = ref or os.environ.get("DETRAY_REF")
+    if not ref:
+        return False
+    ref = Path(ref)
     if not (ref / "core" / "include" / "detray").exists():
         return False
     subprocess.run(["make", "-C", str(REPO / "oracle" / "ref"), f"REF={ref}"],
@@ -117,8 +121,9 @@ def main(argv=None) -> None:
     argv = sys.argv[1:] if argv is None else argv
     build_library(force="--force" in argv, verbose="-v" in argv)
     build_core_host(force="--force" in argv)
+    refs = [a.split("=", 1)[1] for a in argv if a.startswith("--ref=")]
     if "--no-oracle" not in argv:
-        build_oracle()
+        build_oracle(refs[0] if refs else None)
 
 
 if __name__ == "__main__":

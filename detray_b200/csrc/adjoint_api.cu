@@ -140,10 +140,11 @@ dprop_status dprop_propagate_adjoint(const dprop_config* cfg,
     if (!cfg || !det || !field || !tracks || !results || !tape) {
         return fail(DPROP_E_INVALID, "propagate_adjoint: NULL argument");
     }
-    if (cfg->use_eloss_gradient) {
+    if (cfg->use_eloss_gradient || det->vol_material != nullptr) {
         return fail(DPROP_E_UNSUPPORTED,
-                    "propagate_adjoint: use_eloss_gradient needs volume "
-                    "material, which the device path does not support");
+                    "propagate_adjoint: the adjoint has no energy-loss term "
+                    "for volume material (use_eloss_gradient, detectors with "
+                    "volume material)");
     }
     if (cfg->max_iterations == 0u || cfg->max_records == 0u) {
         return fail(DPROP_E_INVALID,

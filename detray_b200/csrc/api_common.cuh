@@ -58,15 +58,16 @@ struct dprop_detector {
     uint32_t* bf_surfaces{nullptr};
     dprop::dev_grid<float>* grids{nullptr};
     uint32_t* grid_bins{nullptr};
+    uint32_t* vol_material{nullptr};  // NULL: no volume carries material
     // double-precision copies of the floating-point tables (fp64 launches)
     dprop::dev_mask<double>* masks_d{nullptr};
     dprop::dev_transform<double>* transforms_d{nullptr};
     dprop::dev_slab<double>* slabs_d{nullptr};
     dprop::dev_grid<double>* grids_d{nullptr};
     uint32_t n_volumes{0}, n_surfaces{0};
-    // the detector holds line surfaces, material rods, multi-entry grid bins
-    // or material maps: launches use the kernels that include the code for
-    // them
+    // the detector holds line surfaces, material rods, multi-entry grid bins,
+    // material maps or volume material: launches use the kernels that
+    // include the code for them
     bool wires{false};
     dprop::detector_view<double> view_d() const {
         dprop::detector_view<double> v;
@@ -78,6 +79,7 @@ struct dprop_detector {
         v.bf_surfaces = bf_surfaces;
         v.grids = grids_d;
         v.grid_bins = grid_bins;
+        v.vol_material = vol_material;
         v.n_volumes = n_volumes;
         v.n_surfaces = n_surfaces;
         return v;
@@ -94,6 +96,7 @@ struct dprop_detector {
         v.bf_surfaces = bf_surfaces;
         v.grids = grids;
         v.grid_bins = grid_bins;
+        v.vol_material = vol_material;
         v.n_volumes = n_volumes;
         v.n_surfaces = n_surfaces;
         return v;

@@ -445,99 +445,6 @@ DPROP_HD void transport_covariance(const S G[4][5], S cov[21]) {
     // rows 4 and 5 (q/p, time) unchanged
 }
 
-// --------------------------------------------------- material physics
-template <typename S>
-struct rel_quantities {
-    S qop, q2_over_beta2, beta2, beta_gamma, gamma, gamma2, E, Wmax;
-};
-
-template <typename S>
-DPROP_HD rel_quantities<S> make_rq(S mass, S qop, S q) {
-    rel_quantities<S> rq;
-    rq.qop = qop;
-    rq.q2_over_beta2 = q * q + (mass * qop) * (mass * qop);
-    const S m_over_p = mass * ((q != S(0)) ? fabs(qop / q) : fabs(qop));
-    const S p_over_m = S(1) / m_over_p;
-    rq.beta2 = S(1) / (S(1) + m_over_p * m_over_p);
-    rq.beta_gamma = p_over_m;
-    rq.gamma = sqrt(S(1) + p_over_m * p_over_m);
-    rq.gamma2 = rq.gamma * rq.gamma;
-    rq.E = rq.gamma * mass;
-    const S me = static_cast<S>(constant::m_e);
-    const S mfrac = me / mass;
-    rq.Wmax = (S(2) * me * rq.beta_gamma * rq.beta_gamma) /
-              (S(1) + S(2) * rq.gamma * mfrac + mfrac * mfrac);
-    return rq;
-}
-
-template <typename S>
-DPROP_HD S eps_per_length(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
-    const S K = static_cast<S>(0.307075 * unit::MeV * unit::cm2);
-    return S(0.5) * K * mat.molar_electron_density * rq.q2_over_beta2;
-}
-
-template <typename S>
-DPROP_HD S delta_half(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
-    if (mat.has_density_effect == S(0)) {
-        if (rq.beta_gamma < S(10)) {
-            return S(0);
-        }
-        const S plasma = static_cast<S>(28.816 * unit::eV) *
-                         sqrt(S(1000) * mat.molar_electron_density);
-        return log(rq.beta_gamma * plasma / mat.mean_excitation_energy) -
-               S(0.5);
-    }
-    const S x = log10(rq.beta_gamma);
-    S delta = S(0);
-    if (x >= mat.density_x0) {
-        delta = S(2) * static_cast<S>(constant::ln10) * x - mat.density_c;
-        if (x < mat.density_x1) {
-            delta += mat.density_a * pow(mat.density_x1 - x, mat.density_m);
-        }
-    }
-    return S(0.5) * delta;
-}
-
-template <typename S>
-DPROP_HD S bethe_bloch(const dev_slab<S>& mat, const rel_quantities<S>& rq) {
-    const S epl = eps_per_length(mat, rq);
-    if (epl <= S(0)) {
-        return S(0);
-    }
-    const S dhalf = delta_half(mat, rq);
-    const S I = mat.mean_excitation_energy;
-    const S u = S(2) * static_cast<S>(constant::m_e) * rq.beta_gamma *
-                rq.beta_gamma;
-    const S A = S(0.5) * log(u * rq.Wmax / (I * I));
-    return S(2) * epl * (A - rq.beta2 - dhalf);
-}
-
-template <typename S>
-DPROP_HD S landau_sigma_qop(S path_segment, const dev_slab<S>& mat,
-                            const rel_quantities<S>& rq, S q) {
-    const S fwhm = S(4) * eps_per_length(mat, rq) * path_segment;
-    const S sigmaE = S(0.5) * static_cast<S>(constant::inv_sqrt2) * fwhm /
-                     sqrt(static_cast<S>(constant::ln2));
-    const S p_inv = rq.qop / q;
-    return sqrt(rq.q2_over_beta2) * p_inv * p_inv * sigmaE;
-}
-
-template <typename S>
-DPROP_HD S scattering_theta0(S x_over_x0, const rel_quantities<S>& rq, S q,
-                             bool electron) {
-    if (x_over_x0 <= S(0)) {
-        return S(0);
-    }
-    const S mom_inv = fabs(rq.qop / q);
-    const S t = sqrt(x_over_x0 * rq.q2_over_beta2);
-    if (electron) {
-        return static_cast<S>(17.5 * unit::MeV) * mom_inv * t *
-               (S(1) + S(0.125) * log10(S(10) * x_over_x0));
-    }
-    return static_cast<S>(13.6 * unit::MeV) * mom_inv * t *
-           (S(1) + S(0.038) * S(2) * log(t));
-}
-
 // Path through a rod of radius r around a line surface at closest approach
 // d (material_rod::path_segment)
 template <typename S>

@@ -187,40 +187,6 @@ DPROP_HD void initial_jacobian(const detector_view<S, W>& det,
     }
 }
 
-// d(-dE/dx)/d(q/p) of the mean Bethe-Bloch stopping power as evaluated by
-// bethe_bloch (the formula of interaction::derive_bethe_bloch,
-// material/interaction.hpp:105-153, except that without density-effect data
-// the derivative of delta/2 follows the forward formula: zero below
-// beta*gamma = 10, -1/(q/p) above).
-template <typename S>
-DPROP_HD S bethe_bloch_dqop(const dev_slab<S>& mat, const rel_quantities<S>& rq,
-                            S bethe) {
-    const S epl = eps_per_length(mat, rq);
-    if (epl <= S(0)) {
-        return S(0);
-    }
-    const S first = S(2) / (rq.qop * rq.gamma2) * bethe;
-    const S dA = S(-1) / (S(2) * rq.qop) * (S(4) - rq.Wmax / rq.E);
-    const S dB = S(-2) * rq.beta2 / (rq.qop * rq.gamma2);
-    S dC;
-    if (mat.has_density_effect == S(0)) {
-        dC = (rq.beta_gamma < S(10)) ? S(0) : S(-1) / rq.qop;
-    } else {
-        const S x = log10(rq.beta_gamma);
-        S delta = S(0);
-        if (x >= mat.density_x0) {
-            delta = S(-2) / rq.qop;
-            if (x < mat.density_x1) {
-                delta += mat.density_a * mat.density_m /
-                         (rq.qop * static_cast<S>(constant::ln10)) *
-                         pow(mat.density_x1 - x, mat.density_m - S(1));
-            }
-        }
-        dC = S(0.5) * delta;
-    }
-    return first + S(2) * epl * (dA - dB - dC);
-}
-
 // Derivatives of the q/p after the kick of interact() with respect to the
 // q/p before it (mq) and to the incidence d.n (mc), for the bound state b
 // before the kick.  (1, 0) where interact() leaves q/p alone; (0, 0) where

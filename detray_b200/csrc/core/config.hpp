@@ -15,6 +15,10 @@ prop_cfg<S> make_prop_cfg(const dprop_config& c) {
     p.step.max_rk_updates = c.max_rk_updates;
     p.step.do_covariance_transport = c.do_covariance_transport != 0;
     p.step.field_gradient = c.use_field_gradient != 0;
+    p.step.use_mean_loss = c.use_mean_loss != 0;
+    p.step.use_eloss_gradient = c.use_eloss_gradient != 0;
+    p.step.mass = static_cast<S>(c.mass);
+    p.step.electron = (c.pdg == 11 || c.pdg == -11);
     p.nav.isect.min_mask_tol = static_cast<S>(c.min_mask_tolerance);
     p.nav.isect.max_mask_tol = static_cast<S>(c.max_mask_tolerance);
     p.nav.isect.mask_tol_scalor = static_cast<S>(c.mask_tolerance_scalor);

@@ -22,6 +22,9 @@ struct host_tables {
     std::vector<uint32_t> bf_surfaces;
     std::vector<dev_grid<S>> grids;
     std::vector<uint32_t> grid_bins;
+    // slab of each volume's homogeneous material (k_invalid: none); empty
+    // when no volume carries material
+    std::vector<uint32_t> vol_material;
 
     detector_view<S> view() const { return view_as<true>(); }
     template <bool W>
@@ -35,6 +38,7 @@ struct host_tables {
         v.bf_surfaces = bf_surfaces.data();
         v.grids = grids.data();
         v.grid_bins = grid_bins.data();
+        v.vol_material = vol_material.empty() ? nullptr : vol_material.data();
         v.n_volumes = static_cast<uint32_t>(volumes.size());
         v.n_surfaces = static_cast<uint32_t>(surfaces.size());
         return v;
@@ -91,6 +95,14 @@ inline std::string validate_desc(const dprop_detector_desc* d) {
               (d->grids[v.grid].kind != DPROP_GRID_CYLINDER &&
                d->grids[v.grid].kind != DPROP_GRID_DISC)))) {
             return "volume " + std::to_string(i) + " has an out-of-range index";
+        }
+        if (v.material != DPROP_INVALID_INDEX &&
+            (v.material >= d->n_slabs ||
+             d->slabs[v.material].kind != DPROP_MATERIAL_SLAB ||
+             !(d->slabs[v.material].X0 > 0.) ||
+             !(d->slabs[v.material].mean_excitation_energy > 0.))) {
+            return "volume " + std::to_string(i) +
+                   " has an invalid material index";
         }
     }
     for (uint32_t i = 0; i < d->n_bf_surfaces; ++i) {
@@ -242,7 +254,29 @@ host_tables<S> convert_desc(const dprop_detector_desc* d) {
         t.grids[i] = o;
     }
     t.grid_bins.assign(d->grid_bins, d->grid_bins + d->n_grid_bins);
+    bool any_material = false;
+    for (uint32_t i = 0; i < d->n_volumes; ++i) {
+        any_material = any_material ||
+                       d->volumes[i].material != DPROP_INVALID_INDEX;
+    }
+    if (any_material) {
+        t.vol_material.resize(d->n_volumes);
+        for (uint32_t i = 0; i < d->n_volumes; ++i) {
+            t.vol_material[i] = d->volumes[i].material;
+        }
+    }
     return t;
+}
+
+// True if any volume carries homogeneous material (the stepper then
+// evaluates the energy loss dq/p/ds: the full kernel variant).
+inline bool has_volume_material(const dprop_detector_desc* d) {
+    for (uint32_t i = 0; i < d->n_volumes; ++i) {
+        if (d->volumes[i].material != DPROP_INVALID_INDEX) {
+            return true;
+        }
+    }
+    return false;
 }
 
 }  // namespace dprop

@@ -177,8 +177,9 @@ DPROP_HD uint8_t machine_step(track_state<S>& ts, loop_state<S>& ls,
         return pc_done;
     }
     const bool reset = nav.is_on_surface() || ls.is_init;
-    ts.heartbeat =
-        ts.heartbeat && rk_step(st, nav.dist(), cfg.step, reset, field);
+    ts.heartbeat = ts.heartbeat &&
+                   rk_step<S, false, W>(st, nav.dist(), cfg.step, reset, field,
+                                        det.volume_material(nav.volume), ts.q);
     rk_policy(nav, st);
     if (ls.i > 0u) {
         ls.is_init = false;

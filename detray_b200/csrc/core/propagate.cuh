@@ -554,7 +554,9 @@ DPROP_HD uint8_t propagate_track_with(Nav& navigator, track_state<S, Grad>& ts,
         } else {
             const bool reset = nav.is_on_surface() || is_init;
             ts.heartbeat =
-                ts.heartbeat && rk_step(st, nav.dist(), cfg.step, reset, field);
+                ts.heartbeat &&
+                rk_step<S, Grad, W>(st, nav.dist(), cfg.step, reset, field,
+                                    det.volume_material(nav.volume), ts.q);
             rk_policy(nav, st);
             if (i > 0u) {
                 is_init = false;

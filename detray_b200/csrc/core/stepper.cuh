@@ -9,11 +9,15 @@
 //   transport Jacobian structure           codegen/detray-sympy/detray_sympy/
 //                                          matrices.py (D * J with the
 //                                          identity sub-structure)
-// Volume material (dqop/ds) is not on the device path: the supported
-// detectors carry surface material only, so qop_n = qop and dqopqop = 1.
+//   energy loss in volume material        rk_stepper.hpp:146-231 (dqopds,
+//                                          d2qopdsdqop), 536-567, 593-629,
+//                                          760-800 (dqop_n/dqop1, dqopqop)
+// Kernels for detectors without volume material are compiled without the
+// energy-loss terms (VM = false): there q/p_n = q/p and dqopqop = 1.
 #pragma once
 
 #include "field.cuh"
+#include "material.cuh"
 
 namespace dprop {
 
@@ -71,6 +75,12 @@ struct step_cfg {
     uint32_t max_rk_updates;
     bool do_covariance_transport;
     bool field_gradient;  // use_field_gradient: kernels with Grad = true
+    // energy loss in volume material (stepping::config)
+    bool use_mean_loss;       // q/p of each RK stage from the previous one
+    bool use_eloss_gradient;  // d(q/p)/d(q/p0) of the energy loss in the
+                              // transport Jacobian
+    S mass;                   // particle hypothesis
+    bool electron;            // e+-: bremsstrahlung in the stopping power
 };
 
 // Per-track stepper state (rk_stepper::state + base_stepper::state); Grad:
@@ -153,11 +163,11 @@ DPROP_HD mat33<S> matmul33(const mat33<S>& a, const mat33<S>& b) {
 // + dk4).
 template <typename S>
 DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
-                                      vec3<S> pos1, vec3<S> pos2, S h, S qop,
-                                      vec3<S> t0, vec3<S> t1, vec3<S> t2,
-                                      vec3<S> t3, vec3<S> b_middle,
-                                      vec3<S> b_last, mat33<S>& dFdr,
-                                      mat33<S>& dGdr) {
+                                      vec3<S> pos1, vec3<S> pos2, S h,
+                                      const S (&qn)[4], vec3<S> t0,
+                                      vec3<S> t1, vec3<S> t2, vec3<S> t3,
+                                      vec3<S> b_middle, vec3<S> b_last,
+                                      mat33<S>& dFdr, mat33<S>& dGdr) {
     const S half_h = h * S(0.5);
     const S h2 = h * h;
     const mat33<S> I = identity33<S>();
@@ -166,7 +176,7 @@ DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
     const mat33<S> g_fin = field_gradient(field, pos2);
     mat33<S> k1 = colwise_cross(g_ini, t0);
     for (int i = 0; i < 9; ++i) {
-        k1.m[i] *= -qop;
+        k1.m[i] *= -qn[0];
     }
     // dr_2/dr_1 = dr_3/dr_1 = I + h^2/8 dk1/dr1
     mat33<S> r23;
@@ -175,7 +185,7 @@ DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
     }
     const mat33<S> gr23 = matmul33(g_mid, r23);
     auto stage = [&](const mat33<S>& prev, S f, vec3<S> b, const mat33<S>& gr,
-                     vec3<S> t) {
+                     vec3<S> t, S qop) {
         mat33<S> a;
         for (int i = 0; i < 9; ++i) {
             a.m[i] = f * prev.m[i];
@@ -188,13 +198,13 @@ DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
         }
         return r;
     };
-    const mat33<S> k2 = stage(k1, half_h, b_middle, gr23, t1);
-    const mat33<S> k3 = stage(k2, half_h, b_middle, gr23, t2);
+    const mat33<S> k2 = stage(k1, half_h, b_middle, gr23, t1, qn[1]);
+    const mat33<S> k3 = stage(k2, half_h, b_middle, gr23, t2, qn[2]);
     mat33<S> r4;
     for (int i = 0; i < 9; ++i) {
         r4.m[i] = I.m[i] + h2 * S(0.5) * k3.m[i];
     }
-    const mat33<S> k4 = stage(k3, h, b_last, matmul33(g_fin, r4), t3);
+    const mat33<S> k4 = stage(k3, h, b_last, matmul33(g_fin, r4), t3, qn[3]);
     const S h_6 = h * static_cast<S>(1. / 6.);
     for (int i = 0; i < 9; ++i) {
         dFdr.m[i] = I.m[i] + h * h_6 * (k1.m[i] + k2.m[i] + k3.m[i]);
@@ -202,10 +212,13 @@ DPROP_HD void rk_position_derivatives(const field_view<S>& field, vec3<S> pos,
     }
 }
 
-// One adaptive RKN4 step towards a surface at (signed) distance dist.
-template <typename S, bool Grad>
+// One adaptive RKN4 step towards a surface at (signed) distance dist.  VM:
+// the detector may carry volume material; vm is the material of the volume
+// the track is in (NULL: none) and q the particle charge.
+template <typename S, bool Grad, bool VM = false>
 DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
-                      bool do_reset, const field_view<S>& field) {
+                      bool do_reset, const field_view<S>& field,
+                      const dev_slab<S>* vm = nullptr, S q = S(1)) {
     const S um = S(unit::um);
     if (fabs(dist) < um) {
         if (fabs(st.next_step_size) < cfg.min_stepsize) {
@@ -224,6 +237,24 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
     const vec3<S> pos = st.pos;
     const vec3<S> dir = st.dir;
     const S qop = st.qop;
+    // energy loss in the volume's material: q/p and d(q/p)/ds of each stage
+    // (evaluate_dqopds); without material every stage has the start q/p
+    const bool mat = VM && vm != nullptr;
+    S qn[4] = {qop, qop, qop, qop};
+    S dq[4] = {S(0), S(0), S(0), S(0)};
+    auto stage_qop = [&](int i, S hs) {
+        if constexpr (VM) {
+            if (mat) {
+                qn[i] = cfg.use_mean_loss ? qop + hs * dq[i - 1] : qop;
+                dq[i] = eloss_dqopds(*vm, qn[i], q, cfg.mass, cfg.electron);
+            }
+        }
+    };
+    if constexpr (VM) {
+        if (mat) {
+            dq[0] = eloss_dqopds(*vm, qop, q, cfg.mass, cfg.electron);
+        }
+    }
 
     // first stage
     const vec3<S> b_first = field_at(field, pos);
@@ -245,15 +276,18 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
         // second and third stage share the field at the mid point
         const vec3<S> pos1 = pos + half_h * t0 + (h2 * S(0.125)) * k0;
         b_middle = field_at(field, pos1);
+        stage_qop(1, half_h);
         t1 = (h == S(0)) ? dir : dir + half_h * k0;
-        k1 = qop * cross(t1, b_middle);
+        k1 = qn[1] * cross(t1, b_middle);
+        stage_qop(2, half_h);
         t2 = (h == S(0)) ? dir : dir + half_h * k1;
-        k2 = qop * cross(t2, b_middle);
+        k2 = qn[2] * cross(t2, b_middle);
         // last stage
         const vec3<S> pos2 = pos + h * t0 + (h2 * S(0.5)) * k2;
         b_last = field_at(field, pos2);
+        stage_qop(3, h);
         t3 = (h == S(0)) ? dir : dir + h * k2;
-        k3 = qop * cross(t3, b_last);
+        k3 = qn[3] * cross(t3, b_last);
         const S one_sixth = static_cast<S>(1. / 6.);
         const vec3<S> err_vec = (one_sixth * h2) * (k0 - k1 - k2 + k3);
         error = max_(norm(err_vec), S(1e-20));
@@ -263,7 +297,7 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
         st.step_size = st.step_size * step_size_scaling(cfg.rk_error_tol, error);
     }
     st.dtds = k3;
-    st.dqopds = S(0);
+    st.dqopds = dq[3];
 
     // step constraints (constrained_step::size, signed by the direction)
     const S dir_sign = st.step_size >= S(0) ? S(1) : S(-1);
@@ -285,17 +319,48 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
     const S h_6 = h * static_cast<S>(1. / 6.);
     st.pos = pos + h * (t0 + h_6 * (k0 + k1 + k2));
     st.dir = normalize(dir + h_6 * (k0 + S(2) * (k1 + k2) + k3));
+    if constexpr (VM) {
+        if (mat) {
+            st.qop = qop + h_6 * (dq[0] + S(2) * (dq[1] + dq[2]) + dq[3]);
+        }
+    }
     st.path_length += static_cast<double>(h);
     st.abs_path_length += static_cast<double>(fabs(h));
     ++st.n_steps;
 
     if (cfg.do_covariance_transport) {
         const S half_h = h * S(0.5);
-        // dk_n/dqop (qop_n = qop, no energy-loss gradient)
+        // dqop_n/dqop1 and the energy loss's d(q/p)/d(q/p1) over the step
+        // (both 1 without material or without the energy-loss gradient)
+        S n1 = S(1), n2 = S(1), n3 = S(1);
+        S dqopqop = S(1);
+        if constexpr (VM) {
+            if (mat && cfg.use_eloss_gradient) {
+                const S g1 = eloss_d2qopdsdqop(*vm, qn[0], q, cfg.mass,
+                                               cfg.electron);
+                n1 = S(1) + half_h * g1;
+                const S g2 = eloss_d2qopdsdqop(*vm, qn[1], q, cfg.mass,
+                                               cfg.electron) *
+                             n1;
+                n2 = S(1) + half_h * g2;
+                const S g3 = eloss_d2qopdsdqop(*vm, qn[2], q, cfg.mass,
+                                               cfg.electron) *
+                             n2;
+                n3 = S(1) + h * g3;
+                const S g4 = eloss_d2qopdsdqop(*vm, qn[3], q, cfg.mass,
+                                               cfg.electron) *
+                             n3;
+                dqopqop = S(1) + h_6 * (g1 + S(2) * (g2 + g3) + g4);
+            }
+        }
+        // dk_n/dqop
         const vec3<S> q0 = cross(t0, b_first);
-        const vec3<S> q1 = cross(t1, b_middle) + (qop * half_h) * cross(q0, b_middle);
-        const vec3<S> q2 = cross(t2, b_middle) + (qop * half_h) * cross(q1, b_middle);
-        const vec3<S> q3 = cross(t3, b_last) + (qop * h) * cross(q2, b_last);
+        const vec3<S> q1 =
+            n1 * cross(t1, b_middle) + (qn[1] * half_h) * cross(q0, b_middle);
+        const vec3<S> q2 =
+            n2 * cross(t2, b_middle) + (qn[2] * half_h) * cross(q1, b_middle);
+        const vec3<S> q3 =
+            n3 * cross(t3, b_last) + (qn[3] * h) * cross(q2, b_last);
         const vec3<S> dFdqop = (h * h_6) * (q0 + q1 + q2);
         const vec3<S> dGdqop = h_6 * (q0 + S(2) * (q1 + q2) + q3);
 
@@ -303,7 +368,7 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
         const mat33<S> I = identity33<S>();
         mat33<S> d0 = colwise_cross(I, b_first);
         for (int k = 0; k < 9; ++k) {
-            d0.m[k] *= qop;
+            d0.m[k] *= qn[0];
         }
         mat33<S> tmp;
         for (int k = 0; k < 9; ++k) {
@@ -311,18 +376,18 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
         }
         mat33<S> d1 = colwise_cross(tmp, b_middle);
         for (int k = 0; k < 9; ++k) {
-            d1.m[k] *= qop;
+            d1.m[k] *= qn[1];
             tmp.m[k] = I.m[k] + half_h * d1.m[k];
         }
         mat33<S> d2 = colwise_cross(tmp, b_middle);
         for (int k = 0; k < 9; ++k) {
-            d2.m[k] *= qop;
+            d2.m[k] *= qn[2];
             tmp.m[k] = I.m[k] + h * d2.m[k];
         }
         mat33<S> d3 = colwise_cross(tmp, b_last);
         mat33<S> dFdt, dGdt;
         for (int k = 0; k < 9; ++k) {
-            d3.m[k] *= qop;
+            d3.m[k] *= qn[3];
             dFdt.m[k] = h * (I.m[k] + h_6 * (d0.m[k] + d1.m[k] + d2.m[k]));
             dGdt.m[k] = I.m[k] + h_6 * (d0.m[k] + S(2) * (d1.m[k] + d2.m[k]) +
                                         d3.m[k]);
@@ -342,7 +407,7 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
             const vec3<S> pos1 = base + half_h * t0 + (h * h * S(0.125)) * k0;
             const vec3<S> pos2 = base + h * t0 + (h * h * S(0.5)) * k2;
             mat33<S> dFdr, dGdr;
-            rk_position_derivatives(field, base, pos1, pos2, h, qop, t0, t1,
+            rk_position_derivatives(field, base, pos1, pos2, h, qn, t0, t1,
                                     t2, t3, b_middle, b_last, dFdr, dGdr);
             mat33<S> nP, nQ;
             for (int r = 0; r < 3; ++r) {
@@ -386,6 +451,7 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
             J.B = nB;
             J.c = {ncv[0], ncv[1], ncv[2]};
             J.d = {ndv[0], ndv[1], ndv[2]};
+            J.e = dqopqop * J.e;
         } else {
             mat33<S> nA, nB;
             vec3<S> nc, nd;
@@ -422,7 +488,7 @@ DPROP_HD bool rk_step(step_state<S, Grad>& st, S dist, const step_cfg<S>& cfg,
             J.B = nB;
             J.c = nc;
             J.d = nd;
-            // J.e unchanged: dqopqop = 1
+            J.e = dqopqop * J.e;
         }
     }
     return true;

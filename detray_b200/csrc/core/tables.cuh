@@ -117,8 +117,9 @@ struct alignas(16) dev_grid {
 };
 
 // Read-only view handed to the kernels by value.  W = false promises that the
-// detector holds no line surfaces, material rods, multi-entry grid bins or
-// material maps: the code for them is then left out of the propagation.
+// detector holds no line surfaces, material rods, multi-entry grid bins,
+// material maps or volume material: the code for them is then left out of
+// the propagation.
 template <typename S, bool W = true>
 struct detector_view {
     const dev_volume* volumes;
@@ -129,8 +130,21 @@ struct detector_view {
     const uint32_t* bf_surfaces;
     const dev_grid<S>* grids;
     const uint32_t* grid_bins;
+    const uint32_t* vol_material;  // [n_volumes] slab of the volume's
+                                   // material or k_invalid; NULL: none has
     uint32_t n_volumes;
     uint32_t n_surfaces;
+
+    // The homogeneous material of volume v, or NULL.
+    DPROP_HD const dev_slab<S>* volume_material(uint32_t v) const {
+        if constexpr (W) {
+            if (vol_material != nullptr) {
+                const uint32_t m = vol_material[v];
+                return m != k_invalid ? slabs + m : nullptr;
+            }
+        }
+        return nullptr;
+    }
 };
 
 // Magnetic field view.  kind 0: constant; kind 1: (r, phi, z) node map of

@@ -135,10 +135,11 @@ dprop_status dprop_propagate_direct(const dprop_config* cfg,
     if (!cfg || !det || !field || !seq || !results) {
         return fail(DPROP_E_INVALID, "propagate_direct: NULL argument");
     }
-    if (cfg->use_field_gradient || cfg->use_eloss_gradient) {
+    if (cfg->use_field_gradient || cfg->use_eloss_gradient ||
+        det->vol_material != nullptr) {
         return fail(DPROP_E_UNSUPPORTED,
-                    "propagate_direct: field/eloss gradients are not "
-                    "supported on the device path");
+                    "propagate_direct: field/eloss gradients and volume "
+                    "material are not supported by the direct navigator");
     }
     if (cfg->max_iterations == 0u) {
         return fail(DPROP_E_INVALID,

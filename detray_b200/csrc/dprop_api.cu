@@ -515,11 +515,6 @@ dprop_status check_config(const dprop_config* cfg) {
     if (!cfg) {
         return fail(DPROP_E_INVALID, "config is NULL");
     }
-    if (cfg->use_eloss_gradient) {
-        return fail(DPROP_E_UNSUPPORTED,
-                    "use_eloss_gradient needs volume material, which the "
-                    "device path does not support");
-    }
     if (cfg->max_iterations == 0u) {
         return fail(DPROP_E_INVALID, "max_iterations must be > 0");
     }
@@ -1045,10 +1040,13 @@ dprop_status dprop_detector_create(const dprop_detector_desc* d, int device,
         (st = upload(t.slabs, &det->slabs)) != DPROP_OK ||
         (st = upload(t.bf_surfaces, &det->bf_surfaces)) != DPROP_OK ||
         (st = upload(t.grids, &det->grids)) != DPROP_OK ||
-        (st = upload(t.grid_bins, &det->grid_bins)) != DPROP_OK) {
+        (st = upload(t.grid_bins, &det->grid_bins)) != DPROP_OK ||
+        (!t.vol_material.empty() &&
+         (st = upload(t.vol_material, &det->vol_material)) != DPROP_OK)) {
         dprop_detector_destroy(det);
         return st;
     }
+    det->wires = has_volume_material(d);
     for (uint32_t i = 0; i < d->n_surfaces; ++i) {
         det->wires = det->wires || d->surfaces[i].shape == DPROP_SHAPE_LINE ||
                      d->surfaces[i].material_kind != 0u;
@@ -1083,6 +1081,7 @@ dprop_status dprop_detector_destroy(dprop_detector* det) {
     cudaFree(det->bf_surfaces);
     cudaFree(det->grids);
     cudaFree(det->grid_bins);
+    cudaFree(det->vol_material);
     cudaFree(det->masks_d);
     cudaFree(det->transforms_d);
     cudaFree(det->slabs_d);

@@ -81,8 +81,18 @@ def load_npz(path) -> dict:
     with np.load(path) as z:
         out = {}
         for name, ctype in TABLES:
-            arr = z[name]
-            out[name] = np.ascontiguousarray(arr).view(dtype_of(ctype)).reshape(-1)
+            arr = np.ascontiguousarray(z[name])
+            dt = dtype_of(ctype)
+            if name == "volumes" and arr.dtype.names is not None and \
+                    "material" not in arr.dtype.names:
+                # tables written before volumes carried a material index
+                vol = np.zeros(arr.shape[0], dtype=dt)
+                for f in arr.dtype.names:
+                    vol[f] = arr[f]
+                vol["material"] = abi.DPROP_INVALID_INDEX
+                out[name] = vol
+                continue
+            out[name] = arr.view(dt).reshape(-1)
         return out
 
 

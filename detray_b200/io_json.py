@@ -375,6 +375,7 @@ def read_detector(files) -> dict:
         vo = volumes_out[vi]
         vo["transform"] = vol_trf_index[vi]
         vo["grid"] = abi.DPROP_INVALID_INDEX
+        vo["material"] = abi.DPROP_INVALID_INDEX
         off = vol_sf_offset[vi]
         has_grid = vi in nav_grids
         vo["bf_begin"] = len(bf_out)

@@ -228,6 +228,46 @@ struct slab_copier {
     }
 };
 
+/// Material-store visitor for a volume's material: a homogeneous material
+/// (material/material.hpp, added by homogeneous_volume_material_builder) as
+/// a slab of zero thickness; volume material maps are not supported.
+struct volume_material_copier {
+    template <typename mat_group_t, typename index_t>
+    void operator()(const mat_group_t& group, const index_t& idx,
+                    flat_detector& out, dprop_volume_desc& vd) const {
+        using mat_t = typename mat_group_t::value_type;
+        if constexpr (requires(const mat_t& m) {
+                          m.X0();
+                          m.molar_electron_density();
+                          m.mean_excitation_energy();
+                      }) {
+            const mat_t& mat = group[idx];
+            dprop_slab_desc d{};
+            d.kind = DPROP_MATERIAL_SLAB;
+            d.X0 = static_cast<double>(mat.X0());
+            d.molar_electron_density =
+                static_cast<double>(mat.molar_electron_density());
+            d.mean_excitation_energy =
+                static_cast<double>(mat.mean_excitation_energy());
+            d.has_density_effect = mat.has_density_effect_data() ? 1u : 0u;
+            if (mat.has_density_effect_data()) {
+                const auto& de = mat.density_effect_data();
+                d.density_a = static_cast<double>(de.get_A_density());
+                d.density_m = static_cast<double>(de.get_M_density());
+                d.density_x0 = static_cast<double>(de.get_X0_density());
+                d.density_x1 = static_cast<double>(de.get_X1_density());
+                d.density_c = static_cast<double>(de.get_C_density());
+            }
+            vd.material = static_cast<uint32_t>(out.slabs.size());
+            out.slabs.push_back(d);
+        } else {
+            throw std::runtime_error(
+                "dprop::flatten: only homogeneous volume material is "
+                "supported on the device path");
+        }
+    }
+};
+
 /// Accelerator-store visitor: brute-force lists and 2D surface grids.
 template <typename detector_t>
 struct accel_copier {
@@ -376,10 +416,11 @@ flat_detector flatten(const detector_t& det) {
         dprop_volume_desc vd{};
         vd.transform = static_cast<uint32_t>(v.transform());
         vd.grid = DPROP_INVALID_INDEX;
+        vd.material = DPROP_INVALID_INDEX;
         if (v.has_material()) {
-            throw std::runtime_error(
-                "dprop::flatten: volume material is not supported on the "
-                "device path");
+            det.material_store()
+                .template visit<adapter_detail::volume_material_copier>(
+                    v.material(), out, vd);
         }
         const auto& links = v.accel_link();
         for (std::size_t li = 0u; li < links.size(); ++li) {

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define DPROP_ABI_VERSION 2u
+#define DPROP_ABI_VERSION 3u
 
 /* ------------------------------------------------------------------ status */
 typedef enum dprop_status {
@@ -189,6 +189,12 @@ typedef struct dprop_volume_desc {
                                passives searched by brute force                 */
     uint32_t bf_end;
     uint32_t grid;          /* into grids, or DPROP_INVALID_INDEX                */
+    uint32_t material;      /* homogeneous volume material: into slabs (kind
+                               DPROP_MATERIAL_SLAB; thickness unused), the
+                               material the stepper's energy loss dq/p/ds
+                               reads (tracking_volume::material_parameters,
+                               rk_stepper.hpp:148-231); DPROP_INVALID_INDEX:
+                               none                                         */
 } dprop_volume_desc;
 
 typedef struct dprop_detector_desc {

@@ -751,7 +751,10 @@ typedef struct ref_tel_cfg {
     double half_x, half_y;     /* rectangle module half lengths (mm)  */
     const double* positions;   /* module positions along the pilot (mm) */
     uint32_t n_positions;
-    uint32_t pad;
+    uint32_t volume_material;  /* homogeneous volume material: 0 none,
+                                  1 cesium iodide (with density-effect
+                                  data), 2 iron, 3 liquid argon, 4 silicon
+                                  (with density-effect data)               */
     double pilot_dir[3];       /* pilot track direction               */
     double mat_thickness;      /* silicon slab thickness (mm)          */
     double envelope;           /* portal envelope (mm); <= 0 default   */
@@ -811,6 +814,24 @@ int ref_build_telescope(const ref_tel_cfg* c, void** out) {
         }
         if (c->envelope > 0.) {
             cfg.envelope(static_cast<scalar>(c->envelope));
+        }
+        switch (c->volume_material) {
+            case 0u:
+                break;
+            case 1u:
+                cfg.volume_material(cesium_iodide_with_ded<scalar>());
+                break;
+            case 2u:
+                cfg.volume_material(iron<scalar>());
+                break;
+            case 3u:
+                cfg.volume_material(argon_liquid<scalar>());
+                break;
+            case 4u:
+                cfg.volume_material(silicon_with_ded<scalar>());
+                break;
+            default:
+                throw std::runtime_error("unknown volume material code");
         }
         auto [det, names] =
             build_telescope_detector<algebra_t, rectangle2D>(h->mr, cfg);

@@ -34,7 +34,7 @@ class _RefTelCfg(C.Structure):
         ("half_y", C.c_double),
         ("positions", C.POINTER(C.c_double)),
         ("n_positions", C.c_uint32),
-        ("pad", C.c_uint32),
+        ("volume_material", C.c_uint32),
         ("pilot_dir", C.c_double * 3),
         ("mat_thickness", C.c_double),
         ("envelope", C.c_double),
@@ -225,13 +225,22 @@ def build_wire_chamber(n_layers=10, square_cells=True,
     return RefDetector(lib, h)
 
 
+# homogeneous volume materials of build_telescope(volume_material=...)
+VOLUME_MATERIALS = {None: 0, "cesium_iodide": 1, "iron": 2,
+                    "argon_liquid": 3, "silicon": 4}
+
+
 def build_telescope(positions=tuple(50.0 * i for i in range(10)),
                     half_x=500.0, half_y=500.0, pilot_dir=(1.0, 0.0, 0.0),
-                    mat_thickness=0.3, envelope=0.0,
+                    mat_thickness=0.3, envelope=0.0, volume_material=None,
                     precision="f64") -> RefDetector:
+    """The reference's telescope (build_telescope_detector.hpp:187), with
+    an optional homogeneous volume material filling the telescope volume
+    (tel_det_config::volume_material)."""
     lib = load(precision)
     pos = (C.c_double * len(positions))(*positions)
-    cfg = _RefTelCfg(half_x, half_y, pos, len(positions), 0,
+    cfg = _RefTelCfg(half_x, half_y, pos, len(positions),
+                     VOLUME_MATERIALS[volume_material],
                      (C.c_double * 3)(*pilot_dir), mat_thickness, envelope)
     h = C.c_void_p()
     _check(lib, lib.ref_build_telescope(C.byref(cfg), C.byref(h)))

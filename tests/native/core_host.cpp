@@ -455,7 +455,7 @@ int run_rounds(const dprop_detector_desc* desc, uint32_t field_kind,
         return 1;
     }
     const host_tables<S> tables = convert_desc<S>(desc);
-    bool wires = false;
+    bool wires = has_volume_material(desc);
     for (uint32_t i = 0; i < desc->n_surfaces; ++i) {
         wires = wires || desc->surfaces[i].shape == DPROP_SHAPE_LINE ||
                 desc->surfaces[i].material_kind != 0u;

@@ -106,9 +106,11 @@ def test_argument_validation_without_device(lib):
                                        None, 0, None) == abi.DPROP_E_INVALID
     assert lib.dprop_backward(None, None, None, None, None, None, 0,
                               None) == abi.DPROP_E_INVALID
+    # the energy-loss gradient is a valid configuration; the missing
+    # detector is what fails
     cfg = abi.make_config(use_eloss_gradient=1)
-    assert lib.dprop_propagate(C.byref(cfg), None, None, None, None, None, 0,
-                               None) == abi.DPROP_E_UNSUPPORTED
+    assert lib.dprop_propagate(C.byref(cfg), None, None, None, None, None, 1,
+                               None) == abi.DPROP_E_INVALID
     assert lib.dprop_propagate_direct(None, None, None, None, None, None, 0,
                                       None) == abi.DPROP_E_INVALID
     assert lib.dprop_helix_scan(None, None, None, 0, 0.0, None,

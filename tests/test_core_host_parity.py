@@ -172,3 +172,35 @@ def test_material_map_tables_are_validated(core_host):
 def _alloc(n, max_records):
     from oracle import ref_oracle
     return ref_oracle.alloc_results(n, max_records)
+
+
+@pytest.mark.parametrize("material", ["cesium_iodide", "iron", "silicon"])
+@pytest.mark.parametrize("eloss_gradient", [0, 1])
+def test_core_f64_volume_material(core_host, oracle, material,
+                                  eloss_gradient):
+    """A telescope whose volume is filled with a homogeneous material
+    (tel_det_config::volume_material): the stepper loses energy along every
+    step (d(q/p)/ds per RK stage from the Bethe-Bloch stopping power) and,
+    with use_eloss_gradient, carries d(q/p)/d(q/p0) into the transport
+    Jacobian (rk_stepper.hpp:146-231, 760-800).  fp64 host core against the
+    fp64 oracle: same surfaces, parameters to ~1e-7, with and without the
+    mean-loss stage update."""
+    from detray_b200 import abi, tracks
+    det = oracle.build_telescope(volume_material=material)
+    assert det.desc.volumes[0].material != abi.DPROP_INVALID_INDEX
+    trk = tracks.telescope_tracks(1000, seed=7)
+    for mean_loss in (1, 0):
+        cfg = abi.make_config(max_records=16, use_mean_loss=mean_loss,
+                              use_eloss_gradient=eloss_gradient)
+        ref = oracle.propagate(det, {"kind": "const", "b": (0, 0, 2 * T)},
+                               cfg, trk)
+        got = run_core(core_host, oracle, det.desc, cfg, trk, 8)
+        s = compare(ref, got, max_seq_mismatch_frac=0.0, tol_abs=TIGHT,
+                    tol_rel=1e-7, cov_rel=1e-5)
+        assert s["seq_mismatch"] == 0 and s["status_mismatch"] == 0
+        # the volume material takes energy: |q/p| grows along the track
+        n = np.minimum(got["n_records"], cfg.max_records)
+        ok = n >= 2
+        last = got["rec_bound"][4][n[ok] - 1, np.nonzero(ok)[0]]
+        first = got["rec_bound"][4][0, ok]
+        assert np.all(np.abs(last) > np.abs(first))

@@ -91,6 +91,37 @@ def test_device_vs_oracle(torch_cuda, oracle, kind):
         print(kind, method, summary)
 
 
+@pytest.mark.parametrize("eloss_gradient", [0, 1])
+def test_device_volume_material_vs_oracle(torch_cuda, oracle,
+                                          eloss_gradient):
+    """Telescope (config 1's 10 000 tracks) whose volume is filled with
+    cesium iodide: energy loss in every RK stage, and with
+    use_eloss_gradient its derivative in the transport Jacobian, on both
+    launch forms against the fp64 oracle built with the same volume
+    material."""
+    from detray_b200 import abi, propagator, tracks
+    from detray_b200.units import T
+    ref_det = oracle.build_telescope(volume_material="cesium_iodide")
+    det = propagator.Detector(ref_det.tables())
+    field = propagator.Field.constant((0.0, 0.0, 2.0 * T))
+    cfg = abi.make_config(max_records=16, use_eloss_gradient=eloss_gradient)
+    trk = tracks.telescope_tracks(10000, seed=11)
+    ref = oracle.propagate(ref_det, field.spec, cfg, trk)
+    for method, sort in ((0, 0), (1, 1)):
+        got = _run_device(torch_cuda, det, field, cfg, trk, method=method,
+                          sort_tracks=sort)
+        summary = compare(ref, got, max_seq_mismatch_frac=1e-3,
+                          tol_abs=TOL_ABS, tol_rel=TOL_REL, cov_rel=COV_REL)
+        print("volume material", eloss_gradient, method, summary)
+        # energy is lost in the volume: |q/p| at the last record above the
+        # first one
+        n = np.minimum(got["n_records"], cfg.max_records)
+        ok = n >= 2
+        cols = np.nonzero(ok)[0]
+        assert np.all(np.abs(got["rec_bound"][4][n[ok] - 1, cols]) >
+                      np.abs(got["rec_bound"][4][0, cols]))
+
+
 def _assert_same_results(a, b, what):
     for key in ["status", "n_records", "n_steps", "n_trials",
                 "n_intersections", "n_transports", "n_material",
@@ -195,11 +226,16 @@ def test_empty_batch_and_invalid_arguments(torch_cuda):
     rc = lib.dprop_propagate(C.byref(cfg), None, None, field.handle,
                              C.byref(ts), C.byref(res.struct), 1, None)
     assert rc == abi.DPROP_E_INVALID
-    bad = abi.make_config(use_eloss_gradient=1)
-    rc = lib.dprop_propagate(C.byref(bad), None, det.handle, field.handle,
-                             C.byref(ts), C.byref(res.struct), 1, None)
-    assert rc == abi.DPROP_E_UNSUPPORTED
-    assert "gradient" in lib.dprop_last_error().decode()
+    # the energy-loss gradient without volume material: accepted (its terms
+    # are identity there)
+    eg = abi.make_config(max_records=16, use_eloss_gradient=1)
+    one = torch_cuda.tensor(trk[:, :1], dtype=torch_cuda.float32,
+                            device="cuda")
+    ts1 = propagator.tracks_struct(one)
+    res1 = propagator.alloc_device_results(1, eg.max_records, "cuda")
+    rc = lib.dprop_propagate(C.byref(eg), None, det.handle, field.handle,
+                             C.byref(ts1), C.byref(res1.struct), 1, None)
+    assert rc == abi.DPROP_OK
 
 
 def test_device_in_field_map_vs_oracle(torch_cuda, oracle):

@@ -64,6 +64,10 @@ def _assert_identical(a, b):
 
 
 def _case(oracle, kind):
+    if kind == "telescope_volume_material":
+        return (oracle.build_telescope(volume_material="iron"),
+                tracks.telescope_tracks(400, seed=8),
+                abi.make_config(max_records=16, use_eloss_gradient=1), None)
     if kind == "telescope":
         return (oracle.build_telescope(), tracks.telescope_tracks(400, seed=3),
                 abi.make_config(max_records=16), None)
@@ -89,7 +93,7 @@ def _case(oracle, kind):
 
 
 @pytest.mark.parametrize("kind", ["telescope", "toy", "toy_map", "toy_maps",
-                                  "wire"])
+                                  "wire", "telescope_volume_material"])
 @pytest.mark.parametrize("prec", [4, 8])
 def test_rounds_equal_one_shot_loop(core_host, oracle, kind, prec):
     det, trk, cfg, fmap = _case(oracle, kind)
