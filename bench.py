@@ -74,6 +74,9 @@ def parse_args():
                         "(telescope; toy in the solenoid map; toy + wire "
                         "chamber in fp32 and fp64) instead of the headline "
                         "line")
+    p.add_argument("--no-config5", action="store_true",
+                   help="skip benchmark configuration 5 (toy + wire chamber, "
+                        "16 M tracks each, fp32 and fp64; single GPU only)")
     p.add_argument("--no-config3", action="store_true",
                    help="skip the field-map configuration object")
     p.add_argument("--dry-run", action="store_true",
@@ -696,6 +699,7 @@ def run_ours(args):
     # ---- end to end through the host-buffer API
     e2e = None
     if not args.no_e2e:
+        link = link_bandwidth(dev)
         pinned_trk = torch.tensor(host_trk, dtype=torch.float64).pin_memory()
         host_in = pinned_trk.numpy()
         out = propagator.alloc_host_results(n, cfg.max_records, pinned=True,
@@ -722,10 +726,16 @@ def run_ours(args):
         n_rec = int(out[0]["rec_offsets"][n])
         rec = n_rec * (8 + 6 * 4 + 21 * 4 + 4 + 1)
         d2h = n * (1 + 7 * 4 + 8 * 4) + (n + 1) * 4 + rec
+        # the copies alone at the measured link bandwidth: the bound the
+        # e2e time approaches when the pipeline hides the propagation
+        copy_ms = (h2d / link["h2d_gbs"] + d2h / link["d2h_gbs"]) / 1e6
+        link["copy_bound_ms"] = round(copy_ms, 3)
+        link["bound_ms"] = round(max(copy_ms, ms), 3)
+        link["frac"] = round(max(copy_ms, ms) / ms_e2e, 4)
         e2e = {"value": total_tracks / (ms_e2e / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(ms_e2e, 3), "steps": k_e2e,
-               "records_per_step": n_rec,
+               "records_per_step": n_rec, "link": link,
                "api": "dprop_propagate_host, jagged records, chunked "
                       "pipeline (4 chunks on prioritized streams, records "
                       "drained on a copy stream), pinned host buffers"}
@@ -741,6 +751,11 @@ def run_ours(args):
     cfg3 = None
     if not args.no_config3:
         cfg3 = config3_row(args, dev, stream, world)
+    cfg5 = None
+    if not args.no_config5 and world == 1:
+        propagator.release_cache()
+        cfg5 = config5_row(args, dev,
+                           oracle_errors=rank == 0 and not args.no_cpu_baseline)
 
     cpu, errors = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -775,6 +790,7 @@ def run_ours(args):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "errors_vs_fp64_oracle": errors,
             "config3": cfg3,
+            "config5": cfg5,
             "adjoint": adj,
             "other_entry_points": extras,
             "gpu_launches": args.steps * per_step,
@@ -906,6 +922,30 @@ def reference_gpu_config3(args, cfg):
                       "records written"}
 
 
+def link_bandwidth(dev, nbytes=1 << 29):
+    """Host <-> device copy bandwidth between pinned host memory and the
+    device, GB/s per direction (one cudaMemcpyAsync of 512 MiB, best of 5):
+    the denominator of the end-to-end leg, whose copies cross this link."""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, dst, src in (("h2d_gbs", d, h), ("d2h_gbs", h, d)):
+        best = None
+        for _ in range(6):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = round(nbytes / (best / 1e3) / 1e9, 2)
+    del h, d
+    return out
+
+
 # ------------------------------------------------ other configurations
 def _time_device(fn, dev, steps, warmup):
     import torch
@@ -959,6 +999,100 @@ def _errors_vs_oracle(ref, got):
             c += 1
     out["cov_rel_max"] = worst
     return out
+
+
+def config5_row(args, dev, oracle_errors):
+    """Benchmark configuration 5: the toy detector and the wire chamber (10
+    layers of square drift cells) in the solenoid field map, 16 M muons per
+    detector (eta in [-4, 4], pT log-uniform in 0.1-100 GeV, the same
+    tracks for both detectors and both builds) in batches of 2 M held in
+    one device buffer: the fp32 build (the autotuner's launch form for the
+    detector, CUDA graph) and the fp64 build (dprop_launch.precision = 8),
+    tracks/s
+    and the FP32 / FP64 roofline fraction of each; with oracle_errors the
+    per-surface errors against the fp64 oracle on a 3 000-track sample."""
+    import numpy as np
+    import torch
+
+    from detray_b200 import abi, fields, flops, geometry, propagator, tracks
+    sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak32 = flops.nominal_fp32_tflops(sm, 1965.0)
+    field = propagator.Field.grid(fields.solenoid_map(), dev.index)
+    cfg = abi.make_config(max_records=48, search_window=(3, 3),
+                          estimate_scattering_noise=0)
+    n5 = 16_000_000
+    batch = 2_000_000
+    batches = [tracks.toy_tracks(batch, seed=args.seed + 50 + b0,
+                                 pt_range=(0.1, 100.0))
+               for b0 in range(0, n5, batch)]
+    out = {}
+    for name in ("toy_4brl_7edc", "wire_chamber_10l_cells"):
+        det = propagator.Detector(geometry.load_geometry(name), dev.index)
+        for prec, dtype in ((4, torch.float32), (8, torch.float64)):
+            dt = torch.empty((8, batch), dtype=dtype, device=dev)
+            if prec == 4:
+                # the autotuner's pick for this detector (on the first batch)
+                dt.copy_(torch.from_numpy(batches[0]))
+                lc, _ = propagator.autotune(cfg, det, field, dt, use_graph=1)
+                propagator.release_cache()
+            else:
+                lc = propagator.make_launch(sort_tracks=1, precision=8)
+            res = propagator.alloc_device_results(batch, cfg.max_records, dev,
+                                                  dtype=dtype)
+            total_ms = 0.0
+            fl = 0.0
+            status = np.zeros(8, dtype=np.int64)
+            for bi, trk in enumerate(batches):
+                dt.copy_(torch.from_numpy(trk))
+                total_ms += _time_device(lambda: propagator.propagate(
+                    cfg, det, field, dt, results=res, launch=lc), dev, 1,
+                    1 if bi == 0 else 0)
+                t = res.tensors
+                fl += flops.algorithmic_flops(
+                    t["n_trials"].cpu().numpy(), t["n_steps"].cpu().numpy(),
+                    t["n_intersections"].cpu().numpy(),
+                    t["n_transports"].cpu().numpy(),
+                    t["n_material"].cpu().numpy())
+                status += np.bincount(t["status"].cpu().numpy(),
+                                      minlength=8)[:8]
+            peak = peak32 if prec == 4 else peak32 / 2.0
+            key = f"{name}_fp{8 * prec}"
+            out[key] = {
+                "tracks": n5, "ms": round(total_ms, 2),
+                "tracks_per_s": n5 / (total_ms / 1e3),
+                "launch": (dict(launch_fields(lc), cuda_graph=1,
+                                how="autotuned on the first batch")
+                           if prec == 4 else "plain fp64, sorted"),
+                "achieved_tflops": fl / (total_ms / 1e3) / 1e12,
+                "roofline_frac": fl / (total_ms / 1e3) / 1e12 / peak,
+                "peak_source": "nominal FP32" if prec == 4 else
+                               "nominal FP64 = FP32 / 2",
+                "status_counts": {
+                    nm: int(status[c]) for nm, c in (
+                        ("exited", abi.TRK_EXITED),
+                        ("path_limit", abi.TRK_PATH_LIMIT),
+                        ("stalled", abi.TRK_STALLED),
+                        ("no_surface", abi.TRK_NO_SURFACE),
+                        ("max_iterations", abi.TRK_MAX_ITER))}}
+            del res, dt
+            torch.cuda.empty_cache()
+            if oracle_errors:
+                from oracle import ref_oracle
+                ref_det = (ref_oracle.build_toy() if name == "toy_4brl_7edc"
+                           else ref_oracle.build_wire_chamber(
+                               square_cells=True))
+                sample = tracks.toy_tracks(3000, seed=args.seed + 99,
+                                           pt_range=(0.1, 100.0))
+                ref = ref_oracle.propagate(ref_det, field.spec, cfg, sample)
+                got = propagator.propagate(
+                    cfg, det, field,
+                    torch.tensor(sample, dtype=dtype, device=dev), launch=lc)
+                got = {k: v.cpu().numpy() for k, v in got.tensors.items()}
+                got["rec_barcode"] = got["rec_barcode"].view(np.uint64)
+                out[key]["errors_vs_fp64_oracle"] = _errors_vs_oracle(ref, got)
+    return {"config": 5, "workload": "toy_4brl_7edc + wire_chamber_10l_cells, "
+            "solenoid map, 16M muons per detector eta -4..4 pT 0.1-100",
+            "results": out}
 
 
 def run_sweep(args):
@@ -1047,66 +1181,9 @@ def run_sweep(args):
                  "dtype": "f32"})
     del res, dt
 
-    # ---- config 5: toy + wire chamber, fp32 and fp64, 16 M tracks
-    cfg = abi.make_config(max_records=48, search_window=(3, 3),
-                          estimate_scattering_noise=0)
-    per_det = {"toy_4brl_7edc": lambda: ref_oracle.build_toy(),
-               "wire_chamber_10l_cells":
-                   lambda: ref_oracle.build_wire_chamber(square_cells=True)}
-    n5 = 8_000_000
-    batch = 2_000_000
-    sweep = {}
-    for name, build_ref in per_det.items():
-        det = propagator.Detector(geometry.load_geometry(name))
-        for prec, dtype in ((4, torch.float32), (8, torch.float64)):
-            lc = propagator.make_launch(sort_tracks=1, precision=prec)
-            res = propagator.alloc_device_results(batch, cfg.max_records, dev,
-                                                  dtype=dtype)
-            total_ms = 0.0
-            fl = 0.0
-            status = np.zeros(8, dtype=np.int64)
-            for b0 in range(0, n5, batch):
-                trk = tracks.toy_tracks(batch, seed=args.seed + 50 + b0,
-                                        pt_range=(0.1, 100.0))
-                dt = torch.tensor(trk, dtype=dtype, device=dev)
-                total_ms += _time_device(lambda: propagator.propagate(
-                    cfg, det, field, dt, results=res, launch=lc), dev, 1,
-                    1 if b0 == 0 else 0)
-                t = res.tensors
-                fl += flops.algorithmic_flops(
-                    t["n_trials"].cpu().numpy(), t["n_steps"].cpu().numpy(),
-                    t["n_intersections"].cpu().numpy(),
-                    t["n_transports"].cpu().numpy(),
-                    t["n_material"].cpu().numpy())
-                status += np.bincount(t["status"].cpu().numpy(),
-                                      minlength=8)[:8]
-            peak = peak32 if prec == 4 else peak32 / 2.0
-            key = f"{name}_fp{8 * prec}"
-            sweep[key] = {"tracks": n5, "ms": round(total_ms, 2),
-                          "tracks_per_s": n5 / (total_ms / 1e3),
-                          "achieved_tflops": fl / (total_ms / 1e3) / 1e12,
-                          "roofline_frac": fl / (total_ms / 1e3) / 1e12 / peak,
-                          "peak_source": "nominal FP32" if prec == 4 else
-                                         "nominal FP64 = FP32 / 2",
-                          "status_counts": {
-                              nm: int(status[c]) for nm, c in (
-                                  ("exited", abi.TRK_EXITED),
-                                  ("path_limit", abi.TRK_PATH_LIMIT),
-                                  ("stalled", abi.TRK_STALLED),
-                                  ("no_surface", abi.TRK_NO_SURFACE),
-                                  ("max_iterations", abi.TRK_MAX_ITER))}}
-            # per-surface errors against the fp64 oracle on a sample
-            sample = tracks.toy_tracks(3000, seed=args.seed + 99,
-                                       pt_range=(0.1, 100.0))
-            ref = ref_oracle.propagate(build_ref(), field.spec, cfg, sample)
-            got = host(propagator.propagate(
-                cfg, det, field,
-                torch.tensor(sample, dtype=dtype, device=dev), launch=lc))
-            sweep[key]["errors_vs_fp64_oracle"] = _errors_vs_oracle(ref, got)
-            del res
-    rows.append({"config": 5, "workload": "toy_4brl_7edc + "
-                 "wire_chamber_10l_cells, solenoid map, 2 x 8M muons "
-                 "eta -4..4 pT 0.1-100", "results": sweep})
+    # ---- config 5: toy + wire chamber, fp32 and fp64, 16 M tracks each
+    propagator.release_cache()
+    rows.append(config5_row(args, dev, oracle_errors=True))
     clk = clocks.stop()
     print(json.dumps({"sweep": rows, "clocks": clk}), flush=True)
 

@@ -121,42 +121,49 @@ struct record_sink {
     }
 };
 
-// The `count` staged records of staging row `row` written to the
-// slot-major arrays of `out` as track `track` (out.stage unset): the same
-// writes record_sink::write makes, so the results are those of writing
-// directly.
+// Staged record k of staging row `row` written to the slot-major arrays of
+// `out` as record k of track `track` (out.stage unset): the writes
+// record_sink::write makes, so the results are those of writing directly.
+template <typename S>
+DPROP_HD void unstage_record(const uint32_t* stage, uint64_t row, uint32_t k,
+                             uint64_t track, record_sink<S> out) {
+    constexpr int nw = staged_record_words<S>();
+    constexpr int ws = static_cast<int>(sizeof(S) / 4);
+    const uint4* src = reinterpret_cast<const uint4*>(
+        stage + (row * out.capacity + k) * static_cast<uint64_t>(nw));
+    uint32_t w[nw];
+    for (int i = 0; i < nw / 4; ++i) {
+#ifdef __CUDA_ARCH__
+        const uint4 v = __ldcs(src + i);
+#else
+        const uint4 v = src[i];
+#endif
+        w[4 * i] = v.x;
+        w[4 * i + 1] = v.y;
+        w[4 * i + 2] = v.z;
+        w[4 * i + 3] = v.w;
+    }
+    uint64_t bc;
+    S b[6], c[21], p;
+    memcpy(&bc, w, sizeof(bc));
+    memcpy(b, w + 2, 6 * sizeof(S));
+    memcpy(c, w + 2 + 6 * ws, 21 * sizeof(S));
+    memcpy(&p, w + 2 + 27 * ws, sizeof(S));
+    out.track = track;
+    out.stage = nullptr;
+    out.count = k;
+    out.write(bc, b, c, p, static_cast<uint8_t>(w[2 + 28 * ws]));
+}
+
+// The `count` staged records of staging row `row` (at most the capacity)
+// as records of track `track`.
 template <typename S>
 DPROP_HD void unstage_records(const uint32_t* stage, uint64_t row,
                               uint32_t count, uint64_t track,
                               record_sink<S> out) {
-    constexpr int nw = staged_record_words<S>();
-    constexpr int ws = static_cast<int>(sizeof(S) / 4);
     const uint32_t m = count < out.capacity ? count : out.capacity;
-    out.track = track;
-    out.stage = nullptr;
     for (uint32_t k = 0; k < m; ++k) {
-        const uint4* src = reinterpret_cast<const uint4*>(
-            stage + (row * out.capacity + k) * static_cast<uint64_t>(nw));
-        uint32_t w[nw];
-        for (int i = 0; i < nw / 4; ++i) {
-#ifdef __CUDA_ARCH__
-            const uint4 v = __ldcs(src + i);
-#else
-            const uint4 v = src[i];
-#endif
-            w[4 * i] = v.x;
-            w[4 * i + 1] = v.y;
-            w[4 * i + 2] = v.z;
-            w[4 * i + 3] = v.w;
-        }
-        uint64_t bc;
-        S b[6], c[21], p;
-        memcpy(&bc, w, sizeof(bc));
-        memcpy(b, w + 2, 6 * sizeof(S));
-        memcpy(c, w + 2 + 6 * ws, 21 * sizeof(S));
-        memcpy(&p, w + 2 + 27 * ws, sizeof(S));
-        out.count = k;
-        out.write(bc, b, c, p, static_cast<uint8_t>(w[2 + 28 * ws]));
+        unstage_record(stage, row, k, track, out);
     }
 }
 

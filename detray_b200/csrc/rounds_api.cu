@@ -420,8 +420,10 @@ __global__ void __launch_bounds__(k_phase_block, 8)
     }
 }
 
-// Staged records to the public slot-major arrays, one thread per input
-// track: consecutive threads write consecutive words of every array.
+// Staged records to the public slot-major arrays: thread (t, k) converts
+// record k of input track t (grid y strides over the record index), so
+// that every record is in flight at once and consecutive threads write
+// consecutive words of every array.
 template <typename In>
 __global__ void __launch_bounds__(k_phase_block)
     rounds_unstage_kernel(const __grid_constant__ prop_cfg<float> cfg,
@@ -429,12 +431,16 @@ __global__ void __launch_bounds__(k_phase_block)
                           const uint32_t* __restrict__ rec_count,
                           const uint32_t* __restrict__ inv,
                           const uint32_t* __restrict__ stage, uint64_t n) {
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) {
+        return;
+    }
     const record_sink<float> out = make_sink(io, n, cfg, nullptr);
-    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-         t < n; t += stride) {
-        const uint64_t slot = inv[t];
-        unstage_records<float>(stage, slot, rec_count[slot], t, out);
+    const uint64_t slot = inv[t];
+    const uint32_t c = rec_count[slot];
+    const uint32_t m = c < out.capacity ? c : out.capacity;
+    for (uint32_t k = blockIdx.y; k < m; k += gridDim.y) {
+        unstage_record<float>(stage, slot, k, t, out);
     }
 }
 
@@ -557,7 +563,11 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                 L.qs.pull, n, L.stage);
             DPROP_CUDA(cudaGetLastError());
             if (L.stage != nullptr) {
-                rounds_unstage_kernel<In><<<g_init, k_phase_block, 0, st>>>(
+                const dim3 ug(static_cast<unsigned int>(
+                                  (n + k_phase_block - 1) / k_phase_block),
+                              cfg.max_records < 65535u ? cfg.max_records
+                                                       : 65535u);
+                rounds_unstage_kernel<In><<<ug, k_phase_block, 0, st>>>(
                     cfg, io, L.slots.rec_count, L.inv, L.stage, n);
                 DPROP_CUDA(cudaGetLastError());
             }

@@ -35,7 +35,7 @@ ABI_SYMBOLS = [
     "dprop_field_destroy", "dprop_propagate", "dprop_propagate_host",
     "dprop_propagate_noalloc", "dprop_autotune", "dprop_propagate_adjoint",
     "dprop_backward", "dprop_propagate_direct", "dprop_helix_scan",
-    "dprop_validate_navigation",
+    "dprop_validate_navigation", "dprop_release_cache",
 ]
 
 
@@ -178,6 +178,12 @@ class Field:
             self.close()
         except Exception:
             pass
+
+
+def release_cache() -> None:
+    """Free the device memory the library keeps between calls (cached CUDA
+    graphs and grow-only scratch; dprop_release_cache)."""
+    _check(load_library().dprop_release_cache())
 
 
 def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,

@@ -582,6 +582,14 @@ dprop_status dprop_autotune(const dprop_config* cfg, const dprop_detector* det,
                             dprop_launch* launch, float* timings_ms,
                             void* stream);
 
+/* Frees the device memory the library keeps between calls: the cached CUDA
+ * graphs (use_graph) with the scratch each owns, and the grow-only scratch
+ * of the direction sort, the persistent method and the host-buffer entry
+ * points.  Synchronises the current device first; no propagate call may be
+ * running on another host thread.  Later calls allocate again on demand.
+ * Counterpart of releasing the vecmem buffers the reference's caller owns. */
+dprop_status dprop_release_cache(void);
+
 /* Number of surfaces / volumes held by a detector (for callers sizing output). */
 dprop_status dprop_detector_info(const dprop_detector* det, uint32_t* n_volumes,
                                  uint32_t* n_surfaces);

@@ -351,6 +351,18 @@ def test_graph_replay_and_autotune(torch_cuda):
     assert chosen in propagator.AUTOTUNE_CANDIDATES
     assert len(times) == len(propagator.AUTOTUNE_CANDIDATES)
     assert all(t > 0 for t in times)
+    # releasing the cached graphs and scratch: the next calls capture and
+    # allocate again and give the same results
+    propagator.release_cache()
+    for method in (abi.METHOD_PLAIN, abi.METHOD_PERSISTENT):
+        lc = propagator.make_launch(method=method, sort_tracks=1, use_graph=1)
+        res.tensors["status"].fill_(255)
+        propagator.propagate(cfg, det, field, dev, results=res, launch=lc)
+        torch_cuda.cuda.synchronize()
+        assert np.array_equal(a["status"], res.tensors["status"].cpu().numpy())
+        assert np.array_equal(a["path_length"],
+                              res.tensors["path_length"].cpu().numpy())
+    propagator.release_cache()
 
 
 def test_launch_shape_does_not_change_results(torch_cuda):
