@@ -272,7 +272,8 @@ class Launch(C.Structure):
         ("rounds", C.c_uint32),
         ("yield_lanes", C.c_uint32),
         ("sort_interval", C.c_uint32),
-        ("reserved", C.c_uint32 * 2),
+        ("tail_tracks", C.c_uint32),
+        ("reserved", C.c_uint32 * 1),
     ]
 
 

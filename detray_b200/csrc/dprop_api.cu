@@ -562,6 +562,10 @@ __global__ void clamp_counts_kernel(const uint32_t* __restrict__ n_rec,
 #ifndef DPROP_PIPE_SPLIT
 #define DPROP_PIPE_SPLIT 4u
 #endif
+// Chunks whose propagation may run at the same time (0: all in flight).
+#ifndef DPROP_PIPE_DEPTH
+#define DPROP_PIPE_DEPTH 0
+#endif
 
 struct record_arrays {
     uint64_t* barcode;
@@ -608,6 +612,7 @@ struct pipe_slot {
     cudaStream_t stream{nullptr};
     cudaEvent_t counted{nullptr};   // packed records and offsets ready
     cudaEvent_t drained{nullptr};   // packed records copied out
+    cudaEvent_t ran{nullptr};       // propagation and packing done
     void* dev{nullptr};
     size_t dev_bytes{0};
     uint32_t* host_offsets{nullptr};  // pinned, chunk + 1 entries
@@ -634,6 +639,7 @@ dprop_status ensure_pipe(pipe_slot& ps, int index, size_t dev_bytes,
         }
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.counted, cudaEventDisableTiming));
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.drained, cudaEventDisableTiming));
+        DPROP_CUDA(cudaEventCreateWithFlags(&ps.ran, cudaEventDisableTiming));
         // nothing to wait for before the first packing
         DPROP_CUDA(cudaEventRecord(ps.drained, g_copy_stream));
     }
@@ -863,17 +869,20 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         return DPROP_OK;
     };
 
-    // propagation, record packing and per-track outputs of one chunk.  The
-    // chunks run concurrently also with the persistent method: run one after
-    // the other, each would pay the method's per-round cost (the phase
-    // kernels' tails, the queue builds) once per chunk, which measured
-    // slower on B200 (1 M toy tracks in 4 chunks: 48.1 against 43.3 ms end
-    // to end) than letting the chunks' rounds interleave and the record
-    // copies follow.
+    // propagation, record packing and per-track outputs of one chunk; with
+    // a pipeline depth d, chunk k propagates after chunk k - d has
+    uint64_t n_run = 0;
+    int run_slot[k_pipe_slots] = {};
     auto stage_run = [&](uint64_t begin, uint64_t m, int sl) -> dprop_status {
         pipe_slot& ps = g_pipe[sl];
         const cudaStream_t st = ps.stream;
         const slot_buffers b = carve(sl);
+        constexpr int depth = DPROP_PIPE_DEPTH;
+        static_assert(depth < k_pipe_slots, "pipeline depth below the slots");
+        if (depth > 0 && n_run >= static_cast<uint64_t>(depth)) {
+            DPROP_CUDA(cudaStreamWaitEvent(
+                st, g_pipe[run_slot[(n_run - depth) % k_pipe_slots]].ran, 0));
+        }
         dprop_tracks dt{};
         for (int i = 0; i < 3; ++i) {
             dt.pos[i] = b.trk[i];
@@ -910,6 +919,9 @@ dprop_status propagate_host_jagged(const dprop_config& c,
                                                 b.offsets,
                                                 static_cast<uint32_t>(m));
         DPROP_CUDA(cudaGetLastError());
+        DPROP_CUDA(cudaEventRecord(ps.ran, st));
+        run_slot[n_run % k_pipe_slots] = sl;
+        ++n_run;
         // per-track outputs and the offsets back to the host
         auto d2h = [&](void* h, const void* d, size_t elem) -> dprop_status {
             if (h && d) {

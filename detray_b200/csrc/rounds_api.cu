@@ -82,9 +82,11 @@ __device__ __forceinline__ int queue_of(uint32_t pc, bool merged) {
 // phase kernels.
 struct queue_set {
     uint32_t* q[3];
-    uint32_t* count;   // [3]
+    uint32_t* count;   // [4]: queue lengths, [3] = 1 when the round runs the
+                       // remaining tracks to their end (merged)
     uint32_t* pull;    // [3]
-    uint32_t* tiles;   // [3 * n_tiles]
+    uint32_t* ticket;  // CTAs of the count kernel done
+    uint32_t* tiles;   // [3 * n_tiles]: counts, then the tiles' offsets
 };
 
 __device__ __forceinline__ void unpack16(uint4 v, uint32_t* b) {
@@ -130,10 +132,26 @@ __global__ void __launch_bounds__(k_build_threads)
     }
 }
 
-// Per-tile counts of the slots of each queue.
+// Block-wide exclusive sum of three counters per thread; returns the totals.
+__device__ void block_scan3(const uint32_t (&v)[3], uint32_t (&excl)[3],
+                            uint32_t (&total)[3]) {
+    using scan_t = cub::BlockScan<uint32_t, k_build_threads>;
+    __shared__ typename scan_t::TempStorage tmp;
+    for (int k = 0; k < 3; ++k) {
+        scan_t(tmp).ExclusiveSum(v[k], excl[k], total[k]);
+        __syncthreads();
+    }
+}
+
+// Per-tile counts of the slots of each queue.  The CTA that finishes last
+// (a ticket taken after a memory fence; no CTA waits for another) turns the
+// counts into the tiles' offsets, in place, and sets the queue lengths:
+// when fewer than tail_tracks tracks are alive (or merged is set: the last
+// round) every live track goes to queue 0 and the round runs them to their
+// end.
 __global__ void __launch_bounds__(k_build_threads)
     queue_count_kernel(const uint8_t* __restrict__ pc, queue_set qs,
-                       int merged) {
+                       uint32_t n_tiles, int merged, uint32_t tail_tracks) {
     if (blockIdx.x == 0 && threadIdx.x < 3) {
         qs.pull[threadIdx.x] = 0u;
     }
@@ -143,7 +161,7 @@ __global__ void __launch_bounds__(k_build_threads)
     unpack16(*reinterpret_cast<const uint4*>(pc + base), b);
     uint32_t c[3] = {0u, 0u, 0u};
     for (int i = 0; i < 16; ++i) {
-        const int q = queue_of(b[i], merged != 0);
+        const int q = queue_of(b[i], false);
         if (q >= 0) {
             ++c[q];
         }
@@ -166,39 +184,70 @@ __global__ void __launch_bounds__(k_build_threads)
         }
         qs.tiles[3u * blockIdx.x + threadIdx.x] = v;
     }
-}
-
-// Slots of each queue in slot order: the tile's offset is the sum of the
-// counts of the tiles before it, positions inside the tile come from a block
-// scan of the per-thread counts (three 21-bit fields of one 64-bit value).
-__global__ void __launch_bounds__(k_build_threads)
-    queue_scatter_kernel(const uint8_t* __restrict__ pc, queue_set qs,
-                         uint32_t n_tiles, int merged) {
-    const uint32_t tile = blockIdx.x;
-    uint32_t before[3] = {0u, 0u, 0u};
-    for (uint32_t j = threadIdx.x; j < tile; j += k_build_threads) {
-        for (int k = 0; k < 3; ++k) {
-            before[k] += qs.tiles[3u * j + k];
-        }
-    }
-    __shared__ uint32_t part[k_build_threads / 32][3];
-    __shared__ uint32_t offset[3];
-    for (int k = 0; k < 3; ++k) {
-        uint32_t v = before[k];
-        for (int o = 16; o > 0; o >>= 1) {
-            v += __shfl_down_sync(0xffffffffu, v, o);
-        }
-        if ((threadIdx.x & 31u) == 0u) {
-            part[threadIdx.x >> 5][k] = v;
-        }
+    // the last CTA to finish scans the tile counts
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(qs.ticket, 1u) == n_tiles - 1u;
     }
     __syncthreads();
-    if (threadIdx.x < 3) {
-        uint32_t v = 0u;
-        for (int w = 0; w < k_build_threads / 32; ++w) {
-            v += part[w][threadIdx.x];
+    if (!last) {
+        return;
+    }
+    __threadfence();
+    const uint32_t per = (n_tiles + k_build_threads - 1u) / k_build_threads;
+    const uint32_t lo = threadIdx.x * per;
+    const uint32_t hi = lo + per < n_tiles ? lo + per : n_tiles;
+    uint32_t sum[3] = {0u, 0u, 0u};
+    for (uint32_t j = lo; j < hi; ++j) {
+        for (int k = 0; k < 3; ++k) {
+            sum[k] += __ldcg(qs.tiles + 3u * j + k);
         }
-        offset[threadIdx.x] = v;
+    }
+    uint32_t excl[3], total[3];
+    block_scan3(sum, excl, total);
+    const uint32_t live = total[0] + total[1] + total[2];
+    const bool m = merged != 0 || live < tail_tracks;
+    // in place: each thread rewrites only its own tiles
+    uint32_t run[3] = {excl[0], excl[1], excl[2]};
+    uint32_t run_m = excl[0] + excl[1] + excl[2];
+    for (uint32_t j = lo; j < hi; ++j) {
+        uint32_t t[3];
+        for (int k = 0; k < 3; ++k) {
+            t[k] = __ldcg(qs.tiles + 3u * j + k);
+        }
+        if (m) {
+            qs.tiles[3u * j] = run_m;
+            qs.tiles[3u * j + 1] = 0u;
+            qs.tiles[3u * j + 2] = 0u;
+            run_m += t[0] + t[1] + t[2];
+        } else {
+            for (int k = 0; k < 3; ++k) {
+                qs.tiles[3u * j + k] = run[k];
+                run[k] += t[k];
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        qs.count[0] = m ? live : total[0];
+        qs.count[1] = m ? 0u : total[1];
+        qs.count[2] = m ? 0u : total[2];
+        qs.count[3] = m ? 1u : 0u;
+        *qs.ticket = 0u;
+    }
+}
+
+// Slots of each queue in slot order: the tile's offset comes from the count
+// kernel, positions inside the tile from a block scan of the per-thread
+// counts (three 21-bit fields of one 64-bit value).
+__global__ void __launch_bounds__(k_build_threads)
+    queue_scatter_kernel(const uint8_t* __restrict__ pc, queue_set qs) {
+    const uint32_t tile = blockIdx.x;
+    const bool m = qs.count[3] != 0u;
+    uint32_t offset[3];
+    for (int k = 0; k < 3; ++k) {
+        offset[k] = qs.tiles[3u * tile + k];
     }
     const uint64_t base = static_cast<uint64_t>(tile) * k_queue_tile +
                           static_cast<uint64_t>(threadIdx.x) * 16u;
@@ -206,7 +255,7 @@ __global__ void __launch_bounds__(k_build_threads)
     unpack16(*reinterpret_cast<const uint4*>(pc + base), b);
     uint64_t mine = 0u;
     for (int i = 0; i < 16; ++i) {
-        const int q = queue_of(b[i], merged != 0);
+        const int q = queue_of(b[i], m);
         if (q >= 0) {
             mine += uint64_t(1) << (21 * q);
         }
@@ -215,21 +264,15 @@ __global__ void __launch_bounds__(k_build_threads)
     __shared__ typename scan_t::TempStorage scan_tmp;
     uint64_t excl = 0u, total = 0u;
     scan_t(scan_tmp).ExclusiveSum(mine, excl, total);
-    __syncthreads();  // offset[] visible
     uint32_t pos[3];
     for (int k = 0; k < 3; ++k) {
         pos[k] = offset[k] + static_cast<uint32_t>((excl >> (21 * k)) & 0x1fffffu);
     }
     for (int i = 0; i < 16; ++i) {
-        const int q = queue_of(b[i], merged != 0);
+        const int q = queue_of(b[i], m);
         if (q >= 0) {
             qs.q[q][pos[q]++] = static_cast<uint32_t>(base + i);
         }
-    }
-    if (tile == n_tiles - 1u && threadIdx.x < 3) {
-        qs.count[threadIdx.x] =
-            offset[threadIdx.x] +
-            static_cast<uint32_t>((total >> (21 * threadIdx.x)) & 0x1fffffu);
     }
 }
 
@@ -329,6 +372,25 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
     const uint32_t cnt = *count;
     const unsigned lane = threadIdx.x & 31u;
     record_sink<float> rec = make_sink(io, n, cfg, stage);
+    if (count[3] != 0u) {
+        // few tracks left: run each to its end in this round (the queue
+        // builder merged all live tracks into this queue)
+        while (true) {
+            const uint32_t base = pull32(pull);
+            if (base >= cnt) {
+                break;
+            }
+            const uint32_t idx = base + lane;
+            if (idx < cnt) {
+                const uint64_t slot = queue[idx];
+                const track_outputs<float> o =
+                    phase_tail<float, W>(s, slot, det, field, cfg, rec);
+                write_outputs(io, s.track[slot], o);
+            }
+            __syncwarp();
+        }
+        return;
+    }
     while (true) {
         const uint32_t base = pull32(pull);
         if (base >= cnt) {
@@ -488,6 +550,7 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
     }
     qs.count = reinterpret_cast<uint32_t*>(p + off);
     qs.pull = qs.count + 4;
+    qs.ticket = qs.count + 8;
     off += 256;
     qs.tiles = reinterpret_cast<uint32_t*>(p + off);
     off += al256(3u * n_tiles * 4u);
@@ -536,7 +599,7 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                               const uint32_t* order, const rounds_layout& L,
                               uint32_t rounds, uint32_t step_budget,
                               uint32_t yield_lanes, uint32_t sort_interval,
-                              cudaStream_t st) {
+                              uint32_t tail_tracks, cudaStream_t st) {
     const uint64_t n_pad = L.n_tiles * k_queue_tile;
     const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
     unsigned int g_init = 0, g_fast = 0, g_nav = 0, g_tail = 0;
@@ -547,15 +610,16 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
         (s = resident_grid(rounds_tail_kernel<In, W>, &g_tail)) != DPROP_OK) {
         return s;
     }
+    DPROP_CUDA(cudaMemsetAsync(L.qs.ticket, 0, sizeof(uint32_t), st));
     rounds_init_kernel<In, W><<<g_init, k_phase_block, 0, st>>>(
         det, cfg, io, L.slots, n, n_pad, order, L.inv);
     DPROP_CUDA(cudaGetLastError());
     for (uint32_t r = 0; r <= rounds; ++r) {
         const int merged = (r == rounds) ? 1 : 0;
-        queue_count_kernel<<<tiles, k_build_threads, 0, st>>>(L.slots.pc, L.qs,
-                                                              merged);
-        queue_scatter_kernel<<<tiles, k_build_threads, 0, st>>>(
-            L.slots.pc, L.qs, tiles, merged);
+        queue_count_kernel<<<tiles, k_build_threads, 0, st>>>(
+            L.slots.pc, L.qs, tiles, merged, tail_tracks);
+        queue_scatter_kernel<<<tiles, k_build_threads, 0, st>>>(L.slots.pc,
+                                                                L.qs);
         DPROP_CUDA(cudaGetLastError());
         if (merged) {
             rounds_tail_kernel<In, W><<<g_tail, k_phase_block, 0, st>>>(
@@ -609,6 +673,8 @@ namespace dprop::api {
 constexpr uint32_t k_default_steps_per_round = 16u;
 constexpr uint32_t k_default_rounds = 64u;
 constexpr uint32_t k_default_yield_lanes = 16u;
+// default tail threshold: n / 64 live tracks
+constexpr uint64_t k_default_tail_div = 64u;
 
 size_t rounds_scratch_bytes(uint64_t n, bool wires, uint32_t rec_cap) {
     return rounds_layout_bytes(n, wires, rec_cap, nullptr, nullptr) + 256u;
@@ -642,6 +708,10 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
     const uint32_t yield = (lc && lc->yield_lanes) ? lc->yield_lanes
                                                    : k_default_yield_lanes;
     const uint32_t sort_interval = lc ? lc->sort_interval : 0u;
+    // live tracks below which a round runs the rest to their end
+    const uint32_t tail_tracks =
+        (lc && lc->tail_tracks) ? lc->tail_tracks
+                                : static_cast<uint32_t>(n / k_default_tail_div);
     if (rounds > 100000u || yield > 32u) {
         return fail(DPROP_E_INVALID,
                     "persistent method: rounds > 100000 or yield_lanes > 32");
@@ -662,12 +732,14 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
             return enqueue_rounds_w<In, true, FB>(det->view_as<true>(),
                                                   field->view, cfg, io, n,
                                                   order, L, rounds, budget,
-                                                  yield, sort_interval, stream);
+                                                  yield, sort_interval,
+                                                  tail_tracks, stream);
         }
         return enqueue_rounds_w<In, false, FB>(det->view_as<false>(),
                                                field->view, cfg, io, n, order,
                                                L, rounds, budget, yield,
-                                               sort_interval, stream);
+                                               sort_interval, tail_tracks,
+                                               stream);
     };
     if (fb == 3u) {
         return go(std::integral_constant<int, 3>{});

@@ -190,11 +190,13 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
                 ctas_per_sm: int = 0, sort_tracks: int = 0,
                 use_graph: int = 0, precision: int = 0,
                 steps_per_round: int = 0, rounds: int = 0,
-                yield_lanes: int = 0, sort_interval: int = 0) -> abi.Launch:
+                yield_lanes: int = 0, sort_interval: int = 0,
+                tail_tracks: int = 0) -> abi.Launch:
     """Launch shape; ``precision`` 8 runs the propagation in fp64 end to end
     (double track tensors and results).  steps_per_round, rounds,
-    yield_lanes and sort_interval shape the persistent (round-based) method;
-    0 picks the library default (sort_interval 0: no re-sort by volume)."""
+    yield_lanes, sort_interval and tail_tracks shape the persistent
+    (round-based) method; 0 picks the library default (sort_interval 0: no
+    re-sort by volume; tail_tracks 0: n / 64)."""
     lc = abi.Launch()
     lc.method = method
     lc.block_size = block_size
@@ -206,6 +208,7 @@ def make_launch(method: int = abi.METHOD_PLAIN, block_size: int = 0,
     lc.rounds = rounds
     lc.yield_lanes = yield_lanes
     lc.sort_interval = sort_interval
+    lc.tail_tracks = tail_tracks
     return lc
 
 

@@ -363,7 +363,11 @@ typedef struct dprop_launch {
     uint32_t sort_interval;      /* re-sort the live tracks of both phases by
                                     volume every sort_interval rounds (0:
                                     never, the default)                       */
-    uint32_t reserved[2];
+    uint32_t tail_tracks;        /* once fewer tracks than this are alive at
+                                    the start of a round, that round runs
+                                    them to their end (0: n_tracks / 64;
+                                    1: only after `rounds` rounds)            */
+    uint32_t reserved[1];
 } dprop_launch;
 
 /* ------------------------------------------------------------------ API */
