@@ -566,6 +566,18 @@ __global__ void clamp_counts_kernel(const uint32_t* __restrict__ n_rec,
 #ifndef DPROP_PIPE_DEPTH
 #define DPROP_PIPE_DEPTH 0
 #endif
+// Persistent method: chunk k + 1 starts its rounds once chunk k has run
+// this many rounds (0: all chunks start together).  Started together, the
+// chunks' rounds interleave and all chunks finish near the end of the batch,
+// so the record copies start late (1 M toy tracks in 4 chunks on B200: the
+// first chunk done after 21.8 ms, copies until 46.7 ms); started 16 rounds
+// apart, the first chunk's records cross PCIe while the later chunks
+// propagate in the earlier ones' tails (first chunk done after 16.5 ms,
+// copies until 39.8 ms).  One chunk after the other costs each chunk the
+// method's per-round latency (48 ms end to end).
+#ifndef DPROP_PIPE_STAGGER
+#define DPROP_PIPE_STAGGER 16
+#endif
 
 struct record_arrays {
     uint64_t* barcode;
@@ -613,6 +625,8 @@ struct pipe_slot {
     cudaEvent_t counted{nullptr};   // packed records and offsets ready
     cudaEvent_t drained{nullptr};   // packed records copied out
     cudaEvent_t ran{nullptr};       // propagation and packing done
+    cudaEvent_t mark{nullptr};      // persistent method: the chunk's rounds
+                                    // reached DPROP_PIPE_STAGGER
     void* dev{nullptr};
     size_t dev_bytes{0};
     uint32_t* host_offsets{nullptr};  // pinned, chunk + 1 entries
@@ -640,6 +654,7 @@ dprop_status ensure_pipe(pipe_slot& ps, int index, size_t dev_bytes,
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.counted, cudaEventDisableTiming));
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.drained, cudaEventDisableTiming));
         DPROP_CUDA(cudaEventCreateWithFlags(&ps.ran, cudaEventDisableTiming));
+        DPROP_CUDA(cudaEventCreateWithFlags(&ps.mark, cudaEventDisableTiming));
         // nothing to wait for before the first packing
         DPROP_CUDA(cudaEventRecord(ps.drained, g_copy_stream));
     }
@@ -870,7 +885,9 @@ dprop_status propagate_host_jagged(const dprop_config& c,
     };
 
     // propagation, record packing and per-track outputs of one chunk; with
-    // a pipeline depth d, chunk k propagates after chunk k - d has
+    // a pipeline depth d, chunk k propagates after chunk k - d has; with
+    // the persistent method chunk k starts DPROP_PIPE_STAGGER rounds after
+    // chunk k - 1
     uint64_t n_run = 0;
     int run_slot[k_pipe_slots] = {};
     auto stage_run = [&](uint64_t begin, uint64_t m, int sl) -> dprop_status {
@@ -892,9 +909,15 @@ dprop_status propagate_host_jagged(const dprop_config& c,
         dt.qop = b.trk[7];
         const io_ptrs<double> io = make_io<double>(dt, b.dr);
         if (rounds) {
+            constexpr uint32_t stagger = DPROP_PIPE_STAGGER;
+            if (stagger > 0u && n_run > 0u) {
+                DPROP_CUDA(cudaStreamWaitEvent(
+                    st, g_pipe[run_slot[(n_run - 1) % k_pipe_slots]].mark, 0));
+            }
             const dprop_status s = dprop::api::enqueue_rounds<double>(
                 lc, det, field, pcfg, io, m, sort ? b.idx_out : nullptr,
-                rounds_scratch(sl), rounds_bytes, st);
+                rounds_scratch(sl), rounds_bytes, st,
+                stagger > 0u ? ps.mark : nullptr, stagger);
             if (s != DPROP_OK) return s;
         } else {
             const dprop_status s = launch_plain<double>(

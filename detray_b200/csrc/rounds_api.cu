@@ -599,7 +599,8 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                               const uint32_t* order, const rounds_layout& L,
                               uint32_t rounds, uint32_t step_budget,
                               uint32_t yield_lanes, uint32_t sort_interval,
-                              uint32_t tail_tracks, cudaStream_t st) {
+                              uint32_t tail_tracks, cudaStream_t st,
+                              cudaEvent_t mark, uint32_t mark_round) {
     const uint64_t n_pad = L.n_tiles * k_queue_tile;
     const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
     unsigned int g_init = 0, g_fast = 0, g_nav = 0, g_tail = 0;
@@ -662,6 +663,12 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
         rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
             det, cfg, L.slots, q_nav, L.qs.count + 2, L.qs.pull + 2);
         DPROP_CUDA(cudaGetLastError());
+        if (mark && r == mark_round) {
+            DPROP_CUDA(cudaEventRecord(mark, st));
+        }
+    }
+    if (mark && mark_round >= rounds) {
+        DPROP_CUDA(cudaEventRecord(mark, st));
     }
     return DPROP_OK;
 }
@@ -685,7 +692,8 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                             const dprop_field* field,
                             const prop_cfg<float>& cfg, const io_ptrs<In>& io,
                             uint64_t n, const uint32_t* order, void* scratch,
-                            size_t scratch_bytes, cudaStream_t stream) {
+                            size_t scratch_bytes, cudaStream_t stream,
+                            cudaEvent_t mark, uint32_t mark_round) {
     if (n > 0x7fffffffull) {
         return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
     }
@@ -733,13 +741,14 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                                                   field->view, cfg, io, n,
                                                   order, L, rounds, budget,
                                                   yield, sort_interval,
-                                                  tail_tracks, stream);
+                                                  tail_tracks, stream, mark,
+                                                  mark_round);
         }
         return enqueue_rounds_w<In, false, FB>(det->view_as<false>(),
                                                field->view, cfg, io, n, order,
                                                L, rounds, budget, yield,
                                                sort_interval, tail_tracks,
-                                               stream);
+                                               stream, mark, mark_round);
     };
     if (fb == 3u) {
         return go(std::integral_constant<int, 3>{});
@@ -756,13 +765,15 @@ template dprop_status enqueue_rounds<float>(const dprop_launch*,
                                             const prop_cfg<float>&,
                                             const io_ptrs<float>&, uint64_t,
                                             const uint32_t*, void*, size_t,
-                                            cudaStream_t);
+                                            cudaStream_t, cudaEvent_t,
+                                            uint32_t);
 template dprop_status enqueue_rounds<double>(const dprop_launch*,
                                              const dprop_detector*,
                                              const dprop_field*,
                                              const prop_cfg<float>&,
                                              const io_ptrs<double>&, uint64_t,
                                              const uint32_t*, void*, size_t,
-                                             cudaStream_t);
+                                             cudaStream_t, cudaEvent_t,
+                                             uint32_t);
 
 }  // namespace dprop::api

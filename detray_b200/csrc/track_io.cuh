@@ -137,11 +137,16 @@ uint32_t staged_capacity(const prop_cfg<S>& cfg, const io_ptrs<In>& io) {
     return io.rec_barcode != nullptr ? cfg.max_records : 0u;
 }
 
+// mark: optional event recorded on the stream after round mark_round's
+// phase kernels (a later propagation can start then, in the tail of this
+// one); NULL: none.
 template <typename In>
 dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                             const dprop_field* field,
                             const prop_cfg<float>& cfg, const io_ptrs<In>& io,
                             uint64_t n, const uint32_t* order, void* scratch,
-                            size_t scratch_bytes, cudaStream_t stream);
+                            size_t scratch_bytes, cudaStream_t stream,
+                            cudaEvent_t mark = nullptr,
+                            uint32_t mark_round = 0u);
 
 }  // namespace dprop::api
