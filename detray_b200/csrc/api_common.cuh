@@ -69,8 +69,10 @@ struct dprop_detector {
     // material maps or volume material: launches use the kernels that
     // include the code for them
     bool wires{false};
-    dprop::detector_view<double> view_d() const {
-        dprop::detector_view<double> v;
+    dprop::detector_view<double> view_d() const { return view_d_as<true>(); }
+    template <bool W>
+    dprop::detector_view<double, W> view_d_as() const {
+        dprop::detector_view<double, W> v;
         v.volumes = volumes;
         v.surfaces = surfaces;
         v.masks = masks_d;
@@ -119,5 +121,8 @@ dprop_status propagate_fp64(const dprop_config& cfg, const dprop_launch* lc,
                             const dprop_tracks& tracks,
                             const dprop_results& results, uint64_t n,
                             cudaStream_t stream);
+
+// Frees the grow-only scratch of fp64 launches (dprop_release_cache).
+void release_fp64_scratch();
 
 }  // namespace dprop::api

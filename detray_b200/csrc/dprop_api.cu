@@ -1524,6 +1524,7 @@ dprop_status dprop_release_cache(void) {
         g_pipe[k].dev = nullptr;
         g_pipe[k].dev_bytes = 0;
     }
+    dprop::api::release_fp64_scratch();
     return DPROP_OK;
 }
 

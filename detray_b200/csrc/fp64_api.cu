@@ -4,10 +4,12 @@
 // and results are double; the field map nodes stay float4 (the reference's
 // covfie field stores floats) and are interpolated in double.
 //
-// Kernel:
+// Kernels:
 //   propagate_fp64_kernel<MB>  one thread per track, the whole propagation,
 //                              register budget MB resident CTAs of 128
 //                              threads per SM (8: 64 registers, 12: 40)
+//   the round-based phase kernels of rounds_api.cu in double
+//                              (dprop_launch.method = DPROP_METHOD_PERSISTENT)
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -46,7 +48,26 @@ struct f64_sort_scratch {
     int device{-1};
 };
 f64_sort_scratch g_f64_sort;
+f64_sort_scratch g_f64_rounds;  // persistent method: slots and queues
 std::mutex g_f64_mutex;
+
+dprop_status ensure_f64(f64_sort_scratch& sc, size_t need,
+                        cudaStream_t stream) {
+    int dev = 0;
+    DPROP_CUDA(cudaGetDevice(&dev));
+    if (sc.bytes < need || sc.device != dev) {
+        if (sc.buf) {
+            DPROP_CUDA(cudaStreamSynchronize(stream));
+            cudaFree(sc.buf);
+            sc.buf = nullptr;
+            sc.bytes = 0;
+        }
+        DPROP_CUDA(cudaMalloc(&sc.buf, need));
+        sc.bytes = need;
+        sc.device = dev;
+    }
+    return DPROP_OK;
+}
 
 }  // namespace
 
@@ -64,19 +85,10 @@ dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
     std::lock_guard<std::mutex> lock(g_f64_mutex);
     const uint32_t* order = nullptr;
     if (lc && lc->sort_tracks) {
-        const size_t need = sort_scratch_bytes(n);
-        int dev = 0;
-        DPROP_CUDA(cudaGetDevice(&dev));
-        if (g_f64_sort.bytes < need || g_f64_sort.device != dev) {
-            if (g_f64_sort.buf) {
-                DPROP_CUDA(cudaStreamSynchronize(stream));
-                cudaFree(g_f64_sort.buf);
-                g_f64_sort.buf = nullptr;
-                g_f64_sort.bytes = 0;
-            }
-            DPROP_CUDA(cudaMalloc(&g_f64_sort.buf, need));
-            g_f64_sort.bytes = need;
-            g_f64_sort.device = dev;
+        const dprop_status e =
+            ensure_f64(g_f64_sort, sort_scratch_bytes(n), stream);
+        if (e != DPROP_OK) {
+            return e;
         }
         const dprop_status s = enqueue_direction_sort(
             io.trk[4], io.trk[5], io.trk[6], io.trk[7], n, g_f64_sort.buf,
@@ -86,6 +98,17 @@ dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
         }
     }
     const prop_cfg<double> pc = make_prop_cfg<double>(c);
+    if (lc && lc->method == DPROP_METHOD_PERSISTENT) {
+        const size_t need = rounds_scratch_bytes_fp64(
+            n, det->wires, staged_capacity(pc, io));
+        const dprop_status e = ensure_f64(g_f64_rounds, need, stream);
+        if (e != DPROP_OK) {
+            return e;
+        }
+        return enqueue_rounds_fp64(lc, det, field, pc, io, n, order,
+                                   g_f64_rounds.buf, g_f64_rounds.bytes,
+                                   stream);
+    }
     const unsigned int grid =
         static_cast<unsigned int>((n + k_f64_block - 1) / k_f64_block);
     if (c.use_field_gradient) {
@@ -100,6 +123,14 @@ dprop_status propagate_fp64(const dprop_config& c, const dprop_launch* lc,
     }
     DPROP_CUDA(cudaGetLastError());
     return DPROP_OK;
+}
+
+void release_fp64_scratch() {
+    std::lock_guard<std::mutex> lock(g_f64_mutex);
+    for (f64_sort_scratch* sc : {&g_f64_sort, &g_f64_rounds}) {
+        cudaFree(sc->buf);
+        *sc = f64_sort_scratch{};
+    }
 }
 
 }  // namespace dprop::api

@@ -101,10 +101,11 @@ __device__ __forceinline__ void unpack16(uint4 v, uint32_t* b) {
 // Sort key of each queue entry: the volume the track's next phase works in
 // (for a track on a portal in the navigation queue, the volume the portal
 // leads to), 0xff past the queue's end.
+template <typename S>
 __global__ void __launch_bounds__(k_build_threads)
     queue_key_kernel(const uint32_t* __restrict__ q,
                      const uint32_t* __restrict__ count,
-                     const __grid_constant__ slot_soa<float> s,
+                     const __grid_constant__ slot_soa<S> s,
                      uint8_t* __restrict__ keys, uint64_t n, int nav_queue) {
     const uint32_t cnt = *count;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(k_build_threads)
             const int next = static_cast<int>(nb & 0xffu);
             const int8_t status = static_cast<int8_t>((nb >> 16) & 0xffu);
             if (status == e_on_portal && next >= 1 && next <= k_cache + 1) {
-                candidate<float> c;
+                candidate<S> c;
                 load_cand(s, slot, next - 1, c);
                 if (c.volume_link != static_cast<uint16_t>(k_invalid_link)) {
                     vol = c.volume_link;
@@ -276,11 +277,11 @@ __global__ void __launch_bounds__(k_build_threads)
     }
 }
 
-template <typename In>
-__device__ __forceinline__ record_sink<float> make_sink(
-    const api::io_ptrs<In>& io, uint64_t n, const prop_cfg<float>& cfg,
+template <typename S, typename In>
+__device__ __forceinline__ record_sink<S> make_sink(
+    const api::io_ptrs<In, S>& io, uint64_t n, const prop_cfg<S>& cfg,
     uint32_t* stage) {
-    record_sink<float> rec;
+    record_sink<S> rec;
     rec.barcode = io.rec_barcode;
     rec.bound = io.rec_bound;
     rec.cov = io.rec_cov;
@@ -294,10 +295,10 @@ __device__ __forceinline__ record_sink<float> make_sink(
     return rec;
 }
 
-template <typename In>
-__device__ __forceinline__ void write_outputs(const api::io_ptrs<In>& io,
+template <typename S, typename In>
+__device__ __forceinline__ void write_outputs(const api::io_ptrs<In, S>& io,
                                               uint64_t t,
-                                              const track_outputs<float>& o) {
+                                              const track_outputs<S>& o) {
     if (io.status) io.status[t] = o.status;
     if (io.n_records) io.n_records[t] = o.n_records;
     if (io.n_steps) io.n_steps[t] = o.n_steps;
@@ -323,12 +324,12 @@ __device__ __forceinline__ uint32_t pull32(uint32_t* pull) {
 // Propagation start of every slot; pads the next-segment array to whole
 // tiles with ended slots.  inv (with staged records) receives the slot of
 // each input track.
-template <typename In, bool W>
+template <typename S, typename In, bool W>
 __global__ void __launch_bounds__(k_phase_block)
-    rounds_init_kernel(const __grid_constant__ detector_view<float, W> det,
-                       const __grid_constant__ prop_cfg<float> cfg,
-                       const __grid_constant__ api::io_ptrs<In> io,
-                       const __grid_constant__ slot_soa<float> s, uint64_t n,
+    rounds_init_kernel(const __grid_constant__ detector_view<S, W> det,
+                       const __grid_constant__ prop_cfg<S> cfg,
+                       const __grid_constant__ api::io_ptrs<In, S> io,
+                       const __grid_constant__ slot_soa<S> s, uint64_t n,
                        uint64_t n_pad, const uint32_t* __restrict__ order,
                        uint32_t* __restrict__ inv) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -342,15 +343,15 @@ __global__ void __launch_bounds__(k_phase_block)
         if (inv) {
             inv[t] = static_cast<uint32_t>(slot);
         }
-        const vec3<float> pos{static_cast<float>(io.trk[0][t]),
-                              static_cast<float>(io.trk[1][t]),
-                              static_cast<float>(io.trk[2][t])};
-        const vec3<float> dir{static_cast<float>(io.trk[4][t]),
-                              static_cast<float>(io.trk[5][t]),
-                              static_cast<float>(io.trk[6][t])};
-        phase_init<float, W>(s, slot, static_cast<uint32_t>(t), pos,
-                             static_cast<float>(io.trk[3][t]), dir,
-                             static_cast<float>(io.trk[7][t]), det, cfg);
+        const vec3<S> pos{static_cast<S>(io.trk[0][t]),
+                              static_cast<S>(io.trk[1][t]),
+                              static_cast<S>(io.trk[2][t])};
+        const vec3<S> dir{static_cast<S>(io.trk[4][t]),
+                              static_cast<S>(io.trk[5][t]),
+                              static_cast<S>(io.trk[6][t])};
+        phase_init<S, W>(s, slot, static_cast<uint32_t>(t), pos,
+                             static_cast<S>(io.trk[3][t]), dir,
+                             static_cast<S>(io.trk[7][t]), det, cfg);
     }
 }
 
@@ -358,20 +359,20 @@ __global__ void __launch_bounds__(k_phase_block)
 // registers: the state and the step's temporaries fit without spills), 4
 // (128) or 5 (102).  The best budget depends on the workload (more warps
 // hide the field map's gather latency), so it is a launch choice.
-template <typename In, bool W, int MinBlocks>
+template <typename S, typename In, bool W, int MinBlocks>
 __global__ void __launch_bounds__(k_phase_block, MinBlocks)
-    rounds_fast_kernel(const __grid_constant__ detector_view<float, W> det,
-                       const __grid_constant__ field_view<float> field,
-                       const __grid_constant__ prop_cfg<float> cfg,
-                       const __grid_constant__ api::io_ptrs<In> io,
-                       const __grid_constant__ slot_soa<float> s,
+    rounds_fast_kernel(const __grid_constant__ detector_view<S, W> det,
+                       const __grid_constant__ field_view<S> field,
+                       const __grid_constant__ prop_cfg<S> cfg,
+                       const __grid_constant__ api::io_ptrs<In, S> io,
+                       const __grid_constant__ slot_soa<S> s,
                        const uint32_t* __restrict__ queue,
                        const uint32_t* __restrict__ count, uint32_t* pull,
                        uint64_t n, uint32_t step_budget, uint32_t yield_lanes,
                        uint32_t* stage) {
     const uint32_t cnt = *count;
     const unsigned lane = threadIdx.x & 31u;
-    record_sink<float> rec = make_sink(io, n, cfg, stage);
+    record_sink<S> rec = make_sink(io, n, cfg, stage);
     if (count[3] != 0u) {
         // few tracks left: run each to its end in this round (the queue
         // builder merged all live tracks into this queue)
@@ -383,8 +384,8 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
             const uint32_t idx = base + lane;
             if (idx < cnt) {
                 const uint64_t slot = queue[idx];
-                const track_outputs<float> o =
-                    phase_tail<float, W>(s, slot, det, field, cfg, rec);
+                const track_outputs<S> o =
+                    phase_tail<S, W>(s, slot, det, field, cfg, rec);
                 write_outputs(io, s.track[slot], o);
             }
             __syncwarp();
@@ -399,19 +400,19 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
         const uint32_t idx = base + lane;
         const bool valid = idx < cnt;
         const uint64_t slot = valid ? queue[idx] : 0u;
-        nav_cache<float> cache;
-        track_state<float> ts;
+        nav_cache<S> cache;
+        track_state<S> ts;
         bind_cache(ts.nav, cache);
-        loop_state<float> ls;
+        loop_state<S> ls;
         cand_window win;
         if (valid) {
-            fast_load<float, W>(s, slot, ts, ls, win);
+            fast_load<S, W>(s, slot, ts, ls, win);
         }
         const int n_valid = __popc(__ballot_sync(0xffffffffu, valid));
         bool active = valid;
         for (uint32_t it = 0;; ++it) {
             if (active) {
-                const uint8_t pc = fast_advance<float, W>(
+                const uint8_t pc = fast_advance<S, W>(
                     ts, ls, win, s, slot, det, field, cfg, rec);
                 active = machine_is_fast(pc);
             }
@@ -422,7 +423,7 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
             }
         }
         if (valid) {
-            fast_store<float, W>(s, slot, ts, ls, win);
+            fast_store<S, W>(s, slot, ts, ls, win);
             if (ls.pc == pc_done) {
                 write_outputs(io, s.track[slot],
                               fast_outputs(s, slot, ts, ls));
@@ -432,11 +433,11 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
 }
 
 // The navigation update's volume-level part.
-template <bool W>
+template <typename S, bool W>
 __global__ void __launch_bounds__(k_phase_block, 4)
-    rounds_nav_kernel(const __grid_constant__ detector_view<float, W> det,
-                      const __grid_constant__ prop_cfg<float> cfg,
-                      const __grid_constant__ slot_soa<float> s,
+    rounds_nav_kernel(const __grid_constant__ detector_view<S, W> det,
+                      const __grid_constant__ prop_cfg<S> cfg,
+                      const __grid_constant__ slot_soa<S> s,
                       const uint32_t* __restrict__ queue,
                       const uint32_t* __restrict__ count, uint32_t* pull) {
     const uint32_t cnt = *count;
@@ -447,25 +448,25 @@ __global__ void __launch_bounds__(k_phase_block, 4)
         }
         const uint32_t idx = base + (threadIdx.x & 31u);
         if (idx < cnt) {
-            phase_nav<float, W>(s, queue[idx], det, cfg);
+            phase_nav<S, W>(s, queue[idx], det, cfg);
         }
         __syncwarp();
     }
 }
 
 // The tracks still alive after the last round, every segment inline.
-template <typename In, bool W>
+template <typename S, typename In, bool W>
 __global__ void __launch_bounds__(k_phase_block, 8)
-    rounds_tail_kernel(const __grid_constant__ detector_view<float, W> det,
-                       const __grid_constant__ field_view<float> field,
-                       const __grid_constant__ prop_cfg<float> cfg,
-                       const __grid_constant__ api::io_ptrs<In> io,
-                       const __grid_constant__ slot_soa<float> s,
+    rounds_tail_kernel(const __grid_constant__ detector_view<S, W> det,
+                       const __grid_constant__ field_view<S> field,
+                       const __grid_constant__ prop_cfg<S> cfg,
+                       const __grid_constant__ api::io_ptrs<In, S> io,
+                       const __grid_constant__ slot_soa<S> s,
                        const uint32_t* __restrict__ queue,
                        const uint32_t* __restrict__ count, uint32_t* pull,
                        uint64_t n, uint32_t* stage) {
     const uint32_t cnt = *count;
-    record_sink<float> rec = make_sink(io, n, cfg, stage);
+    record_sink<S> rec = make_sink(io, n, cfg, stage);
     while (true) {
         const uint32_t base = pull32(pull);
         if (base >= cnt) {
@@ -474,8 +475,8 @@ __global__ void __launch_bounds__(k_phase_block, 8)
         const uint32_t idx = base + (threadIdx.x & 31u);
         if (idx < cnt) {
             const uint64_t slot = queue[idx];
-            const track_outputs<float> o =
-                phase_tail<float, W>(s, slot, det, field, cfg, rec);
+            const track_outputs<S> o =
+                phase_tail<S, W>(s, slot, det, field, cfg, rec);
             write_outputs(io, s.track[slot], o);
         }
         __syncwarp();
@@ -486,10 +487,10 @@ __global__ void __launch_bounds__(k_phase_block, 8)
 // record k of input track t (grid y strides over the record index), so
 // that every record is in flight at once and consecutive threads write
 // consecutive words of every array.
-template <typename In>
+template <typename S, typename In>
 __global__ void __launch_bounds__(k_phase_block)
-    rounds_unstage_kernel(const __grid_constant__ prop_cfg<float> cfg,
-                          const __grid_constant__ api::io_ptrs<In> io,
+    rounds_unstage_kernel(const __grid_constant__ prop_cfg<S> cfg,
+                          const __grid_constant__ api::io_ptrs<In, S> io,
                           const uint32_t* __restrict__ rec_count,
                           const uint32_t* __restrict__ inv,
                           const uint32_t* __restrict__ stage, uint64_t n) {
@@ -497,12 +498,12 @@ __global__ void __launch_bounds__(k_phase_block)
     if (t >= n) {
         return;
     }
-    const record_sink<float> out = make_sink(io, n, cfg, nullptr);
+    const record_sink<S> out = make_sink(io, n, cfg, nullptr);
     const uint64_t slot = inv[t];
     const uint32_t c = rec_count[slot];
     const uint32_t m = c < out.capacity ? c : out.capacity;
     for (uint32_t k = blockIdx.y; k < m; k += gridDim.y) {
-        unstage_record<float>(stage, slot, k, t, out);
+        unstage_record<S>(stage, slot, k, t, out);
     }
 }
 
@@ -519,8 +520,9 @@ dprop_status resident_grid(K kernel, unsigned int* grid) {
     return DPROP_OK;
 }
 
+template <typename S>
 struct rounds_layout {
-    slot_soa<float> slots;
+    slot_soa<S> slots;
     queue_set qs;
     uint64_t n_tiles;
     uint8_t* keys[2];        // volume re-sort: keys in, keys out
@@ -536,11 +538,12 @@ size_t al256(size_t b) { return (b + 255u) & ~size_t(255u); }
 
 // Scratch layout: slot arrays, three queues, counters and tile counts, and
 // with rec_cap > 0 the record staging area and the input -> slot map.
+template <typename S>
 size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
-                           rounds_layout* out, void* base) {
+                           rounds_layout<S>* out, void* base) {
     const uint64_t n_tiles = queue_tiles(n);
-    slot_soa<float> s{};
-    const size_t slot_bytes = carve_slots<float>(base, n, wires, &s);
+    slot_soa<S> s{};
+    const size_t slot_bytes = carve_slots<S>(base, n, wires, &s);
     size_t off = al256(slot_bytes);
     char* p = static_cast<char*>(base);
     queue_set qs{};
@@ -574,7 +577,7 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
         inv = reinterpret_cast<uint32_t*>(p + off);
         off += al256(n * 4u);
         stage = reinterpret_cast<uint32_t*>(p + off);
-        off += al256(n * rec_cap * (4u * staged_record_words<float>()));
+        off += al256(n * rec_cap * (4u * staged_record_words<S>()));
     }
     if (out) {
         out->slots = s;
@@ -591,12 +594,12 @@ size_t rounds_layout_bytes(uint64_t n, bool wires, uint32_t rec_cap,
     return off;
 }
 
-template <typename In, bool W, int FastBlocks>
-dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
-                              const field_view<float>& field,
-                              const prop_cfg<float>& cfg,
-                              const api::io_ptrs<In>& io, uint64_t n,
-                              const uint32_t* order, const rounds_layout& L,
+template <typename S, typename In, bool W, int FastBlocks>
+dprop_status enqueue_rounds_w(const detector_view<S, W>& det,
+                              const field_view<S>& field,
+                              const prop_cfg<S>& cfg,
+                              const api::io_ptrs<In, S>& io, uint64_t n,
+                              const uint32_t* order, const rounds_layout<S>& L,
                               uint32_t rounds, uint32_t step_budget,
                               uint32_t yield_lanes, uint32_t sort_interval,
                               uint32_t tail_tracks, cudaStream_t st,
@@ -605,14 +608,14 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
     const unsigned int tiles = static_cast<unsigned int>(L.n_tiles);
     unsigned int g_init = 0, g_fast = 0, g_nav = 0, g_tail = 0;
     dprop_status s = DPROP_OK;
-    if ((s = resident_grid(rounds_init_kernel<In, W>, &g_init)) != DPROP_OK ||
-        (s = resident_grid(rounds_fast_kernel<In, W, FastBlocks>, &g_fast)) != DPROP_OK ||
-        (s = resident_grid(rounds_nav_kernel<W>, &g_nav)) != DPROP_OK ||
-        (s = resident_grid(rounds_tail_kernel<In, W>, &g_tail)) != DPROP_OK) {
+    if ((s = resident_grid(rounds_init_kernel<S, In, W>, &g_init)) != DPROP_OK ||
+        (s = resident_grid(rounds_fast_kernel<S, In, W, FastBlocks>, &g_fast)) != DPROP_OK ||
+        (s = resident_grid(rounds_nav_kernel<S, W>, &g_nav)) != DPROP_OK ||
+        (s = resident_grid(rounds_tail_kernel<S, In, W>, &g_tail)) != DPROP_OK) {
         return s;
     }
     DPROP_CUDA(cudaMemsetAsync(L.qs.ticket, 0, sizeof(uint32_t), st));
-    rounds_init_kernel<In, W><<<g_init, k_phase_block, 0, st>>>(
+    rounds_init_kernel<S, In, W><<<g_init, k_phase_block, 0, st>>>(
         det, cfg, io, L.slots, n, n_pad, order, L.inv);
     DPROP_CUDA(cudaGetLastError());
     for (uint32_t r = 0; r <= rounds; ++r) {
@@ -623,7 +626,7 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                                                                 L.qs);
         DPROP_CUDA(cudaGetLastError());
         if (merged) {
-            rounds_tail_kernel<In, W><<<g_tail, k_phase_block, 0, st>>>(
+            rounds_tail_kernel<S, In, W><<<g_tail, k_phase_block, 0, st>>>(
                 det, field, cfg, io, L.slots, L.qs.q[0], L.qs.count,
                 L.qs.pull, n, L.stage);
             DPROP_CUDA(cudaGetLastError());
@@ -632,7 +635,7 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
                                   (n + k_phase_block - 1) / k_phase_block),
                               cfg.max_records < 65535u ? cfg.max_records
                                                        : 65535u);
-                rounds_unstage_kernel<In><<<ug, k_phase_block, 0, st>>>(
+                rounds_unstage_kernel<S, In><<<ug, k_phase_block, 0, st>>>(
                     cfg, io, L.slots.rec_count, L.inv, L.stage, n);
                 DPROP_CUDA(cudaGetLastError());
             }
@@ -646,7 +649,7 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
             for (int k = 0; k < 2; ++k) {
                 const int qi = 2 * k;  // step queue 0, navigation queue 2
                 uint32_t* dst = k == 0 ? L.qs.q[1] : L.nav_sorted;
-                queue_key_kernel<<<kg, k_build_threads, 0, st>>>(
+                queue_key_kernel<S><<<kg, k_build_threads, 0, st>>>(
                     L.qs.q[qi], L.qs.count + qi, L.slots, L.keys[0], n, k);
                 DPROP_CUDA(cudaGetLastError());
                 size_t tb = L.sort_temp_bytes;
@@ -657,10 +660,10 @@ dprop_status enqueue_rounds_w(const detector_view<float, W>& det,
             q_fast = L.qs.q[1];
             q_nav = L.nav_sorted;
         }
-        rounds_fast_kernel<In, W, FastBlocks><<<g_fast, k_phase_block, 0, st>>>(
+        rounds_fast_kernel<S, In, W, FastBlocks><<<g_fast, k_phase_block, 0, st>>>(
             det, field, cfg, io, L.slots, q_fast, L.qs.count, L.qs.pull, n,
             step_budget, yield_lanes, L.stage);
-        rounds_nav_kernel<W><<<g_nav, k_phase_block, 0, st>>>(
+        rounds_nav_kernel<S, W><<<g_nav, k_phase_block, 0, st>>>(
             det, cfg, L.slots, q_nav, L.qs.count + 2, L.qs.pull + 2);
         DPROP_CUDA(cudaGetLastError());
         if (mark && r == mark_round) {
@@ -684,16 +687,48 @@ constexpr uint32_t k_default_yield_lanes = 16u;
 constexpr uint64_t k_default_tail_div = 64u;
 
 size_t rounds_scratch_bytes(uint64_t n, bool wires, uint32_t rec_cap) {
-    return rounds_layout_bytes(n, wires, rec_cap, nullptr, nullptr) + 256u;
+    return rounds_layout_bytes<float>(n, wires, rec_cap, nullptr, nullptr) +
+           256u;
 }
 
-template <typename In>
-dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
-                            const dprop_field* field,
-                            const prop_cfg<float>& cfg, const io_ptrs<In>& io,
-                            uint64_t n, const uint32_t* order, void* scratch,
-                            size_t scratch_bytes, cudaStream_t stream,
-                            cudaEvent_t mark, uint32_t mark_round) {
+size_t rounds_scratch_bytes_fp64(uint64_t n, bool wires, uint32_t rec_cap) {
+    return rounds_layout_bytes<double>(n, wires, rec_cap, nullptr, nullptr) +
+           256u;
+}
+
+namespace {
+
+// The detector and field views in the arithmetic type S.
+template <typename S, bool W>
+detector_view<S, W> det_view(const dprop_detector* det) {
+    if constexpr (sizeof(S) == 8) {
+        return det->view_d_as<W>();
+    } else {
+        return det->view_as<W>();
+    }
+}
+
+template <typename S>
+const field_view<S>& fld_view(const dprop_field* field) {
+    if constexpr (sizeof(S) == 8) {
+        return field->view_d;
+    } else {
+        return field->view;
+    }
+}
+
+// The round-based propagation in S; the step phase's register budgets the
+// kernels are built for: fp32 3, 4 or 5 resident CTAs per SM (default 4),
+// fp64 2 or 3 (default 2: twice the registers for the same state).
+template <typename S, typename In>
+dprop_status enqueue_rounds_s(const dprop_launch* lc, const dprop_detector* det,
+                              const dprop_field* field,
+                              const prop_cfg<S>& cfg,
+                              const io_ptrs<In, S>& io, uint64_t n,
+                              const uint32_t* order, void* scratch,
+                              size_t scratch_bytes, cudaStream_t stream,
+                              cudaEvent_t mark, uint32_t mark_round) {
+    constexpr bool fp64 = sizeof(S) == 8;
     if (n > 0x7fffffffull) {
         return fail(DPROP_E_INVALID, "persistent method: n_tracks too large");
     }
@@ -703,13 +738,15 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                     "plain method only");
     }
     const uint32_t rec_cap = staged_capacity(cfg, io);
-    if (scratch_bytes < rounds_scratch_bytes(n, det->wires, rec_cap)) {
+    const size_t need = fp64 ? rounds_scratch_bytes_fp64(n, det->wires, rec_cap)
+                             : rounds_scratch_bytes(n, det->wires, rec_cap);
+    if (scratch_bytes < need) {
         return fail(DPROP_E_INVALID, "persistent method: scratch too small");
     }
     void* base = reinterpret_cast<void*>(
         (reinterpret_cast<uintptr_t>(scratch) + 255u) & ~uintptr_t(255u));
-    rounds_layout L{};
-    rounds_layout_bytes(n, det->wires, rec_cap, &L, base);
+    rounds_layout<S> L{};
+    rounds_layout_bytes<S>(n, det->wires, rec_cap, &L, base);
     const uint32_t rounds = (lc && lc->rounds) ? lc->rounds : k_default_rounds;
     const uint32_t budget = (lc && lc->steps_per_round) ? lc->steps_per_round
                                                         : k_default_steps_per_round;
@@ -728,35 +765,69 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
         return fail(DPROP_E_INVALID,
                     "persistent method: block_size must be 0 or 128");
     }
-    // register budget of the step phase: resident CTAs per SM 3, 4 or 5
-    const uint32_t fb = (lc && lc->ctas_per_sm) ? lc->ctas_per_sm : 4u;
-    if (fb < 3u || fb > 5u) {
+    const uint32_t fb =
+        (lc && lc->ctas_per_sm) ? lc->ctas_per_sm : (fp64 ? 2u : 4u);
+    if (fp64 ? (fb < 2u || fb > 3u) : (fb < 3u || fb > 5u)) {
         return fail(DPROP_E_INVALID,
-                    "persistent method: ctas_per_sm must be 0, 3, 4 or 5");
+                    fp64 ? "persistent method, fp64: ctas_per_sm must be 0, "
+                           "2 or 3"
+                         : "persistent method: ctas_per_sm must be 0, 3, 4 "
+                           "or 5");
     }
     auto go = [&](auto fast_blocks) -> dprop_status {
         constexpr int FB = decltype(fast_blocks)::value;
         if (det->wires) {
-            return enqueue_rounds_w<In, true, FB>(det->view_as<true>(),
-                                                  field->view, cfg, io, n,
-                                                  order, L, rounds, budget,
-                                                  yield, sort_interval,
-                                                  tail_tracks, stream, mark,
-                                                  mark_round);
+            return enqueue_rounds_w<S, In, true, FB>(
+                det_view<S, true>(det), fld_view<S>(field), cfg, io, n, order,
+                L, rounds, budget, yield, sort_interval, tail_tracks, stream,
+                mark, mark_round);
         }
-        return enqueue_rounds_w<In, false, FB>(det->view_as<false>(),
-                                               field->view, cfg, io, n, order,
-                                               L, rounds, budget, yield,
-                                               sort_interval, tail_tracks,
-                                               stream, mark, mark_round);
+        return enqueue_rounds_w<S, In, false, FB>(
+            det_view<S, false>(det), fld_view<S>(field), cfg, io, n, order, L,
+            rounds, budget, yield, sort_interval, tail_tracks, stream, mark,
+            mark_round);
     };
-    if (fb == 3u) {
-        return go(std::integral_constant<int, 3>{});
+    if constexpr (fp64) {
+        if (fb == 3u) {
+            return go(std::integral_constant<int, 3>{});
+        }
+        return go(std::integral_constant<int, 2>{});
+    } else {
+        if (fb == 3u) {
+            return go(std::integral_constant<int, 3>{});
+        }
+        if (fb == 5u) {
+            return go(std::integral_constant<int, 5>{});
+        }
+        return go(std::integral_constant<int, 4>{});
     }
-    if (fb == 5u) {
-        return go(std::integral_constant<int, 5>{});
-    }
-    return go(std::integral_constant<int, 4>{});
+}
+
+}  // namespace
+
+template <typename In>
+dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
+                            const dprop_field* field,
+                            const prop_cfg<float>& cfg, const io_ptrs<In>& io,
+                            uint64_t n, const uint32_t* order, void* scratch,
+                            size_t scratch_bytes, cudaStream_t stream,
+                            cudaEvent_t mark, uint32_t mark_round) {
+    return enqueue_rounds_s<float, In>(lc, det, field, cfg, io, n, order,
+                                       scratch, scratch_bytes, stream, mark,
+                                       mark_round);
+}
+
+dprop_status enqueue_rounds_fp64(const dprop_launch* lc,
+                                 const dprop_detector* det,
+                                 const dprop_field* field,
+                                 const prop_cfg<double>& cfg,
+                                 const io_ptrs<double, double>& io,
+                                 uint64_t n, const uint32_t* order,
+                                 void* scratch, size_t scratch_bytes,
+                                 cudaStream_t stream) {
+    return enqueue_rounds_s<double, double>(lc, det, field, cfg, io, n, order,
+                                            scratch, scratch_bytes, stream,
+                                            nullptr, 0u);
 }
 
 template dprop_status enqueue_rounds<float>(const dprop_launch*,

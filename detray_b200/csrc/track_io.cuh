@@ -129,11 +129,12 @@ __device__ __forceinline__ void run_one(uint64_t t, uint64_t n,
 // or NULL).  rec_cap: records per track staged in the scratch (0 when no
 // records are requested, see staged_capacity).
 size_t rounds_scratch_bytes(uint64_t n, bool wires, uint32_t rec_cap);
+size_t rounds_scratch_bytes_fp64(uint64_t n, bool wires, uint32_t rec_cap);
 
 // Records per track the round-based propagation stages in its scratch: the
 // configuration's capacity when the caller asks for records.
-template <typename S, typename In>
-uint32_t staged_capacity(const prop_cfg<S>& cfg, const io_ptrs<In>& io) {
+template <typename S, typename In, typename O>
+uint32_t staged_capacity(const prop_cfg<S>& cfg, const io_ptrs<In, O>& io) {
     return io.rec_barcode != nullptr ? cfg.max_records : 0u;
 }
 
@@ -148,5 +149,15 @@ dprop_status enqueue_rounds(const dprop_launch* lc, const dprop_detector* det,
                             size_t scratch_bytes, cudaStream_t stream,
                             cudaEvent_t mark = nullptr,
                             uint32_t mark_round = 0u);
+
+// The same in double precision end to end (dprop_launch.precision = 8).
+dprop_status enqueue_rounds_fp64(const dprop_launch* lc,
+                                 const dprop_detector* det,
+                                 const dprop_field* field,
+                                 const prop_cfg<double>& cfg,
+                                 const io_ptrs<double, double>& io,
+                                 uint64_t n, const uint32_t* order,
+                                 void* scratch, size_t scratch_bytes,
+                                 cudaStream_t stream);
 
 }  // namespace dprop::api

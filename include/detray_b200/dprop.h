@@ -336,7 +336,9 @@ typedef struct dprop_launch {
                                     Plain method: 8 (64 registers), 12 (40)
                                     or 16 (32); 0 = 12.  Persistent method,
                                     its step phase: 3 (168 registers), 4
-                                    (128) or 5 (102); 0 = 4                   */
+                                    (128) or 5 (102); 0 = 4.  fp64 plain: 8
+                                    or 12 (0 = 8); fp64 persistent: 2 (255
+                                    registers) or 3 (168); 0 = 2              */
     uint32_t sort_tracks;        /* 1: process tracks ordered by direction
                                     (theta, phi) so that the lanes of a warp
                                     follow similar paths; results are still
@@ -348,9 +350,10 @@ typedef struct dprop_launch {
                                     arrays and results (the default);
                                     8: fp64 end to end - double track arrays,
                                     double arithmetic and double results (the
-                                    reference's full-fp64 build); plain kernel,
-                                    method and use_graph ignored.  Device API
-                                    (dprop_propagate) only                     */
+                                    reference's full-fp64 build); the plain
+                                    or the persistent method, use_graph
+                                    ignored.  Device API (dprop_propagate)
+                                    only                                       */
     /* Persistent method only (0: the library default of each): */
     uint32_t steps_per_round;    /* RK steps a track takes per round at most
                                     (default 16)                               */

@@ -418,14 +418,19 @@ def test_fp64_device_vs_oracle(torch_cuda, oracle, kind):
     ref_det = _oracle_detector(oracle, kind)
     ref = oracle.propagate(ref_det, field.spec, cfg, trk)
     dev = torch_cuda.tensor(trk, dtype=torch_cuda.float64, device="cuda")
-    lc = propagator.make_launch(sort_tracks=1, precision=8)
-    res = propagator.propagate(cfg, det, field, dev, launch=lc)
-    torch_cuda.cuda.synchronize()
-    got = {k: v.cpu().numpy() for k, v in res.tensors.items()}
-    got["rec_barcode"] = got["rec_barcode"].view(np.uint64)
-    assert res.tensors["rec_bound"].dtype == torch_cuda.float64
     tight = {"loc0": 1e-6, "loc1": 1e-6, "phi": 1e-9, "theta": 1e-9,
              "qop": 1e-12, "time": 1e-9}
-    s = compare(ref, got, max_seq_mismatch_frac=1e-4, tol_abs=tight,
-                tol_rel=1e-8, cov_rel=1e-6)
-    print(kind, s)
+    # the plain kernel and the round-based phase kernels in double
+    for kw in (dict(), dict(method=1), dict(method=1, ctas_per_sm=3)):
+        lc = propagator.make_launch(sort_tracks=1, precision=8, **kw)
+        res = propagator.propagate(cfg, det, field, dev, launch=lc)
+        torch_cuda.cuda.synchronize()
+        got = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+        got["rec_barcode"] = got["rec_barcode"].view(np.uint64)
+        assert res.tensors["rec_bound"].dtype == torch_cuda.float64
+        s = compare(ref, got, max_seq_mismatch_frac=1e-4, tol_abs=tight,
+                    tol_rel=1e-8, cov_rel=1e-6)
+        print(kind, kw, s)
+    with pytest.raises(propagator.PropagationError):
+        propagator.propagate(cfg, det, field, dev, launch=propagator.make_launch(
+            precision=8, method=1, ctas_per_sm=4))
