@@ -393,6 +393,12 @@ def test_launch_shape_does_not_change_results(torch_cuda):
         same(base, run(method=abi.METHOD_PERSISTENT, sort_tracks=1,
                        ctas_per_sm=4, sort_interval=si, use_graph=graph,
                        steps_per_round=4))
+    # the tail threshold only decides in which round the last tracks run
+    # to their end (1: after all rounds; n: in the first round)
+    n = trk.shape[1]
+    for tail in (1, n // 8, n, 10 * n):
+        same(base, run(method=abi.METHOD_PERSISTENT, sort_tracks=1,
+                       ctas_per_sm=4, tail_tracks=tail))
     # wire surfaces (the exact-cycle search state travels with the slots)
     det, field, cfg, trk = _setup("wire_chamber_10l_cells")
     dev = torch_cuda.tensor(trk, dtype=torch_cuda.float32, device="cuda")
