@@ -365,6 +365,41 @@ def test_graph_replay_and_autotune(torch_cuda):
     propagator.release_cache()
 
 
+@pytest.mark.parametrize("n", [1, 31, 33, 4095, 4097])
+def test_persistent_small_and_ragged_batches(torch_cuda, n):
+    """Batch sizes around the warp (32) and queue-tile (4096) boundaries:
+    the round-based method, fp32 (graph and direct) and fp64, gives the
+    plain kernel's surfaces and statuses."""
+    from detray_b200 import abi, propagator
+    det, field, cfg, trk = _setup("toy")
+    trk = np.ascontiguousarray(trk[:, :n])
+    for dtype, prec in ((torch_cuda.float32, 0), (torch_cuda.float64, 8)):
+        dev = torch_cuda.tensor(trk, dtype=dtype, device="cuda")
+
+        def run(**kw):
+            res = propagator.propagate(cfg, det, field, dev,
+                                       launch=propagator.make_launch(
+                                           precision=prec, **kw))
+            torch_cuda.cuda.synchronize()
+            out = {k: v.cpu().numpy() for k, v in res.tensors.items()}
+            return out
+
+        a = run(sort_tracks=1)
+        forms = [dict(method=abi.METHOD_PERSISTENT, sort_tracks=1),
+                 dict(method=abi.METHOD_PERSISTENT, sort_tracks=0)]
+        if prec == 0:
+            forms.append(dict(method=abi.METHOD_PERSISTENT, sort_tracks=1,
+                              use_graph=1))
+        for kw in forms:
+            b = run(**kw)
+            assert np.array_equal(a["status"], b["status"]), kw
+            assert np.array_equal(a["n_records"], b["n_records"]), kw
+            m = int(a["n_records"].max())
+            valid = np.arange(m)[:, None] < a["n_records"][None, :]
+            assert np.array_equal(a["rec_barcode"][:m][valid],
+                                  b["rec_barcode"][:m][valid]), kw
+
+
 def test_launch_shape_does_not_change_results(torch_cuda):
     """Block size (plain) and the volume re-sort interval (persistent) only
     reorder the work: every output is bit-identical to the default launch
