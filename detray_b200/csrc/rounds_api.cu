@@ -34,10 +34,18 @@
 //
 // Each phase kernel is persistent: a grid of the SMs' resident CTAs whose
 // warps pull 32 queue entries at a time from a device counter until the
-// queue is empty.  After `rounds` rounds, rounds_tail_kernel runs the tracks
-// still alive to their end with every segment inline.  Each kernel loads
-// and stores only the state its segments use, and a track driven through
-// the phases ends bit-identical to the plain kernel's result.
+// queue is empty.  Once fewer than tail_tracks tracks are alive (the count
+// kernel decides it on the device), that round's step phase runs them to
+// their end with every segment inline, as rounds_tail_kernel does after
+// the last round.  Records are staged as one 128-byte (fp32) or 256-byte
+// (fp64) row per record and converted to the result layout at the end
+// (rounds_unstage_kernel).  Each kernel loads and stores only the state its
+// segments use; the segments perform the loop's operations in its order,
+// so a track driven through the phases ends as it would in the one-shot
+// loop (bit for bit in a host build of both; on the device the separately
+// compiled kernels may contract multiply-adds differently in the last
+// bits).  Everything is templated on the arithmetic type: fp32, and fp64
+// for dprop_launch.precision = 8.
 #include <cuda_runtime.h>
 
 #include <cub/block/block_scan.cuh>
