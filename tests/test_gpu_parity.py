@@ -285,17 +285,20 @@ def test_device_loopers_end_cleanly(torch_cuda):
             assert (st == abi.TRK_NONFINITE).sum() > 0
 
 
-def test_host_api_jagged_equals_device_api(torch_cuda):
-    """The pipelined host path returning jagged records (several chunks, two
-    streams) gives the same records as the device API."""
+@pytest.mark.parametrize("method", [0, 1], ids=["plain", "persistent"])
+def test_host_api_jagged_equals_device_api(torch_cuda, method):
+    """The pipelined host path returning jagged records (several chunks on
+    their own streams, the persistent method's chunks staggered) gives the
+    same records as the device API with the same method."""
     from detray_b200 import abi, geometry, propagator, tracks
     from detray_b200.units import T
     det = propagator.Detector(geometry.load_geometry("toy_4brl_7edc"))
     field = propagator.Field.constant((0.0, 0.0, 2.0 * T))
     cfg = abi.make_config(max_records=24, search_window=(3, 3))
     trk = tracks.toy_tracks(600_000, seed=41)  # 3 chunks
-    a = _run_device(torch_cuda, det, field, cfg, trk)
-    lc = propagator.make_launch(sort_tracks=1)
+    a = _run_device(torch_cuda, det, field, cfg, trk, method=method,
+                    sort_tracks=1)
+    lc = propagator.make_launch(method=method, sort_tracks=1)
     b = propagator.propagate_host(cfg, det, field, trk, launch=lc, jagged=True)
     for key in ["status", "n_records", "n_trials", "path_length"]:
         assert np.array_equal(a[key], b[key]), key
