@@ -65,6 +65,7 @@ constexpr int k_build_threads = 256;  // 16 slots each: one tile per CTA
 static_assert(k_build_threads * 16 == static_cast<int>(k_queue_tile),
               "queue tile = 16 slots per thread");
 constexpr int k_phase_block = 128;
+constexpr uint32_t k_unstage_ways = 8u;
 
 // Queue of a segment: 0 step phase, 2 navigation, -1 ended (queue 1 holds
 // tracks waiting for the surface actors, which the step phase runs itself,
@@ -320,6 +321,15 @@ __device__ __forceinline__ void write_outputs(const api::io_ptrs<In, S>& io,
     }
 }
 
+// Whether the calling warp can find work in a queue of cnt entries: the
+// warps pull 32 entries at a time, so warps beyond the number of 32-entry
+// chunks leave at once instead of each taking a turn on the pull counter
+// (the other warps still take every chunk).
+__device__ __forceinline__ bool warp_has_work(uint32_t cnt) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    return warp < (cnt + 31u) / 32u;
+}
+
 // Next 32 queue entries for the calling warp (all lanes call it together).
 __device__ __forceinline__ uint32_t pull32(uint32_t* pull) {
     uint32_t base = 0u;
@@ -379,6 +389,9 @@ __global__ void __launch_bounds__(k_phase_block, MinBlocks)
                        uint64_t n, uint32_t step_budget, uint32_t yield_lanes,
                        uint32_t* stage) {
     const uint32_t cnt = *count;
+    if (!warp_has_work(cnt)) {
+        return;
+    }
     const unsigned lane = threadIdx.x & 31u;
     record_sink<S> rec = make_sink(io, n, cfg, stage);
     if (count[3] != 0u) {
@@ -453,6 +466,9 @@ __global__ void __launch_bounds__(k_phase_block, sizeof(S) == 4 ? 8 : 4)
                       const uint32_t* __restrict__ queue,
                       const uint32_t* __restrict__ count, uint32_t* pull) {
     const uint32_t cnt = *count;
+    if (!warp_has_work(cnt)) {
+        return;
+    }
     while (true) {
         const uint32_t base = pull32(pull);
         if (base >= cnt) {
@@ -495,10 +511,10 @@ __global__ void __launch_bounds__(k_phase_block, 8)
     }
 }
 
-// Staged records to the public slot-major arrays: thread (t, k) converts
-// record k of input track t (grid y strides over the record index), so
-// that every record is in flight at once and consecutive threads write
-// consecutive words of every array.
+// Staged records to the public slot-major arrays: thread (t, y) converts
+// records y, y + k_unstage_ways, ... of input track t, so that most
+// records are in flight at once and consecutive threads write consecutive
+// words of every array.
 template <typename S, typename In>
 __global__ void __launch_bounds__(k_phase_block)
     rounds_unstage_kernel(const __grid_constant__ prop_cfg<S> cfg,
@@ -643,10 +659,13 @@ dprop_status enqueue_rounds_w(const detector_view<S, W>& det,
                 L.qs.pull, n, L.stage);
             DPROP_CUDA(cudaGetLastError());
             if (L.stage != nullptr) {
+                // 8 record indices in flight per track (a track has ~8
+                // records); more mostly launches threads that find no record
+                // after two dependent loads
                 const dim3 ug(static_cast<unsigned int>(
                                   (n + k_phase_block - 1) / k_phase_block),
-                              cfg.max_records < 65535u ? cfg.max_records
-                                                       : 65535u);
+                              cfg.max_records < k_unstage_ways
+                                  ? cfg.max_records : k_unstage_ways);
                 rounds_unstage_kernel<S, In><<<ug, k_phase_block, 0, st>>>(
                     cfg, io, L.slots.rec_count, L.inv, L.stage, n);
                 DPROP_CUDA(cudaGetLastError());
