@@ -762,7 +762,7 @@ def run_ours(args):
         try:
             cpu = cpu_reference_rate(15.0, cfg, args.seed, 2_000_000,
                                      host_threads())
-            errors = parity_sample(cfg, host_trk, res, 4000)
+            errors = parity_sample(cfg, host_trk, res, 100_000)
         except (FileNotFoundError, OSError) as exc:
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
