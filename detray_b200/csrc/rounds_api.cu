@@ -162,6 +162,14 @@ __device__ void block_scan3(const uint32_t (&v)[3], uint32_t (&excl)[3],
 __global__ void __launch_bounds__(k_build_threads)
     queue_count_kernel(const uint8_t* __restrict__ pc, queue_set qs,
                        uint32_t n_tiles, int merged, uint32_t tail_tracks) {
+    if (qs.count[3] != 0u) {
+        // the previous round ran every live track to its end: nothing is
+        // left, the queues stay empty (count[3] stays set)
+        if (blockIdx.x == 0 && threadIdx.x < 3) {
+            qs.count[threadIdx.x] = 0u;
+        }
+        return;
+    }
     if (blockIdx.x == 0 && threadIdx.x < 3) {
         qs.pull[threadIdx.x] = 0u;
     }
@@ -255,6 +263,9 @@ __global__ void __launch_bounds__(k_build_threads)
     queue_scatter_kernel(const uint8_t* __restrict__ pc, queue_set qs) {
     const uint32_t tile = blockIdx.x;
     const bool m = qs.count[3] != 0u;
+    if (m && qs.count[0] == 0u) {
+        return;  // nothing alive
+    }
     uint32_t offset[3];
     for (int k = 0; k < 3; ++k) {
         offset[k] = qs.tiles[3u * tile + k];
@@ -643,6 +654,8 @@ dprop_status enqueue_rounds_w(const detector_view<S, W>& det,
         return s;
     }
     DPROP_CUDA(cudaMemsetAsync(L.qs.ticket, 0, sizeof(uint32_t), st));
+    // count[3] (the last round ran the tail) from an earlier call
+    DPROP_CUDA(cudaMemsetAsync(L.qs.count, 0, 4 * sizeof(uint32_t), st));
     rounds_init_kernel<S, In, W><<<g_init, k_phase_block, 0, st>>>(
         det, cfg, io, L.slots, n, n_pad, order, L.inv);
     DPROP_CUDA(cudaGetLastError());
