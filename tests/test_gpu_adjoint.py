@@ -76,9 +76,11 @@ def test_device_gradients_match_host_core(torch_cuda, core_host, kind, n):
     same = ah.same_records(href, {"n_records": dres["n_records"].astype(np.uint32),
                                   "rec_barcode": dres["rec_barcode"]})
     assert same.mean() >= 0.998, same.mean()
+    # every gradient component of every track whose records agree, within
+    # the tolerance (measured on B200: worst 6.7e-4 relative)
     for i in (0, 1, 2, 3, 4, 5, 6, 7):
         ok = _close(dfree[i][same], hfree[i][same])
-        assert ok.mean() >= 0.995, (i, ok.mean())
+        assert ok.all(), (i, int((~ok).sum()))
     # alignment: only tracks whose records agree contribute on the host side;
     # redo the host sweep without the others
     Wm = W * same[None, None, :]
@@ -87,7 +89,7 @@ def test_device_gradients_match_host_core(torch_cuda, core_host, kind, n):
     hit = np.abs(halign_m).sum(axis=1) > 0
     assert hit.sum() >= 5
     ok = _close(dalign_m[hit], halign_m[hit])
-    assert ok.mean() >= 0.99, ok.mean()
+    assert ok.all(), int((~ok).sum())
 
 
 def test_adjoint_mode_keeps_the_propagation(torch_cuda):
